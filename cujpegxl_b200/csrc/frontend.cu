@@ -1,0 +1,1171 @@
+// Fused frontend kernel (one CTA per 64x64 colour tile) and its host setup.
+//
+// Arithmetic contract. This file is compiled with -fmad=false: a*b+c is two
+// rounded operations unless written as jx_fma. Every float expression below is
+// the canonical definition that the CPU restatement in oracle/ reproduces
+// operation for operation, so the kernel's integer outputs (quant field,
+// transform choice, CfL maps, quantised coefficients) match it bit for bit.
+// Where the reference has a host twin of a stage (transform selection,
+// src/transform_select_impl.cuh; LLF -> DC, src/vardct_layout.h) the twin's
+// exact arithmetic is used, including its lack of FMA and its partial-sum
+// order, so results equal the twin's too.
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "frontend.cuh"
+#include "jxl_constants.cuh"
+#include "jxl_math.cuh"
+
+namespace jxb {
+namespace {
+
+#include "jxl_dequant_tables.inc"
+
+constexpr int kThreads = 256;
+constexpr int kTile = 64;
+constexpr int kHalo = 2;
+constexpr int kXs = kTile + 2 * kHalo;  // 68: stride of the unsharpened XYB tile
+constexpr int kXplane = kXs * kXs;
+constexpr int kSs = kTile + 1;          // 65: stride of the sharpened tile
+constexpr int kSplane = kTile * kSs;
+constexpr int kRegionAFloats = 3 * kXplane;  // 13872
+
+// Selection bases: double-precision DCT-II basis narrowed to float
+// (basis[k*n + t], src/transform_select.cu:29-37). Final-DCT bases: the float
+// basis of src/frontend_transform.cu:104-106 (cosf of a float argument).
+__constant__ float c_sel8[64];
+__constant__ float c_sel16[256];
+__constant__ float c_sel32[1024];
+__constant__ float c_dct8[64];
+__constant__ float c_dct16[256];
+__constant__ float c_dct32[1024];
+
+template <int N, bool kSel>
+__device__ __forceinline__ float basis(int i) {
+    if (kSel) {
+        return N == 8 ? c_sel8[i] : (N == 16 ? c_sel16[i] : c_sel32[i]);
+    }
+    return N == 8 ? c_dct8[i] : (N == 16 ? c_dct16[i] : c_dct32[i]);
+}
+
+struct Small {
+    float pre[256];       // AQ pre-erosion cells, 16x16 over the tile
+    float cost8[64];
+    float cost16[16];
+    float cost32[4];
+    float cfl[3][64];
+    int qf[64];
+    int nz[3][64];
+    int fb_off[64];       // final-DCT scratch offset of each listed first-block
+    unsigned char fb_list[64];
+    unsigned char owner[64];
+    signed char acs[64];
+    int n32, n16, n8;
+    int mx, mb;
+};
+
+constexpr std::size_t kSmemBytes =
+    sizeof(float) * (kRegionAFloats + 3 * kSplane) + sizeof(Small);
+
+__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
+
+// sRGB transfer function to linear (src/xyb_impl.cuh:37-40).
+__device__ __forceinline__ float srgb_to_linear(float e) {
+    return e <= 0.04045f ? e * (1.0f / 12.92f) : jx_pow24((e + 0.055f) * (1.0f / 1.055f));
+}
+
+// NV12 pixel (gx, gy) -> XYB (src/xyb_impl.cuh:49-70). Chroma is the centred
+// bilinear 2x upsample of the texture path (src/frontend_fused.cu:222), taken
+// exactly: the four taps carry weights {1,3}x{1,3}/16, summed in integers.
+__device__ __forceinline__ void xyb_pixel(const FrontendInputs& in, int gx, int gy, float& ox,
+                                          float& oy, float& ob) {
+    const float yv{static_cast<float>(in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx]) *
+                   kInv255};
+    const int cw{in.width >> 1};
+    const int ch{in.height >> 1};
+    const int jx{gx >> 1};
+    const int jy{gy >> 1};
+    int xa, xb, wxa, wxb, ya, yb, wya, wyb;
+    if (gx & 1) {
+        xa = jx; xb = min(jx + 1, cw - 1); wxa = 3; wxb = 1;
+    } else {
+        xa = max(jx - 1, 0); xb = jx; wxa = 1; wxb = 3;
+    }
+    if (gy & 1) {
+        ya = jy; yb = min(jy + 1, ch - 1); wya = 3; wyb = 1;
+    } else {
+        ya = max(jy - 1, 0); yb = jy; wya = 1; wyb = 3;
+    }
+    const std::uint8_t* ra{in.chroma + static_cast<std::size_t>(ya) * in.chroma_pitch};
+    const std::uint8_t* rb{in.chroma + static_cast<std::size_t>(yb) * in.chroma_pitch};
+    const int scb{wya * (wxa * ra[2 * xa] + wxb * ra[2 * xb]) +
+                  wyb * (wxa * rb[2 * xa] + wxb * rb[2 * xb])};
+    const int scr{wya * (wxa * ra[2 * xa + 1] + wxb * ra[2 * xb + 1]) +
+                  wyb * (wxa * rb[2 * xa + 1] + wxb * rb[2 * xb + 1])};
+    const float cb{static_cast<float>(scb) / 4080.0f - kChromaCenter};
+    const float cr{static_cast<float>(scr) / 4080.0f - kChromaCenter};
+
+    const float r{clamp01(srgb_to_linear(clamp01(jx_fma(kCrToR, cr, yv))))};
+    const float g{clamp01(srgb_to_linear(clamp01(jx_fma(-kCrToG, cr, jx_fma(-kCbToG, cb, yv)))))};
+    const float b{clamp01(srgb_to_linear(clamp01(jx_fma(kCbToB, cb, yv))))};
+
+    float m0{jx_fma(kM02, b, jx_fma(kM01, g, kM00 * r)) + kOpsinBias};
+    float m1{jx_fma(kM12, b, jx_fma(kM11, g, kM10 * r)) + kOpsinBias};
+    float m2{jx_fma(kM22, b, jx_fma(kM21, g, kM20 * r)) + kOpsinBias};
+    m0 = jx_cbrt(fmaxf(m0, 0.0f)) + kNegCbrtBias;
+    m1 = jx_cbrt(fmaxf(m1, 0.0f)) + kNegCbrtBias;
+    m2 = jx_cbrt(fmaxf(m2, 0.0f)) + kNegCbrtBias;
+    ox = 0.5f * (m0 - m1);
+    oy = 0.5f * (m0 + m1);
+    ob = m2;
+}
+
+// RatioOfDerivativesOfCubicRootToSimpleGamma (src/adaptive_quant_impl.cuh:44-55).
+template <bool kInvert>
+__device__ __forceinline__ float ratio_gamma(float v) {
+    v = v < 0.0f ? 0.0f : v;
+    const float v2{v * v};
+    const float num{jx_fma(kRatioNumMul, v2, kRatioEps)};
+    const float den{jx_fma(kRatioDenMul * v, v2, kRatioVOffset)};
+    return kInvert ? num / den : den / num;
+}
+
+// src/adaptive_quant_impl.cuh:57-61.
+__device__ __forceinline__ float masking_sqrt(float v, float sqrt_mul) {
+    return 0.25f * sqrtf(jx_fma(v, sqrt_mul, kMaskLogOffset));
+}
+
+// src/adaptive_quant_impl.cuh:63-76.
+__device__ __forceinline__ float compute_mask(float out_val) {
+    const float v1{fmaxf(out_val * kMaskMul0, 1e-3f)};
+    const float v2{1.0f / (v1 + kMaskOffset2)};
+    const float v3{1.0f / jx_fma(v1, v1, kMaskOffset3)};
+    const float v4{1.0f / jx_fma(v1, v1, kMaskOffset4)};
+    float r{jx_fma(kMaskMul4, v4, kMaskBase)};
+    r = jx_fma(kMaskMul2, v2, r);
+    r = jx_fma(kMaskMul3, v3, r);
+    return r;
+}
+
+__device__ __forceinline__ void swap_if(float& a, float& b) {
+    if (a > b) {
+        const float t{a};
+        a = b;
+        b = t;
+    }
+}
+
+__device__ __forceinline__ void keep_min4(float v, float& m0, float& m1, float& m2, float& m3) {
+    if (v < m3) {
+        if (v < m0) {
+            m3 = m2; m2 = m1; m1 = m0; m0 = v;
+        } else if (v < m1) {
+            m3 = m2; m2 = m1; m1 = v;
+        } else if (v < m2) {
+            m3 = m2; m2 = v;
+        } else {
+            m3 = v;
+        }
+    }
+}
+
+// FuzzyErosion of cell (cx, cy) of one 32x32 AQ tile whose 8x8 cells start at
+// (sx0, sy0) in the 16x16 tile grid: weighted four smallest of the 3x3
+// neighbourhood clamped to the AQ tile (src/frontend_fused.cu:35-53).
+__device__ float erosion_cell(const float* pre, int sx0, int sy0, int cx, int cy, float km0,
+                              float km1, float km2, float km3) {
+    const int xm{cx > 0 ? cx - 1 : cx};
+    const int xp{cx + 1 < 8 ? cx + 1 : cx};
+    const int ym{cy > 0 ? cy - 1 : cy};
+    const int yp{cy + 1 < 8 ? cy + 1 : cy};
+    auto at = [&](int x, int y) { return pre[(sy0 + y) * 16 + sx0 + x]; };
+    float m0{at(cx, cy)};
+    float m1{at(xm, cy)};
+    float m2{at(xp, cy)};
+    float m3{at(xm, ym)};
+    swap_if(m0, m1);
+    swap_if(m0, m2);
+    swap_if(m0, m3);
+    swap_if(m1, m2);
+    swap_if(m1, m3);
+    swap_if(m2, m3);
+    keep_min4(at(cx, ym), m0, m1, m2, m3);
+    keep_min4(at(xp, ym), m0, m1, m2, m3);
+    keep_min4(at(xm, yp), m0, m1, m2, m3);
+    keep_min4(at(cx, yp), m0, m1, m2, m3);
+    keep_min4(at(xp, yp), m0, m1, m2, m3);
+    float r{km0 * m0};
+    r = jx_fma(km1, m1, r);
+    r = jx_fma(km2, m2, r);
+    r = jx_fma(km3, m3, r);
+    return r;
+}
+
+// Sum over the 32 lanes with the shfl_down pairing (offsets 16..1); the total
+// lands in lane 0.
+__device__ __forceinline__ float warp_tree(float v) {
+#pragma unroll
+    for (int off{16}; off > 0; off >>= 1) {
+        v = v + __shfl_down_sync(0xffffffffu, v, off);
+    }
+    return v;
+}
+
+// Row pass of an N-point separable DCT: dst[fx*(N+1)] for fx in [F0, F1) from
+// one pixel row. Selection bases accumulate without FMA (the host twin's
+// arithmetic); final-DCT bases accumulate with FMA.
+template <int N, int F0, int F1, bool kSel>
+__device__ __forceinline__ void row_pass(const float* src, float* dst) {
+    float p[N];
+#pragma unroll
+    for (int c{0}; c < N; ++c) {
+        p[c] = src[c];
+    }
+#pragma unroll
+    for (int fx{F0}; fx < F1; ++fx) {
+        float s{0.0f};
+#pragma unroll
+        for (int c{0}; c < N; ++c) {
+            if (kSel) {
+                s = s + basis<N, true>(fx * N + c) * p[c];
+            } else {
+                s = jx_fma(basis<N, false>(fx * N + c), p[c], s);
+            }
+        }
+        dst[fx * (N + 1)] = s;
+    }
+}
+
+// Column pass of the selection proxy fused with its quantiser: for fy in
+// [Y0, Y1) computes coefficient (fx, fy), quantises it with the DCT8 Y weight
+// sampled at the coefficient's frequency and stores its distortion and rate
+// contributions (zero for the low-frequency corner), as in block_ac_cost
+// (src/transform_select_impl.cuh:80-106).
+template <int N, int Y0, int Y1>
+__device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, float* cr_fx, int fx,
+                                        float qgsf, const float* wsel, const float* l2t) {
+    float rr[N];
+#pragma unroll
+    for (int r{0}; r < N; ++r) {
+        rr[r] = rows_fx[r];
+    }
+#pragma unroll
+    for (int fy{Y0}; fy < Y1; ++fy) {
+        float coeff{0.0f};
+#pragma unroll
+        for (int r{0}; r < N; ++r) {
+            coeff = coeff + basis<N, true>(fy * N + r) * rr[r];
+        }
+        float d{0.0f};
+        float rt{0.0f};
+        if (!(fx < N / 8 && fy < N / 8)) {
+            const float w{wsel[fx * N + fy]};
+            const float q{rintf((coeff * qgsf) / w)};
+            const float err{(q * w) / qgsf - coeff};
+            d = err * err;
+            if (q != 0.0f) {
+                int a{static_cast<int>(fabsf(q))};
+                a = a < kLog2TableSize ? a : kLog2TableSize - 1;
+                rt = 1.0f + l2t[a];
+            }
+        }
+        cd_fx[fy] = d;
+        cr_fx[fy] = rt;
+    }
+}
+
+// Final-DCT column pass: coefficients (fx, fy) for fy in [Y0, Y1), rounded to
+// FP16 and stored at their covered-block slot in the tile's coefficient
+// buffer (src/frontend_transform.cu:252-262).
+template <int N, int Y0, int Y1>
+__device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int fx, int fbx,
+                                        int fby) {
+    float rr[N];
+#pragma unroll
+    for (int r{0}; r < N; ++r) {
+        rr[r] = rows_fx[r];
+    }
+    constexpr int side{N / 8};
+#pragma unroll
+    for (int fy{Y0}; fy < Y1; ++fy) {
+        float coeff{0.0f};
+#pragma unroll
+        for (int r{0}; r < N; ++r) {
+            coeff = jx_fma(basis<N, false>(fy * N + r), rr[r], coeff);
+        }
+        const int raw{fx * N + fy};
+        const int q{raw >> 6};
+        const int lb{(fby + q / side) * 8 + fbx + q % side};
+        coef[lb * 64 + (raw & 63)] = __float2half_rn(coeff);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
+    extern __shared__ __align__(16) float smem[];
+    float* xyb{smem};                                // [3][68*68]
+    float* shp{smem + kRegionAFloats};               // [3][64*65]
+    Small& sm{*reinterpret_cast<Small*>(smem + kRegionAFloats + 3 * kSplane)};
+
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int lane{tid & 31};
+    const int warp{tid >> 5};
+    const int W{in.width};
+    const int H{in.height};
+    const int bw{W >> 3};
+    const int bh{H >> 3};
+    const int nblocks{bw * bh};
+    const int tx{static_cast<int>(blockIdx.x)};
+    const int ty{static_cast<int>(blockIdx.y)};
+    const int px0{tx * kTile};
+    const int py0{ty * kTile};
+    const int bx0{tx * 8};
+    const int by0{ty * 8};
+
+    // ---- 1. NV12 -> XYB over the tile and a 2-pixel halo (clamped coordinates).
+    for (int i{tid}; i < kXplane; i += kThreads) {
+        const int lx{i % kXs};
+        const int ly{i / kXs};
+        const int gx{min(max(px0 - kHalo + lx, 0), W - 1)};
+        const int gy{min(max(py0 - kHalo + ly, 0), H - 1)};
+        float x, y, b;
+        xyb_pixel(in, gx, gy, x, y, b);
+        xyb[i] = x;
+        xyb[kXplane + i] = y;
+        xyb[2 * kXplane + i] = b;
+    }
+    __syncthreads();
+
+    if (out.dbg_xyb != nullptr) {
+        for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
+            const int c{i / (kTile * kTile)};
+            const int p{i % (kTile * kTile)};
+            const int gx{px0 + p % kTile};
+            const int gy{py0 + p / kTile};
+            if (gx < W && gy < H) {
+                out.dbg_xyb[(static_cast<std::size_t>(c) * H + gy) * W + gx] =
+                    xyb[c * kXplane + (p / kTile + kHalo) * kXs + p % kTile + kHalo];
+            }
+        }
+    }
+
+    // ---- 2. adaptive quantisation (src/frontend_fused.cu:233-342).
+    const float* Y{xyb + kXplane};
+    {
+        const int ccx{tid & 15};
+        const int ccy{tid >> 4};
+        float sum{0.0f};
+        for (int dy{0}; dy < 4; ++dy) {
+            for (int dx{0}; dx < 4; ++dx) {
+                const int ix{ccx * 4 + dx + kHalo};
+                const int iy{ccy * 4 + dy + kHalo};
+                const float yv{Y[iy * kXs + ix]};
+                const float base{0.25f * (((Y[(iy + 1) * kXs + ix] + Y[(iy - 1) * kXs + ix]) +
+                                          Y[iy * kXs + ix - 1]) +
+                                         Y[iy * kXs + ix + 1])};
+                float d{ratio_gamma<false>(yv + kMatchGammaOffset) * (yv - base)};
+                d = d * d;
+                d = fminf(d, kDiffLimit);
+                sum = sum + masking_sqrt(d, sc.mask_sqrt_mul);
+            }
+        }
+        sm.pre[tid] = 0.25f * sum;
+    }
+    __syncthreads();
+    for (int lb{warp}; lb < 64; lb += kThreads / 32) {
+        const int lbx{lb & 7};
+        const int lby{lb >> 3};
+        const int gbx{bx0 + lbx};
+        const int gby{by0 + lby};
+        if (gbx >= bw || gby >= bh) {
+            continue;  // warp-uniform
+        }
+        const int fx{lane & 7};
+        float red[2][4];
+        for (int half{0}; half < 2; ++half) {
+            const int fy{(lane >> 3) + 4 * half};
+            const int ix{lbx * 8 + fx + kHalo};
+            const int iy{lby * 8 + fy + kHalo};
+            const float yv{Y[iy * kXs + ix]};
+            const float xv{xyb[iy * kXs + ix]};
+            const float bv{xyb[2 * kXplane + iy * kXs + ix]};
+            float hf{0.0f};
+            if (fx < 7) {
+                hf = hf + fminf(kHfValMin, fabsf(yv - Y[iy * kXs + ix + 1]));
+            }
+            if (fy < 7) {
+                hf = hf + fminf(kHfValMin, fabsf(yv - Y[(iy + 1) * kXs + ix]));
+            }
+            const float iny{yv + kGammaBias};
+            const float gp{ratio_gamma<true>(iny - xv) + ratio_gamma<true>(iny + xv)};
+            const float pye{(yv + kBlueOffset) + fabsf(xv)};
+            const float bp{bv > pye ? fminf(bv - pye, kBlueLimit) : 0.0f};
+            float er{0.0f};
+            if (half == 0 && lane < 4) {
+                er = erosion_cell(sm.pre, (lbx >> 2) * 8, (lby >> 2) * 8, 2 * (lbx & 3) + (lane & 1),
+                                  2 * (lby & 3) + (lane >> 1), sc.km0, sc.km1, sc.km2, sc.km3);
+            }
+            red[half][0] = warp_tree(hf);
+            red[half][1] = warp_tree(gp);
+            red[half][2] = warp_tree(bp);
+            red[half][3] = warp_tree(er);
+        }
+        if (lane == 0) {
+            const float hf_sum{red[0][0] + red[1][0]};
+            const float gamma_overall{(red[0][1] + red[1][1]) * (0.5f / 64.0f)};
+            float blue_sum{red[0][2] + red[1][2]};
+            const float aq{red[0][3] + red[1][3]};
+            if (blue_sum >= 32.0f * kBlueLimit) {
+                blue_sum = 64.0f * kBlueLimit - blue_sum;
+            }
+            if (blue_sum >= kBlueMaxLimit * kBlueLimit) {
+                blue_sum = kBlueMaxLimit * kBlueLimit;
+            }
+            float ov{compute_mask(aq)};
+            ov = ov + jx_fma(hf_sum, kHfMul, kHfAdd);
+            ov = jx_fma(kGammaLogMul, jx_log2(gamma_overall), ov);
+            ov = jx_fma(blue_sum, kBlueMul, ov);
+            const float qval{jx_fma(jx_exp(ov), sc.mul_pb, sc.add_pb)};
+            int qi{static_cast<int>(jx_fma(qval, sc.inv_global_scale, 0.5f))};
+            qi = qi < 1 ? 1 : (qi > kQuantMax ? kQuantMax : qi);
+            sm.qf[lb] = qi;
+        }
+    }
+
+    // ---- 3. inverse gaborish, 5x5 with image-border clamping (src/frontend_transform.cu:19-36).
+    for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
+        const int c{i >> 12};
+        const int p{i & 4095};
+        const int x{p & 63};
+        const int y{p >> 6};
+        const float* P{xyb + c * kXplane + (y + kHalo) * kXs + x + kHalo};
+        auto at = [&](int dx, int dy) { return P[dy * kXs + dx]; };
+        const float e{((at(-1, 0) + at(1, 0)) + at(0, -1)) + at(0, 1)};
+        const float r2{((at(-2, 0) + at(2, 0)) + at(0, -2)) + at(0, 2)};
+        const float dg{((at(-1, -1) + at(1, -1)) + at(-1, 1)) + at(1, 1)};
+        const float l8{((((((at(-2, -1) + at(2, -1)) + at(-2, 1)) + at(2, 1)) + at(-1, -2)) +
+                         at(1, -2)) + at(-1, 2)) + at(1, 2)};
+        const float d4{((at(-2, -2) + at(2, -2)) + at(-2, 2)) + at(2, 2)};
+        float s{kGabC * at(0, 0)};
+        s = jx_fma(kGabEdge, e, s);
+        s = jx_fma(kGabEdge2, r2, s);
+        s = jx_fma(kGabDiag, dg, s);
+        s = jx_fma(kGabKnight, l8, s);
+        s = jx_fma(kGabDiag2, d4, s);
+        shp[c * kSplane + y * kSs + x] = s;
+    }
+    __syncthreads();
+
+    if (out.dbg_sharp != nullptr) {
+        for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
+            const int c{i >> 12};
+            const int p{i & 4095};
+            const int gx{px0 + (p & 63)};
+            const int gy{py0 + (p >> 6)};
+            if (gx < W && gy < H) {
+                out.dbg_sharp[(static_cast<std::size_t>(c) * H + gy) * W + gx] =
+                    shp[c * kSplane + (p >> 6) * kSs + (p & 63)];
+            }
+        }
+    }
+
+    // ---- 4. transform selection on the sharpened Y (src/transform_select.cu:134-262).
+    const float* SY{shp + kSplane};
+    float* rows{smem};             // region A reused: row-pass scratch
+    float* cdist{smem + 4608};     // per-coefficient distortion contributions
+    float* crate{smem + 9216};     // per-coefficient rate contributions
+    const float qg{sc.qgsf_select};
+    // 4a. DCT8 candidates: one per block inside the image.
+    for (int k{tid}; k < 512; k += kThreads) {
+        const int lb{k >> 3};
+        const int r{k & 7};
+        const int lbx{lb & 7};
+        const int lby{lb >> 3};
+        if (bx0 + lbx < bw && by0 + lby < bh) {
+            row_pass<8, 0, 8, true>(SY + (lby * 8 + r) * kSs + lbx * 8, rows + lb * 72 + r);
+        }
+    }
+    __syncthreads();
+    for (int k{tid}; k < 512; k += kThreads) {
+        const int lb{k >> 3};
+        const int fx{k & 7};
+        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
+            sel_col<8, 0, 8>(rows + lb * 72 + fx * 9, cdist + lb * 72 + fx * 9,
+                             crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p);
+        }
+    }
+    __syncthreads();
+    for (int lb{warp}; lb < 64; lb += kThreads / 32) {
+        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
+            const int i0{lb * 72 + (lane >> 3) * 9 + (lane & 7)};
+            const int i1{lb * 72 + ((lane + 32) >> 3) * 9 + (lane & 7)};
+            const float D{warp_tree(cdist[i0] + cdist[i1])};
+            const float R{warp_tree(crate[i0] + crate[i1])};
+            if (lane == 0) {
+                sm.cost8[lb] = 64.0f * D + kSelectLambda * R;
+            }
+        }
+    }
+    __syncthreads();
+    // 4b. DCT16 candidates: the 16 quads of the tile that fit in the image.
+    for (int k{tid}; k < 256; k += kThreads) {
+        const int qd{k >> 4};
+        const int r{k & 15};
+        const int qx{qd & 3};
+        const int qy{qd >> 2};
+        if (bx0 + 2 * qx + 2 <= bw && by0 + 2 * qy + 2 <= bh) {
+            row_pass<16, 0, 16, true>(SY + (qy * 16 + r) * kSs + qx * 16, rows + qd * 272 + r);
+        }
+    }
+    __syncthreads();
+    for (int k{tid}; k < 256; k += kThreads) {
+        const int qd{k >> 4};
+        const int fx{k & 15};
+        if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh) {
+            sel_col<16, 0, 16>(rows + qd * 272 + fx * 17, cdist + qd * 272 + fx * 17,
+                               crate + qd * 272 + fx * 17, fx, qg, tb.sel_weight + 1024,
+                               tb.log2_1p);
+        }
+    }
+    __syncthreads();
+    for (int qd{warp}; qd < 16; qd += kThreads / 32) {
+        if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh) {
+            float pd[8];
+            float pr[8];
+#pragma unroll
+            for (int j{0}; j < 8; ++j) {
+                const int t{lane + 32 * j};
+                pd[j] = cdist[qd * 272 + (t >> 4) * 17 + (t & 15)];
+                pr[j] = crate[qd * 272 + (t >> 4) * 17 + (t & 15)];
+            }
+#pragma unroll
+            for (int j{0}; j < 4; ++j) {
+                pd[j] = pd[j] + pd[j + 4];
+                pr[j] = pr[j] + pr[j + 4];
+            }
+            pd[0] = pd[0] + pd[2];
+            pd[1] = pd[1] + pd[3];
+            pr[0] = pr[0] + pr[2];
+            pr[1] = pr[1] + pr[3];
+            const float D{warp_tree(pd[0] + pd[1])};
+            const float R{warp_tree(pr[0] + pr[1])};
+            if (lane == 0) {
+                sm.cost16[qd] = 256.0f * D + kSelectLambda * R;
+            }
+        }
+    }
+    __syncthreads();
+    // 4c. DCT32 candidates: the 4 regions of the tile that fit in the image.
+    for (int k{tid}; k < 256; k += kThreads) {
+        const int ri{k >> 6};
+        const int r{k & 31};
+        const bool hi{(k & 32) != 0};
+        const int rx{ri & 1};
+        const int ry{ri >> 1};
+        if (bx0 + 4 * rx + 4 <= bw && by0 + 4 * ry + 4 <= bh) {
+            const float* src{SY + (ry * 32 + r) * kSs + rx * 32};
+            float* dst{rows + ri * 1056 + r};
+            if (hi) {
+                row_pass<32, 16, 32, true>(src, dst);
+            } else {
+                row_pass<32, 0, 16, true>(src, dst);
+            }
+        }
+    }
+    __syncthreads();
+    for (int k{tid}; k < 256; k += kThreads) {
+        const int ri{k >> 6};
+        const int fx{k & 31};
+        const bool hi{(k & 32) != 0};
+        if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh) {
+            const float* src{rows + ri * 1056 + fx * 33};
+            float* cd{cdist + ri * 1056 + fx * 33};
+            float* cr{crate + ri * 1056 + fx * 33};
+            if (hi) {
+                sel_col<32, 16, 32>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p);
+            } else {
+                sel_col<32, 0, 16>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p);
+            }
+        }
+    }
+    __syncthreads();
+    if (warp < 4) {
+        const int ri{warp};
+        if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh) {
+            float pd[8];
+            float pr[8];
+#pragma unroll
+            for (int j{0}; j < 8; ++j) {
+                float d{0.0f};
+                float r{0.0f};
+#pragma unroll
+                for (int m{0}; m < 4; ++m) {
+                    const int e{lane + 32 * j + 256 * m};
+                    d = d + cdist[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+                    r = r + crate[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+                }
+                pd[j] = d;
+                pr[j] = r;
+            }
+#pragma unroll
+            for (int j{0}; j < 4; ++j) {
+                pd[j] = pd[j] + pd[j + 4];
+                pr[j] = pr[j] + pr[j + 4];
+            }
+            pd[0] = pd[0] + pd[2];
+            pd[1] = pd[1] + pd[3];
+            pr[0] = pr[0] + pr[2];
+            pr[1] = pr[1] + pr[3];
+            const float D{warp_tree(pd[0] + pd[1])};
+            const float R{warp_tree(pr[0] + pr[1])};
+            if (lane == 0) {
+                sm.cost32[ri] = 1024.0f * D + kSelectLambda * R;
+            }
+        }
+    }
+    __syncthreads();
+    // 4d. RD decision per region (src/transform_select_impl.cuh:130-201).
+    if (tid < 4) {
+        const int ri{tid};
+        const int rlx{(ri & 1) * 4};
+        const int rly{(ri >> 1) * 4};
+        const int rbx{bx0 + rlx};
+        const int rby{by0 + rly};
+        if (rbx < bw && rby < bh) {
+            constexpr float kInf{1.0e30f};
+            const bool fit32{rbx + 4 <= bw && rby + 4 <= bh};
+            const float c32{fit32 ? sm.cost32[ri] : kInf};
+            float split{0.0f};
+            int choice[2][2];
+            for (int qy{0}; qy < 2; ++qy) {
+                for (int qx{0}; qx < 2; ++qx) {
+                    const int bx{rbx + 2 * qx};
+                    const int by{rby + 2 * qy};
+                    float sum8{0.0f};
+                    bool any{false};
+                    for (int dy{0}; dy < 2; ++dy) {
+                        for (int dx{0}; dx < 2; ++dx) {
+                            if (bx + dx < bw && by + dy < bh) {
+                                sum8 = sum8 + sm.cost8[(rly + 2 * qy + dy) * 8 + rlx + 2 * qx + dx];
+                                any = true;
+                            }
+                        }
+                    }
+                    if (!any) {
+                        choice[qy][qx] = -1;
+                        continue;
+                    }
+                    const bool fit16{bx + 2 <= bw && by + 2 <= bh};
+                    const float c16{fit16 ? sm.cost16[((rly >> 1) + qy) * 4 + (rlx >> 1) + qx] : kInf};
+                    if (fit16 && c16 <= sum8 + kSelectSplitEps) {
+                        choice[qy][qx] = 16;
+                        split = split + c16;
+                    } else {
+                        choice[qy][qx] = 8;
+                        split = split + sum8;
+                    }
+                }
+            }
+            if (fit32 && c32 <= split + kSelectSplitEps) {
+                for (int dy{0}; dy < 4; ++dy) {
+                    for (int dx{0}; dx < 4; ++dx) {
+                        sm.acs[(rly + dy) * 8 + rlx + dx] = (dx == 0 && dy == 0) ? 32 : 0;
+                    }
+                }
+            } else {
+                for (int qy{0}; qy < 2; ++qy) {
+                    for (int qx{0}; qx < 2; ++qx) {
+                        const int ch{choice[qy][qx]};
+                        if (ch < 0) {
+                            continue;
+                        }
+                        for (int dy{0}; dy < 2; ++dy) {
+                            for (int dx{0}; dx < 2; ++dx) {
+                                const int l{(rly + 2 * qy + dy) * 8 + rlx + 2 * qx + dx};
+                                if (ch == 16) {
+                                    sm.acs[l] = (dx == 0 && dy == 0) ? 16 : 0;
+                                } else if (rbx + 2 * qx + dx < bw && rby + 2 * qy + dy < bh) {
+                                    sm.acs[l] = 8;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // 4e. first-block list (largest first) and covering owner of every block.
+    if (tid == 0) {
+        int n[3]{0, 0, 0};
+        for (int lb{0}; lb < 64; ++lb) {
+            sm.owner[lb] = 255;
+        }
+        for (int lb{0}; lb < 64; ++lb) {
+            if (bx0 + (lb & 7) >= bw || by0 + (lb >> 3) >= bh) {
+                continue;
+            }
+            const int side{sm.acs[lb]};
+            if (side == 0) {
+                continue;
+            }
+            n[side == 32 ? 0 : (side == 16 ? 1 : 2)]++;
+            const int s{side >> 3};
+            for (int dy{0}; dy < s; ++dy) {
+                for (int dx{0}; dx < s; ++dx) {
+                    sm.owner[lb + dy * 8 + dx] = static_cast<unsigned char>(lb);
+                }
+            }
+        }
+        int at[3]{0, n[0], n[0] + n[1]};
+        int off[3]{0, n[0] * 1056, n[0] * 1056 + n[1] * 272};
+        for (int lb{0}; lb < 64; ++lb) {
+            if (bx0 + (lb & 7) >= bw || by0 + (lb >> 3) >= bh || sm.acs[lb] == 0) {
+                continue;
+            }
+            const int side{sm.acs[lb]};
+            const int g{side == 32 ? 0 : (side == 16 ? 1 : 2)};
+            sm.fb_list[at[g]] = static_cast<unsigned char>(lb);
+            sm.fb_off[at[g]] = off[g];
+            at[g]++;
+            off[g] += side * (side + 1);
+        }
+        sm.n32 = n[0];
+        sm.n16 = n[1];
+        sm.n8 = n[2];
+    }
+    if (tid < 192) {
+        sm.nz[tid >> 6][tid & 63] = 0;
+    }
+    __syncthreads();
+
+    // ---- 5. variable DCT of X, Y, B -> FP16 coefficients (src/frontend_transform.cu:190-266).
+    __half* coef{reinterpret_cast<__half*>(smem)};  // [3][64 blocks][64 slots]
+    float* drows{smem + 6144};
+    const int n32{sm.n32};
+    const int n16{sm.n16};
+    const int n8{sm.n8};
+    const int t32{64 * n32};
+    const int t16{t32 + 16 * n16};
+    const int tall{t16 + 8 * n8};
+    for (int c{0}; c < 3; ++c) {
+        const float* P{shp + c * kSplane};
+        for (int k{tid}; k < tall; k += kThreads) {
+            if (k < t32) {
+                const int f{k >> 6};
+                const int lb{sm.fb_list[f]};
+                const int r{k & 31};
+                const float* src{P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8};
+                float* dst{drows + sm.fb_off[f] + r};
+                if (k & 32) {
+                    row_pass<32, 16, 32, false>(src, dst);
+                } else {
+                    row_pass<32, 0, 16, false>(src, dst);
+                }
+            } else if (k < t16) {
+                const int f{n32 + ((k - t32) >> 4)};
+                const int lb{sm.fb_list[f]};
+                const int r{(k - t32) & 15};
+                row_pass<16, 0, 16, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8,
+                                           drows + sm.fb_off[f] + r);
+            } else {
+                const int f{n32 + n16 + ((k - t16) >> 3)};
+                const int lb{sm.fb_list[f]};
+                const int r{(k - t16) & 7};
+                row_pass<8, 0, 8, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8,
+                                         drows + sm.fb_off[f] + r);
+            }
+        }
+        __syncthreads();
+        __half* cc{coef + c * 4096};
+        for (int k{tid}; k < tall; k += kThreads) {
+            if (k < t32) {
+                const int f{k >> 6};
+                const int lb{sm.fb_list[f]};
+                const int fx{k & 31};
+                const float* src{drows + sm.fb_off[f] + fx * 33};
+                if (k & 32) {
+                    dct_col<32, 16, 32>(src, cc, fx, lb & 7, lb >> 3);
+                } else {
+                    dct_col<32, 0, 16>(src, cc, fx, lb & 7, lb >> 3);
+                }
+            } else if (k < t16) {
+                const int f{n32 + ((k - t32) >> 4)};
+                const int lb{sm.fb_list[f]};
+                const int fx{(k - t32) & 15};
+                dct_col<16, 0, 16>(drows + sm.fb_off[f] + fx * 17, cc, fx, lb & 7, lb >> 3);
+            } else {
+                const int f{n32 + n16 + ((k - t16) >> 3)};
+                const int lb{sm.fb_list[f]};
+                const int fx{(k - t16) & 7};
+                dct_col<8, 0, 8>(drows + sm.fb_off[f] + fx * 9, cc, fx, lb & 7, lb >> 3);
+            }
+        }
+        __syncthreads();
+    }
+
+    if (out.dbg_coeff != nullptr) {
+        for (int i{tid}; i < 3 * 4096; i += kThreads) {
+            const int c{i >> 12};
+            const int lb{(i >> 6) & 63};
+            const int gbx{bx0 + (lb & 7)};
+            const int gby{by0 + (lb >> 3)};
+            if (gbx < bw && gby < bh) {
+                out.dbg_coeff[static_cast<std::size_t>(c) * nblocks * 64 +
+                              (static_cast<std::size_t>(gby) * bw + gbx) * 64 + (i & 63)] =
+                    __half_as_ushort(coef[i]);
+            }
+        }
+    }
+
+    // ---- 6. chroma from luma over the tile (src/frontend_quantize.cu:49-117).
+    if (tid < 64) {
+        float sxy{0.0f};
+        float syy{0.0f};
+        float sby{0.0f};
+        const int lb{tid};
+        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
+            const int n{sm.acs[lb]};
+            const int side{n >> 3};
+            for (int raw{0}; raw < n * n; ++raw) {
+                if ((raw / n) < side && (raw % n) < side) {
+                    continue;
+                }
+                const int q{raw >> 6};
+                const int l{lb + (q / side) * 8 + q % side};
+                const int idx{l * 64 + (raw & 63)};
+                const float xr{__half2float(coef[idx])};
+                const float yr{__half2float(coef[4096 + idx])};
+                const float br{__half2float(coef[8192 + idx])};
+                sxy = jx_fma(xr, yr, sxy);
+                syy = jx_fma(yr, yr, syy);
+                sby = jx_fma(br - yr, yr, sby);
+            }
+        }
+        sm.cfl[0][lb] = sxy;
+        sm.cfl[1][lb] = syy;
+        sm.cfl[2][lb] = sby;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const float sxy{warp_tree(sm.cfl[0][lane] + sm.cfl[0][lane + 32])};
+        const float syy{warp_tree(sm.cfl[1][lane] + sm.cfl[1][lane + 32])};
+        const float sby{warp_tree(sm.cfl[2][lane] + sm.cfl[2][lane + 32])};
+        if (lane == 0) {
+            const double dxy{sxy};
+            const double dyy{syy};
+            const double dby{sby};
+            const float fx{dyy > 0.0 ? static_cast<float>(dxy / dyy) : 0.0f};
+            const float fb{dyy > 0.0 ? static_cast<float>(dby / dyy) : 0.0f};
+            int mx{static_cast<int>(lrintf(fx * static_cast<float>(kCflColorFactor)))};
+            int mb{static_cast<int>(lrintf(fb * static_cast<float>(kCflColorFactor)))};
+            mx = mx < -128 ? -128 : (mx > 127 ? 127 : mx);
+            mb = mb < -128 ? -128 : (mb > 127 ? 127 : mb);
+            sm.mx = mx;
+            sm.mb = mb;
+            const int tile{ty * static_cast<int>(gridDim.x) + tx};
+            out.ytox[tile] = static_cast<std::int8_t>(mx);
+            out.ytob[tile] = static_cast<std::int8_t>(mb);
+        }
+    }
+    __syncthreads();
+
+    // ---- 7. quantisation (src/frontend_quantize.cu:125-201).
+    const float ytox{static_cast<float>(sm.mx) * kCflColorScale};
+    const float ytob{jx_fma(static_cast<float>(sm.mb), kCflColorScale, kCflBaseB)};
+    const std::size_t cplane{static_cast<std::size_t>(nblocks) * 64};
+    for (int k{tid}; k < 4096; k += kThreads) {
+        const int lb{k >> 6};
+        const int slot{k & 63};
+        const int lbx{lb & 7};
+        const int lby{lb >> 3};
+        if (bx0 + lbx >= bw || by0 + lby >= bh) {
+            continue;
+        }
+        const int f{sm.owner[lb]};
+        const int n{sm.acs[f]};
+        const int side{n >> 3};
+        const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
+        const int raw{q * 64 + slot};
+        const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
+        std::int16_t ax{0};
+        std::int16_t ay{0};
+        std::int16_t ab{0};
+        if (!((raw / n) < side && (raw % n) < side)) {
+            const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
+            const float* wt{tb.dequant + si * 3072};
+            const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
+            const float xr{__half2float(coef[k])};
+            const float yr{__half2float(coef[4096 + k])};
+            const float br{__half2float(coef[8192 + k])};
+            const float wy{wt[1024 + raw]};
+            const int qy{static_cast<int>(lrintf((yr * qgsf) / wy))};
+            const float yq{(static_cast<float>(qy) * wy) / qgsf};
+            const float wx{wt[raw]};
+            const int qx{static_cast<int>(lrintf((jx_fma(-ytox, yq, xr) * qgsf) / wx))};
+            const float wb{wt[2048 + raw]};
+            const int qb{static_cast<int>(lrintf((jx_fma(-ytob, yq, br) * qgsf) / wb))};
+            ax = static_cast<std::int16_t>(qx);
+            ay = static_cast<std::int16_t>(qy);
+            ab = static_cast<std::int16_t>(qb);
+            if (ax != 0) atomicAdd(&sm.nz[0][f], 1);
+            if (ay != 0) atomicAdd(&sm.nz[1][f], 1);
+            if (ab != 0) atomicAdd(&sm.nz[2][f], 1);
+        }
+        out.ac[g] = ax;
+        out.ac[cplane + g] = ay;
+        out.ac[2 * cplane + g] = ab;
+    }
+    // DC from the low-frequency corner (src/frontend_quantize.cu:180-200,
+    // src/vardct_layout.h:88-111).
+    if (tid < 64) {
+        const int lb{tid};
+        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
+            const int n{sm.acs[lb]};
+            const int m{n >> 3};
+            const float dcq_x{kDcInvQuant[0] * sc.dc_scale};
+            const float dcq_y{kDcInvQuant[1] * sc.dc_scale};
+            const float dcq_b{kDcInvQuant[2] * sc.dc_scale};
+            float llf[3][16];
+            for (int c{0}; c < 3; ++c) {
+                for (int fx{0}; fx < m; ++fx) {
+                    for (int fy{0}; fy < m; ++fy) {
+                        const int raw{fx * n + fy};
+                        const int q{raw >> 6};
+                        llf[c][fx * m + fy] =
+                            __half2float(coef[c * 4096 + (lb + (q / m) * 8 + q % m) * 64 + (raw & 63)]);
+                    }
+                }
+            }
+            float dcv[3][16];
+            if (m == 1) {
+                for (int c{0}; c < 3; ++c) {
+                    dcv[c][0] = llf[c][0];
+                }
+            } else {
+                const double* ob{tb.llf_basis + (m == 2 ? 0 : 16)};
+                const double s16[2]{1.0, 0.901764195028874394};
+                const double s32[4]{1.0, 0.974886821136879522, 0.901764195028874394,
+                                    0.787054918159101335};
+                const double* scl{m == 2 ? s16 : s32};
+                for (int c{0}; c < 3; ++c) {
+                    for (int oy{0}; oy < m; ++oy) {
+                        for (int ox{0}; ox < m; ++ox) {
+                            double sum{0.0};
+                            for (int fx{0}; fx < m; ++fx) {
+                                for (int fy{0}; fy < m; ++fy) {
+                                    const double cv{llf[c][fx * m + fy]};
+                                    sum = sum + ob[fx * 4 + ox] * ob[fy * 4 + oy] * cv * scl[fx] * scl[fy];
+                                }
+                            }
+                            dcv[c][oy * m + ox] = static_cast<float>(static_cast<double>(m) * sum);
+                        }
+                    }
+                }
+            }
+            for (int oy{0}; oy < m; ++oy) {
+                for (int ox{0}; ox < m; ++ox) {
+                    const int p{oy * m + ox};
+                    const std::size_t blk{static_cast<std::size_t>(by0 + (lb >> 3) + oy) * bw + bx0 +
+                                          (lb & 7) + ox};
+                    const int qdy{static_cast<int>(lrintf(dcv[1][p] * dcq_y))};
+                    const float ydr{static_cast<float>(qdy) / dcq_y};
+                    out.dc[nblocks + blk] = qdy;
+                    out.dc[blk] = static_cast<int>(lrintf(dcv[0][p] * dcq_x));
+                    out.dc[2 * static_cast<std::size_t>(nblocks) + blk] =
+                        static_cast<int>(lrintf((dcv[2][p] - ydr) * dcq_b));
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- 8. side information.
+    for (int k{tid}; k < 64; k += kThreads) {
+        const int lb{k};
+        const int gbx{bx0 + (lb & 7)};
+        const int gby{by0 + (lb >> 3)};
+        if (gbx >= bw || gby >= bh) {
+            continue;
+        }
+        const std::size_t blk{static_cast<std::size_t>(gby) * bw + gbx};
+        const int f{sm.owner[lb]};
+        const int n{sm.acs[f]};
+        const int covered{(n >> 3) * (n >> 3)};
+        const int l2{n == 16 ? 2 : (n == 32 ? 4 : 0)};
+        for (int c{0}; c < 3; ++c) {
+            const int nz{sm.nz[c][f]};
+            out.nzn[c * static_cast<std::size_t>(nblocks) + blk] =
+                static_cast<std::uint8_t>((nz + covered - 1) >> l2);
+            out.nzc[c * static_cast<std::size_t>(nblocks) + blk] =
+                static_cast<std::uint16_t>(f == lb ? nz : 0);
+        }
+        out.acs[blk] = sm.acs[lb];
+        out.qf[blk] = sm.qf[lb];
+    }
+}
+
+}  // namespace
+
+FrontendScalars frontend_scalars(float distance, std::uint32_t* global_scale,
+                                 std::uint32_t* quant_dc) {
+    // Quantiser calibration (src/quant_calibration.h:49-88).
+    const float quant_ac{kAcQuant / distance};
+    const float bt_dc{std::max(
+        0.5f * distance,
+        std::min(distance, kDcMul * std::pow((1.0f / kDcMul) * distance, kDcQuantPow)))};
+    const float quant_dc_float{std::min(kDcQuant / bt_dc, 50.0f)};
+    float scale{static_cast<float>(kGlobalScaleDenom) * quant_ac / kQuantFieldTarget};
+    scale = scale < 1.0f ? 1.0f : scale;
+    scale = scale > static_cast<float>(1 << 15) ? static_cast<float>(1 << 15) : scale;
+    int gs{static_cast<int>(scale)};
+    const int scaled_quant_dc{static_cast<int>(quant_dc_float * kGlobalScaleNumerator * 1.6f)};
+    if (gs > scaled_quant_dc) {
+        gs = scaled_quant_dc <= 0 ? 1 : scaled_quant_dc;
+    }
+    const float inv_gs{1.0f * static_cast<float>(kGlobalScaleDenom) / static_cast<float>(gs)};
+    float fval{quant_dc_float * inv_gs + 0.5f};
+    fval = std::min<float>(static_cast<float>(1 << 16), fval);
+    const int qdc{static_cast<int>(fval)};
+    int raw_q{static_cast<int>(std::lround(quant_ac * inv_gs))};
+    raw_q = std::max(1, std::min(kQuantMax, raw_q));
+    const float gsf{static_cast<float>(gs) * (1.0f / kGlobalScaleDenom)};
+
+    FrontendScalars s{};
+    // AQ mapping and FuzzyErosion weights (src/frontend_fused.cu:349-380).
+    const float ascale{kAcQuant / distance};
+    const float base_level{0.48f * ascale};
+    float dampen{1.0f};
+    if (distance >= 2.0f) {
+        dampen = 1.0f - (distance - 2.0f) / (14.0f - 2.0f);
+        if (dampen < 0.0f) {
+            dampen = 0.0f;
+        }
+    }
+    s.mul_pb = ascale * dampen;
+    s.add_pb = (1.0f - dampen) * base_level;
+    const float efm{distance < 2.0f ? (2.0f - distance) * 0.5f : 0.0f};
+    float km0{0.125f};
+    float km1{0.10f - efm * 0.10f};
+    float km2{0.09f - efm * 0.09f};
+    float km3{0.06f - efm * 0.06f};
+    const float norm{0.29959705784054957f / (km0 + km1 + km2 + km3)};
+    s.km0 = km0 * norm;
+    s.km1 = km1 * norm;
+    s.km2 = km2 * norm;
+    s.km3 = km3 * norm;
+    s.inv_global_scale = inv_gs;
+    s.mask_sqrt_mul = std::sqrt(kMaskMul);
+    s.qgsf_select = static_cast<float>(raw_q) * gsf;
+    s.gsf = gsf;
+    s.dc_scale = gsf * static_cast<float>(qdc);
+    if (global_scale != nullptr) *global_scale = static_cast<std::uint32_t>(gs);
+    if (quant_dc != nullptr) *quant_dc = static_cast<std::uint32_t>(qdc);
+    return s;
+}
+
+bool frontend_tables_init(FrontendTables* tables) {
+    // Bases.
+    for (int n : {8, 16, 32}) {
+        std::vector<float> sel(static_cast<std::size_t>(n) * n);
+        std::vector<float> dct(static_cast<std::size_t>(n) * n);
+        for (int k{0}; k < n; ++k) {
+            const double g{k == 0 ? 1.0 / n : 1.4142135623730950488 / n};
+            const float gf{k == 0 ? 1.0f / n : 1.4142135623730951f / n};
+            for (int t{0}; t < n; ++t) {
+                sel[k * n + t] =
+                    static_cast<float>(g * std::cos(3.14159265358979323846 * (t + 0.5) * k / n));
+                const float arg{3.14159265358979323846f * (t + 0.5f) * k / n};
+                dct[k * n + t] = gf * std::cos(arg);
+            }
+        }
+        const void* sel_sym{n == 8 ? static_cast<const void*>(&c_sel8)
+                                   : (n == 16 ? static_cast<const void*>(&c_sel16)
+                                              : static_cast<const void*>(&c_sel32))};
+        const void* dct_sym{n == 8 ? static_cast<const void*>(&c_dct8)
+                                   : (n == 16 ? static_cast<const void*>(&c_dct16)
+                                              : static_cast<const void*>(&c_dct32))};
+        if (cudaMemcpyToSymbol(sel_sym, sel.data(), sel.size() * sizeof(float)) != cudaSuccess ||
+            cudaMemcpyToSymbol(dct_sym, dct.data(), dct.size() * sizeof(float)) != cudaSuccess) {
+            return false;
+        }
+    }
+    // Dequantisation weights [size][channel][1024].
+    std::vector<float> deq(3 * 3 * 1024, 0.0f);
+    for (int c{0}; c < 3; ++c) {
+        for (int i{0}; i < 64; ++i) std::memcpy(&deq[(0 * 3 + c) * 1024 + i], &kDequantBits8[c][i], 4);
+        for (int i{0}; i < 256; ++i) std::memcpy(&deq[(1 * 3 + c) * 1024 + i], &kDequantBits16[c][i], 4);
+        for (int i{0}; i < 1024; ++i) std::memcpy(&deq[(2 * 3 + c) * 1024 + i], &kDequantBits32[c][i], 4);
+    }
+    // Selection weights: DCT8 Y weight at (round(fx*8/N), round(fy*8/N)) clamped to 7.
+    std::vector<float> sw(3 * 1024, 0.0f);
+    for (int si{0}; si < 3; ++si) {
+        const int n{8 << si};
+        for (int fx{0}; fx < n; ++fx) {
+            for (int fy{0}; fy < n; ++fy) {
+                int sx{static_cast<int>(std::lround(fx * 8.0 / n))};
+                int sy{static_cast<int>(std::lround(fy * 8.0 / n))};
+                sx = sx > 7 ? 7 : sx;
+                sy = sy > 7 ? 7 : sy;
+                sw[si * 1024 + fx * n + fy] = deq[(0 * 3 + 1) * 1024 + sx * 8 + sy];
+            }
+        }
+    }
+    // log2f(1 + i) with the host libm: the rate proxy of the selection host twin.
+    std::vector<float> l2(kLog2TableSize);
+    for (int i{0}; i < kLog2TableSize; ++i) {
+        l2[i] = std::log2(1.0f + static_cast<float>(i));
+    }
+    // Orthonormal m-point DCT basis for the LLF -> DC resampling, m = 2 and 4:
+    // [m][k][n] stride 4 (src/vardct_layout.h:75-79).
+    std::vector<double> ob(32, 0.0);
+    for (int mi{0}; mi < 2; ++mi) {
+        const int m{mi == 0 ? 2 : 4};
+        const double md{static_cast<double>(m)};
+        for (int k{0}; k < m; ++k) {
+            for (int nn{0}; nn < m; ++nn) {
+                const double normv{k == 0 ? std::sqrt(1.0 / md) : std::sqrt(2.0 / md)};
+                ob[mi * 16 + k * 4 + nn] =
+                    normv * std::cos(3.14159265358979323846 * (static_cast<double>(nn) + 0.5) *
+                                     static_cast<double>(k) / md);
+            }
+        }
+    }
+    float* d_deq{nullptr};
+    float* d_sw{nullptr};
+    float* d_l2{nullptr};
+    double* d_ob{nullptr};
+    if (cudaMalloc(&d_deq, deq.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_sw, sw.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_l2, l2.size() * 4) != cudaSuccess ||
+        cudaMalloc(&d_ob, ob.size() * 8) != cudaSuccess) {
+        return false;
+    }
+    if (cudaMemcpy(d_deq, deq.data(), deq.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_sw, sw.data(), sw.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_l2, l2.data(), l2.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_ob, ob.data(), ob.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        return false;
+    }
+    tables->dequant = d_deq;
+    tables->sel_weight = d_sw;
+    tables->log2_1p = d_l2;
+    tables->llf_basis = d_ob;
+    return cudaFuncSetAttribute(frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kSmemBytes)) == cudaSuccess;
+}
+
+bool frontend_launch(const FrontendInputs& in, const FrontendScalars& s, const FrontendTables& t,
+                     const FrontendOutputs& out, void* stream) {
+    const dim3 grid{static_cast<unsigned>((in.width + kTile - 1) / kTile),
+                    static_cast<unsigned>((in.height + kTile - 1) / kTile)};
+    frontend_kernel<<<grid, kThreads, kSmemBytes, static_cast<cudaStream_t>(stream)>>>(in, s, t, out);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+}  // namespace jxb
