@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""4K NV12 -> JPEG XL VarDCT encode throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the seeded synthetic 3840x2160 NV12 frame (seed 0), distance 1.0,
+the plain path (XYB, AQ, gaborish, transform selection, DCT, CfL, quantise,
+histograms, prefix codes, packing, headers). One step encodes a batch of 16
+device-resident copies of that frame back to back on the encoder's stream;
+the 16 distinct input buffers (199 MB) exceed the 126 MB L2, so no step reads
+its input from L2.
+
+value: frames/s over exactly K steps, CUDA events on the encoder's stream,
+barrier + synchronize on both sides, max over ranks (one process per GPU,
+independent replicas: frames do not shard, so there is no collective).
+e2e: the same metric through the public C ABI with host buffers: every frame
+is copied host->device from pinned memory, encoded with
+cujpegxl_encoder_encode and its file copied back to pinned host memory.
+roofline: the fused frontend kernel, its algorithmic bytes per 4K frame over
+its event-timed duration inside the timed region, against the measured HBM
+copy bandwidth.
+--impl reference: the CPU encoder restated from the reference (the reference
+has no CPU implementation of its device stages) run with every host core on
+the same frame, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+W_4K, H_4K = 3840, 2160
+BATCH = 16
+PUBLISHED_FPS = 15.0  # reference README.md:17, GTX 1080 Ti, 4K sustained
+
+
+def frontend_algorithmic_bytes(w: int, h: int) -> int:
+    """NV12 in; int16 AC, int32 DC, acs, int32 quant field, CfL maps out."""
+    p = w * h
+    b = p // 64
+    t = ((w // 8 + 7) // 8) * ((h // 8 + 7) // 8)
+    return int(1.5 * p) + 6 * p + 12 * b + 5 * b + 2 * t
+
+
+def measured_peak() -> tuple[float, str]:
+    f = REPO / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per frontend launch at 4K from the committed ncu summary."""
+    f = REPO / "profiles" / "frontend_kernel_4k.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch_4k:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"bench_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        time.sleep(0.1)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self) -> dict:
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        try:
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+                for n, v in zip(names, parts[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            self.path.unlink()
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(nv12, w, h, d, runs: int) -> dict:
+    from oracle import api
+
+    threads = os.cpu_count() or 1
+    api.encode(nv12, w, h, d, threads)  # warm tables
+    t0 = time.perf_counter()
+    for _ in range(runs):
+        api.encode(nv12, w, h, d, threads)
+    dt = time.perf_counter() - t0
+    return {"value": runs / dt, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{runs} full {w}x{h} frames (seed 0, d={d}) through the CPU restatement, "
+                      f"{threads} threads"}
+
+
+def run_reference(args) -> None:
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    from cujpegxl_b200.synth import make_nv12
+    from oracle import api
+
+    nv12 = make_nv12(args.width, args.height, 0)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        api.encode(nv12, args.width, args.height, args.distance, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        api.encode(nv12, args.width, args.height, args.distance, threads)
+        times.append(time.perf_counter() - t0)
+    value = args.steps / sum(times)
+    line = {
+        "impl": "reference", "metric": "4K frames/s", "value": value, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_FPS, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.width}x{args.height} NV12 seed 0, d={args.distance}, plain VarDCT path",
+                   "step": "one frame"},
+        "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"one full {args.width}x{args.height} frame per step, {threads} threads"},
+        "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from cujpegxl_b200 import Encoder, _capi
+    from cujpegxl_b200.synth import make_nv12
+
+    W, H, d = args.width, args.height, args.distance
+    nv12 = make_nv12(W, H, 0)
+    luma_h = torch.from_numpy(nv12[: W * H].reshape(H, W).copy())
+    chroma_h = torch.from_numpy(nv12[W * H:].reshape(H // 2, W).copy())
+    frames = [(luma_h.cuda(), chroma_h.cuda()) for _ in range(BATCH)]
+    torch.cuda.synchronize()
+
+    enc = Encoder(W, H, d, local)
+    stream = torch.cuda.ExternalStream(enc.stream())
+    kernels = int(_capi.lib().cujpegxl_b200_kernels_per_encode())
+
+    def enqueue_batch(ev_front=None, ev_mid=None, k=0):
+        for i, (lm, ch) in enumerate(frames):
+            if ev_front is not None:
+                ev_front[k * BATCH + i].record(stream)
+            enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 1)
+            if ev_mid is not None:
+                ev_mid[k * BATCH + i].record(stream)
+            enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 2)
+
+    for _ in range(args.warmup):
+        enqueue_batch()
+    size, _ = enc.result()
+
+    n = args.steps * BATCH
+    ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+    ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+
+    with ClockSampler(local) as clocks:
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        for k in range(args.steps):
+            enqueue_batch(ev_a, ev_b, k)
+        stop.record(stream)
+        enc.result()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+    total_ms = start.elapsed_time(stop)
+    front = [ev_a[i].elapsed_time(ev_b[i]) for i in range(n)]
+    frame_ms = [ev_a[i].elapsed_time(ev_a[i + 1]) for i in range(n - 1)] + [ev_a[n - 1].elapsed_time(stop)]
+    if pg:
+        t = torch.tensor([total_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n / (total_ms / 1000.0)
+
+    # End to end through the C ABI with host buffers.
+    pinned_l = luma_h.pin_memory()
+    pinned_c = chroma_h.pin_memory()
+    out_cap = 64 << 20
+    out_h = torch.empty(out_cap, dtype=torch.uint8).pin_memory()
+    dl, dc = frames[0]
+    e2e_n = max(args.steps, 4)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            dl.copy_(pinned_l, non_blocking=True)
+            dc.copy_(pinned_c, non_blocking=True)
+            enc.encode_device_into(dl.data_ptr(), dc.data_ptr(), W, W, out_h.data_ptr(), out_cap)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        d2h = 0
+        for _ in range(e2e_n):
+            dl.copy_(pinned_l, non_blocking=True)
+            dc.copy_(pinned_c, non_blocking=True)
+            d2h = enc.encode_device_into(dl.data_ptr(), dc.data_ptr(), W, W, out_h.data_ptr(), out_cap)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * e2e_n / (e2e_ms / 1000.0)
+
+    front_ms = statistics.mean(front)
+    alg = frontend_algorithmic_bytes(W, H)
+    achieved = alg / (front_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+    sorted_ms = sorted(frame_ms)
+    p50 = sorted_ms[len(sorted_ms) // 2]
+    p99 = sorted_ms[min(len(sorted_ms) - 1, int(round(0.99 * (len(sorted_ms) - 1))))]
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(nv12, W, H, d, args.cpu_runs)
+        line = {
+            "metric": "4K frames/s", "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": value / PUBLISHED_FPS, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{W}x{H} NV12 seed 0, d={d}, plain VarDCT path",
+                       "step": f"{BATCH} device-resident frames", "width": W, "height": H, "distance": d,
+                       "l2": f"{BATCH} distinct input buffers ({BATCH * W * H * 3 // 2 / 1e6:.0f} MB > 126 MB L2)",
+                       "parallelism": f"{world} independent replica(s)"},
+            "mp_per_s": value * W * H / 1e6,
+            "bytes_per_frame": size, "bpp": 8.0 * size / (W * H),
+            "p50_frame_ms": p50, "p99_frame_ms": p99,
+            "frontend_ms": front_ms, "entropy_ms": statistics.mean(frame_ms) - front_ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(),
+                         "kernel": "frontend_kernel", "algorithmic_bytes": alg, "peak_kind": peak_kind},
+            "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": W * H * 3 // 2,
+                    "d2h_bytes_per_step": d2h + 32, "step": "one frame"},
+            "gpu_launches": kernels * n,
+            "clocks": clocks.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    # Torch's allocators record events on the streams their blocks were used
+    # on when they are freed, so release every torch object that touched the
+    # encoder's stream before the encoder destroys that stream.
+    torch.cuda.synchronize()
+    del frames, dl, dc, pinned_l, pinned_c, out_h, ev_a, ev_b, start, stop, e0, e1, stream
+    import gc
+
+    gc.collect()
+    torch.cuda.synchronize()
+    enc.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--width", type=int, default=W_4K)
+    ap.add_argument("--height", type=int, default=H_4K)
+    ap.add_argument("--distance", type=float, default=1.0)
+    ap.add_argument("--cpu-runs", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

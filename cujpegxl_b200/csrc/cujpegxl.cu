@@ -1,0 +1,654 @@
+// The C ABI of libcujpegxl.so.1: the reference's nine entry points
+// (include/cujpegxl/cujpegxl.h:66-82 in m-pilia/cujpegxl, implemented there in
+// src/cujpegxl.cc) plus the additional entry points of
+// include/cujpegxl_b200/cujpegxl_b200.h, over a per-encoder CUDA stream and
+// device arena allocated once per geometry.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "cujpegxl/cujpegxl.h"
+#include "cujpegxl_b200/cujpegxl_b200.h"
+#include "entropy.cuh"
+#include "frontend.cuh"
+#include "jxl_constants.cuh"
+
+namespace jxb {
+bool entropy_kernels_init();
+}
+
+struct cujpegxl_encoder {
+    cujpegxl_config config{};
+    int device{0};
+    cudaStream_t stream{nullptr};
+    void* arena{nullptr};
+    std::uint32_t geo_w{0};
+    std::uint32_t geo_h{0};
+    float geo_distance{-1.0f};
+    bool debug{false};
+    jxb::FrontendOutputs fo{};
+    jxb::EntropyDev ed{};
+    jxb::FrontendScalars fs{};
+    std::uint32_t global_scale{0};
+    std::uint32_t quant_dc{0};
+    std::uint8_t* dc_global_dev{nullptr};
+    float* dbg_xyb{nullptr};
+    float* dbg_sharp{nullptr};
+    std::uint16_t* dbg_coeff{nullptr};
+    std::uint8_t* nv12_dev{nullptr};
+    std::uint8_t* nv12_pinned{nullptr};
+    unsigned long long* result_pinned{nullptr};
+    bool pending{false};
+};
+
+namespace {
+
+struct DeviceTables {
+    bool ready{false};
+    jxb::FrontendTables ft{};
+};
+
+std::mutex g_mutex;
+DeviceTables g_tables[64];
+
+// Restores the caller's current device on scope exit.
+class DeviceScope {
+public:
+    explicit DeviceScope(int device) {
+        ok_ = cudaGetDevice(&prev_) == cudaSuccess && cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceScope() { cudaSetDevice(prev_); }
+    bool ok() const { return ok_; }
+
+private:
+    int prev_{0};
+    bool ok_{false};
+};
+
+bool device_tables(int device, jxb::FrontendTables* out) {
+    if (device < 0 || device >= 64) return false;
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceTables& t{g_tables[device]};
+    if (!t.ready) {
+        if (!jxb::frontend_tables_init(&t.ft) || !jxb::entropy_kernels_init()) return false;
+        t.ready = true;
+    }
+    *out = t.ft;
+    return true;
+}
+
+bool device_exists(std::int32_t ordinal, int* major, int* minor) {
+    int count{0};
+    if (cudaGetDeviceCount(&count) != cudaSuccess || ordinal < 0 || ordinal >= count) return false;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, ordinal) != cudaSuccess) return false;
+    *major = prop.major;
+    *minor = prop.minor;
+    return true;
+}
+
+// src/cujpegxl.cc:36-48: distance must be positive and finite; width and
+// height positive multiples of 8 spanning more than one 256x256 AC group.
+cujpegxl_status validate_config(const cujpegxl_config& c) {
+    if (!(c.distance > 0.0f) || !std::isfinite(c.distance)) return CUJPEGXL_INVALID_ARGUMENT;
+    if (c.width == 0 || c.height == 0 || c.width % 8 != 0 || c.height % 8 != 0) {
+        return CUJPEGXL_UNSUPPORTED_RESOLUTION;
+    }
+    const std::size_t nac{((c.width / 8 + 31) / 32) * static_cast<std::size_t>((c.height / 8 + 31) / 32)};
+    if (nac <= 1) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
+    return CUJPEGXL_OK;
+}
+
+std::size_t align256(std::size_t v) { return (v + 255) & ~static_cast<std::size_t>(255); }
+
+// Sub-allocates the encoder's device buffers from one arena.
+struct ArenaPlan {
+    std::size_t total{0};
+    std::size_t take(std::size_t bytes) {
+        const std::size_t at{total};
+        total += align256(bytes);
+        return at;
+    }
+};
+
+void release(cujpegxl_encoder* e) {
+    if (e->arena) cudaFree(e->arena);
+    if (e->nv12_pinned) cudaFreeHost(e->nv12_pinned);
+    e->arena = nullptr;
+    e->nv12_pinned = nullptr;
+    e->geo_w = e->geo_h = 0;
+}
+
+// Allocates every per-geometry buffer (nothing is allocated per frame).
+bool allocate(cujpegxl_encoder* e) {
+    release(e);
+    const std::uint32_t W{e->config.width};
+    const std::uint32_t H{e->config.height};
+    const std::size_t bw{W / 8};
+    const std::size_t bh{H / 8};
+    const std::size_t nb{bw * bh};
+    const std::size_t nt{((bw + 7) / 8) * ((bh + 7) / 8)};
+    const jxb::EntropyHostPlan plan{jxb::entropy_plan(static_cast<int>(W), static_cast<int>(H))};
+    const int ndc{static_cast<int>(((bw + 255) / 256) * ((bh + 255) / 256))};
+    const int nac{static_cast<int>(((bw + 31) / 32) * ((bh + 31) / 32))};
+    const std::uint32_t tiles{(plan.total_items + jxb::kScanTile - 1) / jxb::kScanTile};
+    const std::size_t out_cap{(jxb::worst_case_output(W, H) + 15) & ~static_cast<std::size_t>(15)};
+
+    ArenaPlan a;
+    const std::size_t o_ac{a.take(3 * nb * 64 * 2)};
+    const std::size_t o_dc{a.take(3 * nb * 4)};
+    const std::size_t o_acs{a.take(nb)};
+    const std::size_t o_qf{a.take(nb * 4)};
+    const std::size_t o_tx{a.take(nt)};
+    const std::size_t o_tb{a.take(nt)};
+    const std::size_t o_nzn{a.take(3 * nb)};
+    const std::size_t o_nzc{a.take(3 * nb * 2)};
+    const std::size_t o_sec{a.take(plan.sections.size() * sizeof(jxb::Section))};
+    const std::size_t o_ord{a.take(plan.order.size() * 2)};
+    const std::size_t o_pre{a.take(plan.pre_const.size())};
+    const std::size_t o_mid{a.take(plan.mid_const.size())};
+    const std::size_t o_acp{a.take(plan.ac_prefix.size())};
+    const std::size_t o_dcg{a.take(64)};
+    const std::size_t o_ach{a.take(32 * 256 * 4)};
+    const std::size_t o_dch{a.take(static_cast<std::size_t>(ndc) * 256 * 4)};
+    const std::size_t o_amh{a.take(static_cast<std::size_t>(ndc) * 256 * 4)};
+    const std::size_t o_fb{a.take(static_cast<std::size_t>(ndc) * 4)};
+    const std::size_t o_acd{a.take(32 * 256)};
+    const std::size_t o_acb{a.take(32 * 256 * 2)};
+    const std::size_t o_dcd{a.take(static_cast<std::size_t>(ndc) * 256)};
+    const std::size_t o_dcb{a.take(static_cast<std::size_t>(ndc) * 256 * 2)};
+    const std::size_t o_amd{a.take(static_cast<std::size_t>(ndc) * 256)};
+    const std::size_t o_amb{a.take(static_cast<std::size_t>(ndc) * 256 * 2)};
+    const std::size_t o_alpha{a.take(32 * 4)};
+    const std::size_t o_desc{a.take(static_cast<std::size_t>(32 + 2 * ndc) * jxb::kDescBytes)};
+    const std::size_t o_descb{a.take(static_cast<std::size_t>(32 + 2 * ndc) * 4)};
+    const std::size_t o_ib{a.take(static_cast<std::size_t>(plan.total_items) * 4)};
+    const std::size_t o_ip{a.take(static_cast<std::size_t>(plan.total_items) * 4)};
+    const std::size_t o_ts{a.take(static_cast<std::size_t>(tiles) * 4)};
+    const std::size_t o_to{a.take(static_cast<std::size_t>(tiles + 1) * 8)};
+    const std::size_t o_sp{a.take(plan.sections.size() * 8)};
+    const std::size_t o_res{a.take(4 * 8)};
+    const std::size_t o_out{a.take(out_cap)};
+    const std::size_t o_nv12{a.take(static_cast<std::size_t>(W) * H * 3 / 2)};
+    std::size_t o_dbg{0};
+    if (e->debug) {
+        o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2);
+    }
+    void* base{nullptr};
+    if (cudaMalloc(&base, a.total) != cudaSuccess) return false;
+    e->arena = base;
+    auto* b{static_cast<std::uint8_t*>(base)};
+
+    jxb::FrontendOutputs& fo{e->fo};
+    fo.ac = reinterpret_cast<std::int16_t*>(b + o_ac);
+    fo.dc = reinterpret_cast<std::int32_t*>(b + o_dc);
+    fo.acs = reinterpret_cast<std::int8_t*>(b + o_acs);
+    fo.qf = reinterpret_cast<std::int32_t*>(b + o_qf);
+    fo.ytox = reinterpret_cast<std::int8_t*>(b + o_tx);
+    fo.ytob = reinterpret_cast<std::int8_t*>(b + o_tb);
+    fo.nzn = b + o_nzn;
+    fo.nzc = reinterpret_cast<std::uint16_t*>(b + o_nzc);
+    e->dbg_xyb = e->debug ? reinterpret_cast<float*>(b + o_dbg) : nullptr;
+    e->dbg_sharp = e->debug ? e->dbg_xyb + 3 * static_cast<std::size_t>(W) * H : nullptr;
+    e->dbg_coeff = e->debug ? reinterpret_cast<std::uint16_t*>(e->dbg_sharp + 3 * static_cast<std::size_t>(W) * H)
+                            : nullptr;
+    fo.dbg_xyb = e->dbg_xyb;
+    fo.dbg_sharp = e->dbg_sharp;
+    fo.dbg_coeff = e->dbg_coeff;
+
+    jxb::EntropyDev& ed{e->ed};
+    ed = jxb::EntropyDev{};
+    ed.width = static_cast<int>(W);
+    ed.height = static_cast<int>(H);
+    ed.bw = static_cast<int>(bw);
+    ed.bh = static_cast<int>(bh);
+    ed.nblocks = static_cast<int>(nb);
+    ed.xg = static_cast<int>((bw + 31) / 32);
+    ed.nac = nac;
+    ed.xdg = static_cast<int>((bw + 255) / 256);
+    ed.ndc = ndc;
+    ed.cmw = static_cast<int>((bw + 7) / 8);
+    ed.nsec = static_cast<int>(plan.sections.size());
+    ed.total_items = plan.total_items;
+    ed.num_tiles = tiles;
+    ed.sections = reinterpret_cast<const jxb::Section*>(b + o_sec);
+    ed.ac = fo.ac;
+    ed.dc = fo.dc;
+    ed.acs = fo.acs;
+    ed.qf = fo.qf;
+    ed.ytox = fo.ytox;
+    ed.ytob = fo.ytob;
+    ed.nzn = fo.nzn;
+    ed.nzc = fo.nzc;
+    ed.order = reinterpret_cast<const std::uint16_t*>(b + o_ord);
+    ed.pre_const = b + o_pre;
+    ed.pre_const_bits = plan.pre_const_bits;
+    ed.mid_const = b + o_mid;
+    ed.mid_const_bits = plan.mid_const_bits;
+    ed.ac_prefix = b + o_acp;
+    ed.ac_prefix_bits = plan.ac_prefix_bits;
+    e->dc_global_dev = b + o_dcg;
+    ed.dc_global = e->dc_global_dev;
+    ed.ac_hist = reinterpret_cast<std::uint32_t*>(b + o_ach);
+    ed.dc_hist = reinterpret_cast<std::uint32_t*>(b + o_dch);
+    ed.am_hist = reinterpret_cast<std::uint32_t*>(b + o_amh);
+    ed.fb_count = reinterpret_cast<std::uint32_t*>(b + o_fb);
+    ed.ac_depth = b + o_acd;
+    ed.ac_bits = reinterpret_cast<std::uint16_t*>(b + o_acb);
+    ed.dc_depth = b + o_dcd;
+    ed.dc_bits = reinterpret_cast<std::uint16_t*>(b + o_dcb);
+    ed.am_depth = b + o_amd;
+    ed.am_bits = reinterpret_cast<std::uint16_t*>(b + o_amb);
+    ed.ac_alpha = reinterpret_cast<std::uint32_t*>(b + o_alpha);
+    ed.desc = b + o_desc;
+    ed.desc_bits = reinterpret_cast<std::uint32_t*>(b + o_descb);
+    ed.item_bits = reinterpret_cast<std::uint32_t*>(b + o_ib);
+    ed.item_pre = reinterpret_cast<std::uint32_t*>(b + o_ip);
+    ed.tile_sum = reinterpret_cast<std::uint32_t*>(b + o_ts);
+    ed.tile_off = reinterpret_cast<unsigned long long*>(b + o_to);
+    ed.sec_pos = reinterpret_cast<unsigned long long*>(b + o_sp);
+    ed.result = reinterpret_cast<unsigned long long*>(b + o_res);
+    ed.out = b + o_out;
+    ed.out_capacity = out_cap;
+    e->nv12_dev = b + o_nv12;
+
+    bool ok{cudaMemcpy(b + o_sec, plan.sections.data(), plan.sections.size() * sizeof(jxb::Section),
+                       cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(b + o_ord, plan.order.data(), plan.order.size() * 2, cudaMemcpyHostToDevice) ==
+                cudaSuccess &&
+            cudaMemcpy(b + o_pre, plan.pre_const.data(), plan.pre_const.size(), cudaMemcpyHostToDevice) ==
+                cudaSuccess &&
+            cudaMemcpy(b + o_mid, plan.mid_const.data(), plan.mid_const.size(), cudaMemcpyHostToDevice) ==
+                cudaSuccess &&
+            cudaMemcpy(b + o_acp, plan.ac_prefix.data(), plan.ac_prefix.size(), cudaMemcpyHostToDevice) ==
+                cudaSuccess};
+    ok = ok && cudaHostAlloc(reinterpret_cast<void**>(&e->nv12_pinned),
+                             static_cast<std::size_t>(W) * H * 3 / 2 + 64, cudaHostAllocDefault) == cudaSuccess;
+    if (!ok) {
+        release(e);
+        return false;
+    }
+    e->result_pinned = reinterpret_cast<unsigned long long*>(e->nv12_pinned + static_cast<std::size_t>(W) * H * 3 / 2);
+    e->geo_w = W;
+    e->geo_h = H;
+    e->geo_distance = -1.0f;
+    return true;
+}
+
+// Per-distance state: quantiser scalars and the DcGlobal section.
+bool set_distance(cujpegxl_encoder* e) {
+    if (e->geo_distance == e->config.distance) return true;
+    e->fs = jxb::frontend_scalars(e->config.distance, &e->global_scale, &e->quant_dc);
+    std::uint32_t nbits{0};
+    const std::vector<std::uint8_t> dcg{jxb::dc_global_bits(e->global_scale, e->quant_dc, &nbits)};
+    if (dcg.size() > 64 || cudaMemcpy(e->dc_global_dev, dcg.data(), dcg.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        return false;
+    }
+    e->ed.dc_global_bits = nbits;
+    e->geo_distance = e->config.distance;
+    return true;
+}
+
+bool prepare(cujpegxl_encoder* e) {
+    if (e->geo_w != e->config.width || e->geo_h != e->config.height || e->arena == nullptr) {
+        if (!allocate(e)) return false;
+    }
+    return set_distance(e);
+}
+
+bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp, const std::uint8_t* chroma,
+                   std::size_t cp, std::uint32_t stages = 3u) {
+    jxb::FrontendTables ft{};
+    if (!device_tables(e->device, &ft)) return false;
+    const jxb::FrontendInputs in{luma, chroma, lp, cp, static_cast<int>(e->config.width),
+                                 static_cast<int>(e->config.height)};
+    if ((stages & 1u) && !jxb::frontend_launch(in, e->fs, ft, e->fo, e->stream)) return false;
+    return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, e->stream);
+}
+
+// Waits for the encode and copies the file into `output`.
+cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output) {
+    if (cudaMemcpyAsync(e->result_pinned, e->ed.result, 4 * 8, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    if (e->result_pinned[2] != 0) return CUJPEGXL_INTERNAL_ERROR;
+    const std::size_t total{static_cast<std::size_t>(e->result_pinned[0])};
+    if (total > output->capacity) {
+        output->size = total;
+        return CUJPEGXL_BUFFER_TOO_SMALL;
+    }
+    if (cudaMemcpyAsync(output->data, e->ed.out, total, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    output->size = total;
+    return CUJPEGXL_OK;
+}
+
+// Non-zero counts of uploaded planes (the frontend computes these itself):
+// per first-block and channel the count over its non-LLF coefficients, and
+// its normalised value at every covered position (src/entropy.cu:686-721).
+__global__ void nz_kernel(const std::int16_t* ac, const std::int8_t* acs, int bw, int bh,
+                          std::uint8_t* nzn, std::uint16_t* nzc) {
+    const int blk{static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x)};
+    const int nb{bw * bh};
+    if (blk >= nb) return;
+    const int n{acs[blk]};
+    for (int c{0}; c < 3; ++c) nzc[c * nb + blk] = 0;
+    if (n == 0) return;
+    const int bx{blk % bw};
+    const int by{blk / bw};
+    const int side{n / 8};
+    const int l2{n == 16 ? 2 : (n == 32 ? 4 : 0)};
+    for (int c{0}; c < 3; ++c) {
+        const std::int16_t* p{ac + static_cast<std::size_t>(c) * nb * 64};
+        int cnt{0};
+        for (int raw{0}; raw < n * n; ++raw) {
+            if ((raw / n) < side && (raw % n) < side) continue;
+            if (p[jxb::covered_slot(n, bx, by, bw, raw)] != 0) ++cnt;
+        }
+        const int norm{(cnt + side * side - 1) >> l2};
+        for (int dy{0}; dy < side; ++dy) {
+            for (int dx{0}; dx < side; ++dx) {
+                nzn[c * nb + (by + dy) * bw + bx + dx] = static_cast<std::uint8_t>(norm);
+            }
+        }
+        nzc[c * nb + blk] = static_cast<std::uint16_t>(cnt);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t cujpegxl_api_version(void) { return CUJPEGXL_API_VERSION; }
+
+const char* cujpegxl_status_string(cujpegxl_status status) {
+    switch (status) {
+        case CUJPEGXL_OK: return "ok";
+        case CUJPEGXL_NOT_IMPLEMENTED: return "not-implemented";
+        case CUJPEGXL_INVALID_ARGUMENT: return "invalid-argument";
+        case CUJPEGXL_UNSUPPORTED_RESOLUTION: return "unsupported-resolution";
+        case CUJPEGXL_NO_DEVICE: return "no-device";
+        case CUJPEGXL_INTERNAL_ERROR: return "internal-error";
+        case CUJPEGXL_BUFFER_TOO_SMALL: return "buffer-too-small";
+    }
+    return "internal-error";
+}
+
+const char* cujpegxl_backend_string(cujpegxl_backend backend) {
+    switch (backend) {
+        case CUJPEGXL_BACKEND_FP32_SIMT: return "fp32-simt";
+        case CUJPEGXL_BACKEND_FP16_TENSOR: return "fp16-tensor";
+        case CUJPEGXL_BACKEND_UNKNOWN: return "unknown";
+    }
+    return "unknown";
+}
+
+// Same label rule as the reference (src/capability.h:25-34): compute
+// capability >= 8.0 -> FP16_TENSOR, >= 6.0 -> FP32_SIMT.
+cujpegxl_status cujpegxl_query_backend(int32_t device_ordinal, cujpegxl_backend* out_backend) {
+    if (out_backend == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    int major{0};
+    int minor{0};
+    if (!device_exists(device_ordinal, &major, &minor)) return CUJPEGXL_NO_DEVICE;
+    const int cc{major * 10 + minor};
+    *out_backend = cc >= 80 ? CUJPEGXL_BACKEND_FP16_TENSOR
+                            : (cc >= 60 ? CUJPEGXL_BACKEND_FP32_SIMT : CUJPEGXL_BACKEND_UNKNOWN);
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_max_output_size(const cujpegxl_config* config, size_t* out_bytes) {
+    if (config == nullptr || out_bytes == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    const cujpegxl_status st{validate_config(*config)};
+    if (st != CUJPEGXL_OK) return st;
+    *out_bytes = jxb::worst_case_output(config->width, config->height);
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_encoder_create(const cujpegxl_config* config, cujpegxl_encoder** out_encoder) {
+    if (config == nullptr || out_encoder == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    *out_encoder = nullptr;
+    const cujpegxl_status st{validate_config(*config)};
+    if (st != CUJPEGXL_OK) return st;
+    int major{0};
+    int minor{0};
+    if (!device_exists(config->device_ordinal, &major, &minor)) return CUJPEGXL_NO_DEVICE;
+    auto* e{new (std::nothrow) cujpegxl_encoder{}};
+    if (e == nullptr) return CUJPEGXL_INTERNAL_ERROR;
+    e->config = *config;
+    e->device = config->device_ordinal;
+    DeviceScope scope{e->device};
+    jxb::FrontendTables ft{};
+    if (!scope.ok() || !device_tables(e->device, &ft) ||
+        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess || !prepare(e)) {
+        if (e->stream) cudaStreamDestroy(e->stream);
+        release(e);
+        delete e;
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    *out_encoder = e;
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_encoder_configure(cujpegxl_encoder* encoder, const cujpegxl_config* config) {
+    if (encoder == nullptr || config == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    const cujpegxl_status st{validate_config(*config)};
+    if (st != CUJPEGXL_OK) return st;
+    if (config->device_ordinal != encoder->config.device_ordinal) {
+        int major{0};
+        int minor{0};
+        if (!device_exists(config->device_ordinal, &major, &minor)) return CUJPEGXL_NO_DEVICE;
+        DeviceScope old{encoder->device};
+        cudaStreamSynchronize(encoder->stream);
+        cudaStreamDestroy(encoder->stream);
+        encoder->stream = nullptr;
+        release(encoder);
+        encoder->device = config->device_ordinal;
+        DeviceScope scope{encoder->device};
+        if (cudaStreamCreateWithFlags(&encoder->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            return CUJPEGXL_INTERNAL_ERROR;
+        }
+    }
+    encoder->config = *config;
+    DeviceScope scope{encoder->device};
+    cudaStreamSynchronize(encoder->stream);
+    return prepare(encoder) ? CUJPEGXL_OK : CUJPEGXL_INTERNAL_ERROR;
+}
+
+cujpegxl_status cujpegxl_encoder_encode(cujpegxl_encoder* encoder, const cujpegxl_nv12_input* input,
+                                        cujpegxl_output* output) {
+    if (encoder == nullptr || input == nullptr || output == nullptr || output->data == nullptr ||
+        input->luma == 0 || input->chroma == 0) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    const cujpegxl_status st{validate_config(encoder->config)};
+    if (st != CUJPEGXL_OK) return st;
+    if (input->luma_pitch < encoder->config.width || input->chroma_pitch < encoder->config.width) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    if (!scope.ok() || !prepare(encoder)) return CUJPEGXL_INTERNAL_ERROR;
+    if (!enqueue_frame(encoder, reinterpret_cast<const std::uint8_t*>(input->luma), input->luma_pitch,
+                       reinterpret_cast<const std::uint8_t*>(input->chroma), input->chroma_pitch)) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    return finish(encoder, output);
+}
+
+void cujpegxl_encoder_destroy(cujpegxl_encoder* encoder) {
+    if (encoder == nullptr) return;
+    {
+        DeviceScope scope{encoder->device};
+        if (encoder->stream) {
+            cudaStreamSynchronize(encoder->stream);
+            cudaStreamDestroy(encoder->stream);
+        }
+        release(encoder);
+    }
+    delete encoder;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_set_debug(cujpegxl_encoder* encoder, int32_t enable) {
+    if (encoder == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    const bool want{enable != 0};
+    if (want == encoder->debug) return CUJPEGXL_OK;
+    DeviceScope scope{encoder->device};
+    cudaStreamSynchronize(encoder->stream);
+    encoder->debug = want;
+    release(encoder);
+    return prepare(encoder) ? CUJPEGXL_OK : CUJPEGXL_INTERNAL_ERROR;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_read_planes(cujpegxl_encoder* encoder, const cujpegxl_b200_planes* host) {
+    if (encoder == nullptr || host == nullptr || encoder->arena == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    DeviceScope scope{encoder->device};
+    if (cudaStreamSynchronize(encoder->stream) != cudaSuccess) return CUJPEGXL_INTERNAL_ERROR;
+    const std::size_t W{encoder->config.width};
+    const std::size_t H{encoder->config.height};
+    const std::size_t nb{(W / 8) * (H / 8)};
+    const std::size_t nt{((W / 8 + 7) / 8) * ((H / 8 + 7) / 8)};
+    struct Copy {
+        void* dst;
+        const void* src;
+        std::size_t bytes;
+    };
+    const Copy copies[]{
+        {host->ac, encoder->fo.ac, 3 * nb * 64 * 2},
+        {host->dc, encoder->fo.dc, 3 * nb * 4},
+        {host->acs, encoder->fo.acs, nb},
+        {host->qf, encoder->fo.qf, nb * 4},
+        {host->ytox, encoder->fo.ytox, nt},
+        {host->ytob, encoder->fo.ytob, nt},
+        {host->xyb, encoder->dbg_xyb, 3 * W * H * 4},
+        {host->sharp, encoder->dbg_sharp, 3 * W * H * 4},
+        {host->coeff, encoder->dbg_coeff, 3 * nb * 64 * 2},
+    };
+    for (const Copy& c : copies) {
+        if (c.dst == nullptr) continue;
+        if (c.src == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+        if (cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return CUJPEGXL_INTERNAL_ERROR;
+    }
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encode_planes(cujpegxl_encoder* encoder, const cujpegxl_b200_planes* host,
+                                            uint32_t global_scale, uint32_t quant_dc, cujpegxl_output* output) {
+    if (encoder == nullptr || host == nullptr || output == nullptr || output->data == nullptr ||
+        host->ac == nullptr || host->dc == nullptr || host->acs == nullptr || host->qf == nullptr ||
+        host->ytox == nullptr || host->ytob == nullptr) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    if (!scope.ok() || !prepare(encoder)) return CUJPEGXL_INTERNAL_ERROR;
+    const std::size_t W{encoder->config.width};
+    const std::size_t H{encoder->config.height};
+    const std::size_t nb{(W / 8) * (H / 8)};
+    const std::size_t nt{((W / 8 + 7) / 8) * ((H / 8 + 7) / 8)};
+    std::uint32_t nbits{0};
+    const std::vector<std::uint8_t> dcg{jxb::dc_global_bits(global_scale, quant_dc, &nbits)};
+    cudaStream_t st{encoder->stream};
+    bool ok{cudaMemcpyAsync(encoder->fo.ac, host->ac, 3 * nb * 64 * 2, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->fo.dc, host->dc, 3 * nb * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->fo.acs, host->acs, nb, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->fo.qf, host->qf, nb * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->fo.ytox, host->ytox, nt, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->fo.ytob, host->ytob, nt, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaMemcpyAsync(encoder->dc_global_dev, dcg.data(), dcg.size(), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+            cudaStreamSynchronize(st) == cudaSuccess};
+    if (!ok) return CUJPEGXL_INTERNAL_ERROR;
+    // The DcGlobal blob now belongs to these planes; force a refresh on the next encode.
+    encoder->geo_distance = -1.0f;
+    const std::uint32_t saved_bits{encoder->ed.dc_global_bits};
+    encoder->ed.dc_global_bits = nbits;
+    nz_kernel<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, st>>>(
+        encoder->fo.ac, encoder->fo.acs, static_cast<int>(W / 8), static_cast<int>(H / 8), encoder->fo.nzn,
+        encoder->fo.nzc);
+    ok = cudaGetLastError() == cudaSuccess && jxb::entropy_launch(encoder->ed, st);
+    encoder->ed.dc_global_bits = saved_bits;
+    if (!ok) return CUJPEGXL_INTERNAL_ERROR;
+    return finish(encoder, output);
+}
+
+cujpegxl_status cujpegxl_b200_encode_host(cujpegxl_encoder* encoder, const uint8_t* nv12, size_t nv12_size,
+                                          cujpegxl_output* output) {
+    if (encoder == nullptr || nv12 == nullptr || output == nullptr || output->data == nullptr) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    const std::size_t W{encoder->config.width};
+    const std::size_t H{encoder->config.height};
+    if (nv12_size != W * H * 3 / 2) return CUJPEGXL_INVALID_ARGUMENT;
+    DeviceScope scope{encoder->device};
+    if (!scope.ok() || !prepare(encoder)) return CUJPEGXL_INTERNAL_ERROR;
+    std::memcpy(encoder->nv12_pinned, nv12, nv12_size);
+    if (cudaMemcpyAsync(encoder->nv12_dev, encoder->nv12_pinned, nv12_size, cudaMemcpyHostToDevice,
+                        encoder->stream) != cudaSuccess ||
+        !enqueue_frame(encoder, encoder->nv12_dev, W, encoder->nv12_dev + W * H, W)) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    return finish(encoder, output);
+}
+
+cujpegxl_status cujpegxl_b200_encoder_enqueue(cujpegxl_encoder* encoder, const cujpegxl_nv12_input* input) {
+    if (encoder == nullptr || input == nullptr || input->luma == 0 || input->chroma == 0 ||
+        input->luma_pitch < encoder->config.width || input->chroma_pitch < encoder->config.width) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    if (!scope.ok() || !prepare(encoder)) return CUJPEGXL_INTERNAL_ERROR;
+    if (!enqueue_frame(encoder, reinterpret_cast<const std::uint8_t*>(input->luma), input->luma_pitch,
+                       reinterpret_cast<const std::uint8_t*>(input->chroma), input->chroma_pitch)) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    encoder->pending = true;
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_enqueue_stages(cujpegxl_encoder* encoder,
+                                                     const cujpegxl_nv12_input* input, uint32_t stages) {
+    if (encoder == nullptr || input == nullptr || input->luma == 0 || input->chroma == 0 ||
+        input->luma_pitch < encoder->config.width || input->chroma_pitch < encoder->config.width ||
+        stages == 0 || stages > 3) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    if (!scope.ok() || !prepare(encoder)) return CUJPEGXL_INTERNAL_ERROR;
+    if (!enqueue_frame(encoder, reinterpret_cast<const std::uint8_t*>(input->luma), input->luma_pitch,
+                       reinterpret_cast<const std::uint8_t*>(input->chroma), input->chroma_pitch, stages)) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    encoder->pending = true;
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_result(cujpegxl_encoder* encoder, size_t* out_size,
+                                             uintptr_t* out_device_bytes) {
+    if (encoder == nullptr || out_size == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    DeviceScope scope{encoder->device};
+    if (cudaMemcpyAsync(encoder->result_pinned, encoder->ed.result, 4 * 8, cudaMemcpyDeviceToHost,
+                        encoder->stream) != cudaSuccess ||
+        cudaStreamSynchronize(encoder->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    encoder->pending = false;
+    if (encoder->result_pinned[2] != 0) return CUJPEGXL_INTERNAL_ERROR;
+    *out_size = static_cast<std::size_t>(encoder->result_pinned[0]);
+    if (out_device_bytes != nullptr) *out_device_bytes = reinterpret_cast<uintptr_t>(encoder->ed.out);
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_t* out_stream) {
+    if (encoder == nullptr || out_stream == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    *out_stream = reinterpret_cast<uintptr_t>(encoder->stream);
+    return CUJPEGXL_OK;
+}
+
+uint32_t cujpegxl_b200_kernels_per_encode(void) { return 9u; }
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Device entropy coding and frame assembly: quantised planes -> .jxl bytes in
+// device memory, with no host round trip.
+//
+// The codestream is modelled as a list of sections (DcGlobal, the DcGroups,
+// AcGlobal, the AcGroups, in TOC order), each a list of "items" whose bit
+// lengths are data dependent but whose number is fixed by the frame geometry:
+// a header blob, one AC block-channel, one DC sample, one AcMetadata sample.
+// Per frame:
+//   1. histogram pass over all items (AC clusters, per-DC-group DC and
+//      AcMetadata histograms, first-block counts);
+//   2. prefix codes built on the device, one warp per histogram;
+//   3. bit-length pass over all items, then a two-level exclusive scan;
+//   4. a layout CTA sizes every section, writes the container, headers and
+//      TOC, and places the sections;
+//   5. an emit pass writes every item's bits at its final position.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace jxb {
+
+enum SectionKind : int { kSecDcGlobal = 0, kSecDcGroup = 1, kSecAcGlobal = 2, kSecAcGroup = 3 };
+
+struct Section {
+    std::uint32_t first;   // first global item index
+    std::uint32_t count;   // items in the section
+    int kind;
+    int group;             // DC or AC group index
+};
+
+// Geometry and per-frame device state of the entropy stage. All pointers are
+// device memory owned by the encoder.
+struct EntropyDev {
+    // geometry
+    int width, height, bw, bh, nblocks, xg, nac, xdg, ndc, cmw, nsec;
+    std::uint32_t total_items;
+    std::uint32_t num_tiles;         // scan tiles of kScanTile items
+    const Section* sections;
+
+    // inputs (frontend outputs)
+    const std::int16_t* ac;
+    const std::int32_t* dc;
+    const std::int8_t* acs;
+    const std::int32_t* qf;
+    const std::int8_t* ytox;
+    const std::int8_t* ytob;
+    const std::uint8_t* nzn;
+    const std::uint16_t* nzc;
+
+    // constant tables
+    const std::uint16_t* order;      // natural orders: 64 (DCT8) | 256 (DCT16) | 1024 (DCT32)
+    const std::uint8_t* pre_const;   // DcGroup header bits before the DC code description
+    std::uint32_t pre_const_bits;
+    const std::uint8_t* mid_const;   // AcMetadata header bits after the count field
+    std::uint32_t mid_const_bits;
+    const std::uint8_t* ac_prefix;   // AcGlobal bits before the per-cluster sizes
+    std::uint32_t ac_prefix_bits;
+    const std::uint8_t* dc_global;   // DcGlobal section bits (per distance)
+    std::uint32_t dc_global_bits;
+
+    // per-frame scratch
+    std::uint32_t* ac_hist;          // [32][256]
+    std::uint32_t* dc_hist;          // [ndc][256]
+    std::uint32_t* am_hist;          // [ndc][256]
+    std::uint32_t* fb_count;         // [ndc]
+    std::uint8_t* ac_depth;          // [32][256]
+    std::uint16_t* ac_bits;
+    std::uint8_t* dc_depth;          // [ndc][256]
+    std::uint16_t* dc_bits;
+    std::uint8_t* am_depth;          // [ndc][256]
+    std::uint16_t* am_bits;
+    std::uint32_t* ac_alpha;         // [32]
+    std::uint8_t* desc;              // [32 + 2*ndc][kDescBytes] code descriptions
+    std::uint32_t* desc_bits;        // [32 + 2*ndc]
+    std::uint32_t* item_bits;        // [total_items]
+    std::uint32_t* item_pre;         // [total_items] exclusive prefix within its scan tile
+    std::uint32_t* tile_sum;         // [num_tiles]
+    unsigned long long* tile_off;    // [num_tiles + 1]
+    unsigned long long* sec_pos;     // [nsec] absolute byte offset of each section in `out`
+    unsigned long long* result;      // [4]: total bytes, body start, status, 0
+    std::uint8_t* out;               // output buffer (container + codestream)
+    std::size_t out_capacity;
+};
+
+constexpr int kDescBytes = 256;
+constexpr int kScanTile = 4096;
+
+// Builds the constant header blobs and section table for a geometry. Fills the
+// host-side vectors; the caller uploads them.
+struct EntropyHostPlan {
+    std::vector<Section> sections;
+    std::uint32_t total_items{0};
+    std::vector<std::uint8_t> pre_const;
+    std::uint32_t pre_const_bits{0};
+    std::vector<std::uint8_t> mid_const;
+    std::uint32_t mid_const_bits{0};
+    std::vector<std::uint8_t> ac_prefix;
+    std::uint32_t ac_prefix_bits{0};
+    std::vector<std::uint16_t> order;
+};
+EntropyHostPlan entropy_plan(int width, int height);
+
+// DcGlobal section bits for the quantiser state.
+std::vector<std::uint8_t> dc_global_bits(std::uint32_t global_scale, std::uint32_t quant_dc,
+                                         std::uint32_t* nbits);
+
+// Worst-case output size (same bound as the reference's cujpegxl.cc:50-59).
+std::size_t worst_case_output(std::uint32_t width, std::uint32_t height);
+
+// Enqueues the whole entropy + assembly stage on `stream`. After completion
+// result[0] holds the file size and result[2] a status (0 = ok, 1 = output
+// capacity exceeded).
+bool entropy_launch(const EntropyDev& e, void* stream);
+
+}  // namespace jxb

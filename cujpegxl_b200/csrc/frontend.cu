@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -928,9 +929,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
             const int n{sm.acs[lb]};
             const int m{n >> 3};
-            const float dcq_x{kDcInvQuant[0] * sc.dc_scale};
-            const float dcq_y{kDcInvQuant[1] * sc.dc_scale};
-            const float dcq_b{kDcInvQuant[2] * sc.dc_scale};
+            const float dcq_x{4096.0f * sc.dc_scale};
+            const float dcq_y{512.0f * sc.dc_scale};
+            const float dcq_b{256.0f * sc.dc_scale};
             float llf[3][16];
             for (int c{0}; c < 3; ++c) {
                 for (int fx{0}; fx < m; ++fx) {

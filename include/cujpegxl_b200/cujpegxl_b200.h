@@ -1,0 +1,89 @@
+/* Additional entry points of libcujpegxl.so.1 beyond the reference's nine.
+ *
+ * None of these replaces a reference entry point; they expose the encoder's
+ * stages and device buffers for parity testing, benchmarking and callers that
+ * keep frames on the device. They use the same opaque encoder handle and
+ * status codes as include/cujpegxl/cujpegxl.h. Plain C, no CUDA types. */
+
+#ifndef CUJPEGXL_B200_H_
+#define CUJPEGXL_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "cujpegxl/cujpegxl.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Host views of the frontend's planes for one frame (B = (W/8)*(H/8)
+ * blocks, T = ceil(W/64)*ceil(H/64) colour tiles). Any pointer may be NULL.
+ * The optional float/FP16 stage dumps are filled only while debug dumps are
+ * enabled on the encoder. */
+typedef struct cujpegxl_b200_planes {
+    int16_t* ac;      /* [3][B*64] quantised AC, covered-block layout, X,Y,B */
+    int32_t* dc;      /* [3][B] quantised DC */
+    int8_t* acs;      /* [B] transform side at first-blocks, 0 at covered blocks */
+    int32_t* qf;      /* [B] adaptive quant field */
+    int8_t* ytox;     /* [T] */
+    int8_t* ytob;     /* [T] */
+    float* xyb;       /* [3][H][W] XYB before sharpening */
+    float* sharp;     /* [3][H][W] XYB after inverse gaborish */
+    uint16_t* coeff;  /* [3][B*64] FP16 DCT coefficients (bit patterns) */
+} cujpegxl_b200_planes;
+
+/* Enables (non-zero) or disables the float/FP16 stage dumps of the frontend.
+ * Replaces no reference interface. */
+cujpegxl_status cujpegxl_b200_encoder_set_debug(cujpegxl_encoder* encoder, int32_t enable);
+
+/* Copies the planes of the most recent encode to host memory. Replaces no
+ * reference interface. */
+cujpegxl_status cujpegxl_b200_encoder_read_planes(cujpegxl_encoder* encoder,
+                                                  const cujpegxl_b200_planes* host);
+
+/* Entropy coding and assembly only: uploads quantised planes (ac, dc, acs,
+ * qf, ytox, ytob must be non-NULL) and writes the .jxl file, exactly as
+ * cujpegxl_encoder_encode does after its frontend. The stage the reference
+ * runs as encode_frame (src/frame_encoder.h:49-53). */
+cujpegxl_status cujpegxl_b200_encode_planes(cujpegxl_encoder* encoder,
+                                            const cujpegxl_b200_planes* host,
+                                            uint32_t global_scale, uint32_t quant_dc,
+                                            cujpegxl_output* output);
+
+/* Host NV12 in (width*height*3/2 bytes, pitch = width), .jxl out: uploads
+ * through a pinned staging buffer, then encodes. The path of the reference's
+ * Python binding (python/nv12_host_encode.cu:10-40). */
+cujpegxl_status cujpegxl_b200_encode_host(cujpegxl_encoder* encoder, const uint8_t* nv12,
+                                          size_t nv12_size, cujpegxl_output* output);
+
+/* Enqueues one encode on the encoder's stream and returns without waiting;
+ * the file stays in device memory. cujpegxl_b200_encoder_result waits and
+ * reports its size and device address. For callers that keep bytes on the
+ * device and for throughput measurement. Replaces no reference interface. */
+cujpegxl_status cujpegxl_b200_encoder_enqueue(cujpegxl_encoder* encoder,
+                                              const cujpegxl_nv12_input* input);
+cujpegxl_status cujpegxl_b200_encoder_result(cujpegxl_encoder* encoder, size_t* out_size,
+                                             uintptr_t* out_device_bytes);
+
+/* As cujpegxl_b200_encoder_enqueue, restricted to the stages in `stages`
+ * (bit 0: the fused frontend kernel, bit 1: entropy coding and assembly).
+ * For timing one stage in isolation. Replaces no reference interface. */
+#define CUJPEGXL_B200_STAGE_FRONTEND 1u
+#define CUJPEGXL_B200_STAGE_ENTROPY 2u
+cujpegxl_status cujpegxl_b200_encoder_enqueue_stages(cujpegxl_encoder* encoder,
+                                                     const cujpegxl_nv12_input* input,
+                                                     uint32_t stages);
+
+/* The encoder's CUDA stream (a cudaStream_t as an integer), for callers that
+ * order their own work or timing events against it. */
+cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_t* out_stream);
+
+/* Number of kernels one encode launches. */
+uint32_t cujpegxl_b200_kernels_per_encode(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CUJPEGXL_B200_H_ */

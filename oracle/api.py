@@ -71,6 +71,10 @@ def oracle() -> ctypes.CDLL:
         lib.oracle_gaborish_weights.argtypes = [_P]
         lib.oracle_sel_cost.restype = ctypes.c_float
         lib.oracle_sel_cost.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_float]
+        lib.oracle_select_plane.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P]
+        lib.oracle_dc_from_llf.argtypes = [ctypes.c_int, _P, _P]
+        lib.oracle_cfl_maps.argtypes = [ctypes.c_float] * 3 + [_P, _P]
+        lib.oracle_xyb_pixel.argtypes = [ctypes.POINTER(_Frame), ctypes.c_int, ctypes.c_int, _P]
         _oracle = lib
     return _oracle
 

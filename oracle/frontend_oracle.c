@@ -396,6 +396,9 @@ static float tree32(float* v) {
 
 /* ---- tile processing ---- */
 
+void oracle_dc_from_llf(int m, const float* llf, float* dc);
+void oracle_cfl_maps(float sxy, float syy, float sby, int* mx, int* mb);
+
 #define XS 68
 #define XP (XS * XS)
 #define SS 65
@@ -699,12 +702,8 @@ static void process_tile(const OracleFrame* in, const OracleScalars* sc, const O
         for (int l = 0; l < 32; ++l) v[l] = part[k][l] + part[k][l + 32];
         sums[k] = tree32(v);
     }
-    const double dxy = sums[0], dyy = sums[1], dby = sums[2];
-    const float fxr = dyy > 0.0 ? (float)(dxy / dyy) : 0.0f;
-    const float fbr = dyy > 0.0 ? (float)(dby / dyy) : 0.0f;
-    int mx = (int)lrintf(fxr * 84.0f), mb = (int)lrintf(fbr * 84.0f);
-    mx = mx < -128 ? -128 : (mx > 127 ? 127 : mx);
-    mb = mb < -128 ? -128 : (mb > 127 ? 127 : mb);
+    int mx, mb;
+    oracle_cfl_maps(sums[0], sums[1], sums[2], &mx, &mb);
     out->ytox[ty * cmw + tx] = (int8_t)mx;
     out->ytob[ty * cmw + tx] = (int8_t)mb;
 
@@ -757,25 +756,7 @@ static void process_tile(const OracleFrame* in, const OracleScalars* sc, const O
                     const int raw = fx * n + fy, q = raw >> 6;
                     llf[c][fx * m + fy] = oracle_h2f(T->coef[c][(lb + (q / m) * 8 + q % m) * 64 + (raw & 63)]);
                 }
-        if (m == 1) {
-            for (int c = 0; c < 3; ++c) dcv[c][0] = llf[c][0];
-        } else {
-            const double* ob = g_ob[m == 2 ? 0 : 1];
-            const double s16[2] = {1.0, 0.901764195028874394};
-            const double s32[4] = {1.0, 0.974886821136879522, 0.901764195028874394, 0.787054918159101335};
-            const double* scl = m == 2 ? s16 : s32;
-            for (int c = 0; c < 3; ++c)
-                for (int oy = 0; oy < m; ++oy)
-                    for (int ox = 0; ox < m; ++ox) {
-                        double sum = 0.0;
-                        for (int fx = 0; fx < m; ++fx)
-                            for (int fy = 0; fy < m; ++fy) {
-                                const double cv = llf[c][fx * m + fy];
-                                sum = sum + ob[fx * 4 + ox] * ob[fy * 4 + oy] * cv * scl[fx] * scl[fy];
-                            }
-                        dcv[c][oy * m + ox] = (float)((double)m * sum);
-                    }
-        }
+        for (int c = 0; c < 3; ++c) oracle_dc_from_llf(m, llf[c], dcv[c]);
         for (int oy = 0; oy < m; ++oy)
             for (int ox = 0; ox < m; ++ox) {
                 const int p = oy * m + ox;
@@ -841,6 +822,90 @@ int oracle_frontend(const OracleFrame* in, float distance, const OracleOutputs* 
     for (int i = 0; i < threads; ++i) pthread_create(&tids[i], NULL, worker, &w);
     for (int i = 0; i < threads; ++i) pthread_join(tids[i], NULL);
     return 0;
+}
+
+/* Transform selection over a whole plane `y` (width x height, row stride
+ * width) with the same costs and decision as the tile path. */
+void oracle_select_plane(const float* y, int width, int height, float distance, int8_t* acs) {
+    ensure_tables();
+    OracleScalars sc;
+    oracle_scalars(distance, &sc);
+    const int bw = width / 8, bh = height / 8;
+    for (int rby = 0; rby < bh; rby += 4)
+        for (int rbx = 0; rbx < bw; rbx += 4) {
+            float c8[4][4], c16[2][2], c32 = 0.0f;
+            for (int dy = 0; dy < 4; ++dy)
+                for (int dx = 0; dx < 4; ++dx)
+                    if (rbx + dx < bw && rby + dy < bh)
+                        c8[dy][dx] = oracle_sel_cost(y + (size_t)(rby + dy) * 8 * width + (rbx + dx) * 8, width, 8,
+                                                     sc.qgsf_select);
+            for (int qy = 0; qy < 2; ++qy)
+                for (int qx = 0; qx < 2; ++qx)
+                    if (rbx + 2 * qx + 2 <= bw && rby + 2 * qy + 2 <= bh)
+                        c16[qy][qx] = oracle_sel_cost(y + (size_t)(rby + 2 * qy) * 8 * width + (rbx + 2 * qx) * 8,
+                                                      width, 16, sc.qgsf_select);
+            const int fit32 = rbx + 4 <= bw && rby + 4 <= bh;
+            if (fit32) c32 = oracle_sel_cost(y + (size_t)rby * 8 * width + rbx * 8, width, 32, sc.qgsf_select);
+            float split = 0.0f;
+            int choice[2][2];
+            for (int qy = 0; qy < 2; ++qy)
+                for (int qx = 0; qx < 2; ++qx) {
+                    const int bx = rbx + 2 * qx, by = rby + 2 * qy;
+                    float sum8 = 0.0f;
+                    int any = 0;
+                    for (int dy = 0; dy < 2; ++dy)
+                        for (int dx = 0; dx < 2; ++dx)
+                            if (bx + dx < bw && by + dy < bh) { sum8 = sum8 + c8[2 * qy + dy][2 * qx + dx]; any = 1; }
+                    if (!any) { choice[qy][qx] = -1; continue; }
+                    const int fit16 = bx + 2 <= bw && by + 2 <= bh;
+                    if (fit16 && c16[qy][qx] <= sum8 + 1.0e-6f) { choice[qy][qx] = 16; split = split + c16[qy][qx]; }
+                    else { choice[qy][qx] = 8; split = split + sum8; }
+                }
+            if (fit32 && c32 <= split + 1.0e-6f) {
+                for (int dy = 0; dy < 4; ++dy)
+                    for (int dx = 0; dx < 4; ++dx) acs[(rby + dy) * bw + rbx + dx] = (dx == 0 && dy == 0) ? 32 : 0;
+                continue;
+            }
+            for (int qy = 0; qy < 2; ++qy)
+                for (int qx = 0; qx < 2; ++qx) {
+                    if (choice[qy][qx] < 0) continue;
+                    for (int dy = 0; dy < 2; ++dy)
+                        for (int dx = 0; dx < 2; ++dx) {
+                            const int bx = rbx + 2 * qx + dx, by = rby + 2 * qy + dy;
+                            if (choice[qy][qx] == 16) acs[by * bw + bx] = (dx == 0 && dy == 0) ? 16 : 0;
+                            else if (bx < bw && by < bh) acs[by * bw + bx] = 8;
+                        }
+                }
+        }
+}
+
+/* LLF -> DC resampling of an m x m corner (src/vardct_layout.h:88-111). */
+void oracle_dc_from_llf(int m, const float* llf, float* dc) {
+    ensure_tables();
+    if (m == 1) { dc[0] = llf[0]; return; }
+    const double* ob = g_ob[m == 2 ? 0 : 1];
+    const double s16[2] = {1.0, 0.901764195028874394};
+    const double s32[4] = {1.0, 0.974886821136879522, 0.901764195028874394, 0.787054918159101335};
+    const double* scl = m == 2 ? s16 : s32;
+    for (int oy = 0; oy < m; ++oy)
+        for (int ox = 0; ox < m; ++ox) {
+            double sum = 0.0;
+            for (int fx = 0; fx < m; ++fx)
+                for (int fy = 0; fy < m; ++fy)
+                    sum = sum + g_ob[m == 2 ? 0 : 1][fx * 4 + ox] * ob[fy * 4 + oy] * (double)llf[fx * m + fy] * scl[fx] *
+                                    scl[fy];
+            dc[oy * m + ox] = (float)((double)m * sum);
+        }
+}
+
+/* CfL regression sums -> map values (src/cfl.h:63-77). */
+void oracle_cfl_maps(float sxy, float syy, float sby, int* mx, int* mb) {
+    const double dxy = sxy, dyy = syy, dby = sby;
+    const float fxr = dyy > 0.0 ? (float)(dxy / dyy) : 0.0f;
+    const float fbr = dyy > 0.0 ? (float)(dby / dyy) : 0.0f;
+    int x = (int)lrintf(fxr * 84.0f), b = (int)lrintf(fbr * 84.0f);
+    *mx = x < -128 ? -128 : (x > 127 ? 127 : x);
+    *mb = b < -128 ? -128 : (b > 127 ? 127 : b);
 }
 
 /* Individual formulas, exposed for tests. */

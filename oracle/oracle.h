@@ -69,6 +69,9 @@ float oracle_masking_sqrt(float v);
 float oracle_compute_mask(float v);
 void oracle_gaborish_weights(float* out6);
 float oracle_sel_cost(const float* y, int stride, int n, float qgsf);
+void oracle_select_plane(const float* y, int width, int height, float distance, int8_t* acs);
+void oracle_dc_from_llf(int m, const float* llf, float* dc);
+void oracle_cfl_maps(float sxy, float syy, float sby, int* mx, int* mb);
 size_t oracle_huffman(const uint32_t* hist, size_t len, uint8_t* depth, uint16_t* bits,
                       uint8_t* out, size_t cap);
 
