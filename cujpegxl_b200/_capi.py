@@ -28,7 +28,7 @@ EXPORTS = (
     "cujpegxl_b200_encoder_set_debug", "cujpegxl_b200_encoder_read_planes",
     "cujpegxl_b200_encode_planes", "cujpegxl_b200_encode_host", "cujpegxl_b200_encoder_enqueue",
     "cujpegxl_b200_encoder_enqueue_stages", "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream",
-    "cujpegxl_b200_kernels_per_encode",
+    "cujpegxl_b200_kernels_per_encode", "cujpegxl_b200_encode_planes_noalloc",
 )
 
 
@@ -48,6 +48,10 @@ class Output(ctypes.Structure):
 
 class Planes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("ac", "dc", "acs", "qf", "ytox", "ytob", "xyb", "sharp", "coeff")]
+
+
+class DevicePlanes(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_size_t) for n in ("ac", "dc", "acs", "qf", "ytox", "ytob")]
 
 
 _lib: ctypes.CDLL | None = None
@@ -83,6 +87,10 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_encoder_result.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encoder_stream.argtypes = [E, P(ctypes.c_size_t)]
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
+    L.cujpegxl_b200_encode_planes_noalloc.argtypes = [P(DevicePlanes), ctypes.c_uint32, ctypes.c_uint32,
+                                                      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                                      ctypes.c_size_t, P(ctypes.c_size_t), ctypes.c_size_t]
+    L.cujpegxl_b200_encode_planes_noalloc.restype = ctypes.c_int
     for name in ("cujpegxl_query_backend", "cujpegxl_max_output_size", "cujpegxl_encoder_create",
                  "cujpegxl_encoder_configure", "cujpegxl_encoder_encode", "cujpegxl_b200_encoder_set_debug",
                  "cujpegxl_b200_encoder_read_planes", "cujpegxl_b200_encode_planes",

@@ -365,6 +365,18 @@ __global__ void nz_kernel(const std::int16_t* ac, const std::int8_t* acs, int bw
 
 }  // namespace
 
+namespace jxb {
+// Launches the non-zero-count kernel above on `stream` (used by entry points
+// that take quantised planes from the caller).
+bool launch_nz_counts(const std::int16_t* ac, const std::int8_t* acs, int bw, int bh, std::uint8_t* nzn,
+                      std::uint16_t* nzc, void* stream) {
+    const int nb{bw * bh};
+    nz_kernel<<<static_cast<unsigned>((nb + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        ac, acs, bw, bh, nzn, nzc);
+    return cudaGetLastError() == cudaSuccess;
+}
+}  // namespace jxb
+
 extern "C" {
 
 uint32_t cujpegxl_api_version(void) { return CUJPEGXL_API_VERSION; }

@@ -79,6 +79,42 @@ cujpegxl_status cujpegxl_b200_encoder_enqueue_stages(cujpegxl_encoder* encoder,
  * order their own work or timing events against it. */
 cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_t* out_stream);
 
+/* Device views of quantised planes (layouts as cujpegxl_b200_planes), as
+ * integer device addresses. */
+typedef struct cujpegxl_b200_device_planes {
+    uintptr_t ac;     /* int16_t [3][B*64] */
+    uintptr_t dc;     /* int32_t [3][B] */
+    uintptr_t acs;    /* int8_t [B] */
+    uintptr_t qf;     /* int32_t [B] */
+    uintptr_t ytox;   /* int8_t [T] */
+    uintptr_t ytob;   /* int8_t [T] */
+} cujpegxl_b200_device_planes;
+
+/* No counterpart in the reference. Entropy coding and assembly of one frame
+ * from quantised planes already in device memory, producing the same file as
+ * cujpegxl_b200_encode_planes, for callers that cannot allocate device memory
+ * while they encode (inside a stream capture, in a real-time loop where
+ * cudaMalloc would synchronise the device, or with all device memory held by
+ * their own pool). It allocates nothing: the caller passes the planes and a
+ * device output buffer (16-byte aligned, `out_capacity` bytes), and every
+ * intermediate lives in one fixed 7 MiB array that each GPU loading the
+ * library holds until the process exits.
+ *  - Frames above 4,194,304 pixels (width*height) are rejected with
+ *    CUJPEGXL_UNSUPPORTED_RESOLUTION; other geometry rules are those of
+ *    cujpegxl_encoder_create.
+ *  - The first call on a device looks up the array's device address and sets
+ *    kernel attributes; make that first call before any stream capture.
+ *  - Calls share the array: calls that overlap on the GPU (different streams
+ *    or threads without ordering) race and corrupt each other's output.
+ *  - Work is enqueued on `stream` (a cudaStream_t as an integer, 0 for the
+ *    default stream); the call waits for it and sets *out_size to the file
+ *    length, or to the required length with CUJPEGXL_BUFFER_TOO_SMALL. */
+cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_planes* planes,
+                                                    uint32_t width, uint32_t height,
+                                                    uint32_t global_scale, uint32_t quant_dc,
+                                                    uint8_t* out_device, size_t out_capacity,
+                                                    size_t* out_size, uintptr_t stream);
+
 /* Number of kernels one encode launches. */
 uint32_t cujpegxl_b200_kernels_per_encode(void);
 
