@@ -11,6 +11,7 @@ exports only the cujpegxl_* symbols, as the reference library does.
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -23,7 +24,7 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libcujpegxl.so.1"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["frontend.cu", "entropy.cu", "cujpegxl.cu", "noalloc.cu"]
+SOURCES = ["frontend.cu", "entropy.cu", "entropy_host.cu", "cujpegxl.cu", "noalloc.cu"]
 HEADERS = ["frontend.cuh", "entropy.cuh", "jxl_constants.cuh", "jxl_math.cuh", "prefix_code.cuh",
            "jxl_dequant_tables.inc", "cujpegxl.map"]
 
@@ -45,6 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     OUT_DIR.mkdir(exist_ok=True)
     hdrs = [CSRC / h for h in HEADERS] + list((REPO / "include").rglob("*.h"))
     objs = []
+    jobs = []
     for src in SOURCES:
         obj = OUT_DIR / (Path(src).stem + ".o")
         if force or _stale(obj, [CSRC / src] + hdrs):
@@ -52,8 +54,11 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
         objs.append(obj)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, len(jobs))) as pool:
+        for _ in pool.map(lambda c: subprocess.run(c, check=True), jobs):
+            pass
     if force or _stale(LIB, objs + [CSRC / "cujpegxl.map"]):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIB)] + [str(o) for o in objs] + [
             "-Xlinker", f"--version-script={CSRC / 'cujpegxl.map'}",

@@ -101,6 +101,10 @@ cujpegxl_status validate_config(const cujpegxl_config& c) {
     }
     const std::size_t nac{((c.width / 8 + 31) / 32) * static_cast<std::size_t>((c.height / 8 + 31) / 32)};
     if (nac <= 1) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
+    // The TOC is written in one CTA's shared memory: about 25,000 sections
+    // (1.6 gigapixels) at most.
+    const std::size_t ndc{((c.width / 8 + 255) / 256) * static_cast<std::size_t>((c.height / 8 + 255) / 256)};
+    if (2 + ndc + nac > static_cast<std::size_t>(jxb::kMaxSections)) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
     return CUJPEGXL_OK;
 }
 
@@ -215,6 +219,7 @@ bool allocate(cujpegxl_encoder* e) {
     ed.cmw = static_cast<int>((bw + 7) / 8);
     ed.nsec = static_cast<int>(plan.sections.size());
     ed.total_items = plan.total_items;
+    ed.ac_first = plan.ac_first;
     ed.num_tiles = tiles;
     ed.sections = reinterpret_cast<const jxb::Section*>(b + o_sec);
     ed.ac = fo.ac;
@@ -661,6 +666,6 @@ cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_
     return CUJPEGXL_OK;
 }
 
-uint32_t cujpegxl_b200_kernels_per_encode(void) { return 9u; }
+uint32_t cujpegxl_b200_kernels_per_encode(void) { return 12u; }
 
 }  // extern "C"

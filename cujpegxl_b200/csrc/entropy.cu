@@ -8,12 +8,17 @@
 // (src/entropy.cu:252-274); hybrid-uint (4,2,0) tokens; prefix codes from
 // prefix_code.cuh; section layout and headers as src/frame_encoder.cu:88-292
 // and src/bitstream/{frame_assembly,codestream,container}.cc.
+//
+// AC block-channels are tokenised one warp per item: each lane takes one scan
+// position of a 32-position chunk, and ballots plus prefix counts give every
+// lane the reference's sequential state at its position (non-zeros left,
+// previous-coefficient flag), so a chunk's tokens, contexts, bit lengths and
+// bit offsets come out in one step. Every other item (header blobs, DC
+// residuals, AcMetadata samples) takes one thread.
 
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstring>
-#include <vector>
 
 #include "entropy.cuh"
 #include "jxl_constants.cuh"
@@ -22,12 +27,13 @@
 namespace jxb {
 namespace {
 
+constexpr unsigned kFull = 0xffffffffu;
+
 // Token channel order Y, X, B over planes stored X, Y, B.
 __device__ __forceinline__ int phys_channel(int p) { return p == 0 ? 1 : (p == 1 ? 0 : 2); }
 
-__device__ __forceinline__ int find_section(const Section* secs, int nsec, std::uint32_t item) {
-    int lo{0};
-    int hi{nsec - 1};
+// Section holding `item`, searched in sections [lo, hi].
+__device__ __forceinline__ int find_section(const Section* secs, int lo, int hi, std::uint32_t item) {
     while (lo < hi) {
         const int mid{(lo + hi + 1) >> 1};
         if (__ldg(&secs[mid].first) <= item) {
@@ -61,16 +67,18 @@ __device__ __forceinline__ GroupGeom dc_group_geom(const EntropyDev& e, int g) {
     return r;
 }
 
-// Table selectors for tokens.
-enum TokTable : int { kTabAc = 0, kTabDc = 1, kTabAm = 2 };
+enum TokTable : int { kTabDc = 1, kTabAm = 2 };
 
-// Visits the bits of one item in stream order. The visitor receives
-//   blob(bytes, nbits), raw(nbits, value),
-//   token(table, index, symbol, extra_bits, extra_value, hist_weight_flag)
-// where `index` is the AC cluster or the DC group.
+__device__ __forceinline__ int misc_hi(const EntropyDev& e) { return e.ndc + 1; }
+
+// ---- items other than AC block-channels -------------------------------------------
+
+// Visits the bits of one non-AC item in stream order: blob(bytes, nbits),
+// varlen(v), count_field(group, nbits), epf(group), first_block(group),
+// token(table, group, symbol, extra_bits, extra_value).
 template <class V>
-__device__ void visit_item(const EntropyDev& e, std::uint32_t item, V& v) {
-    const int s{find_section(e.sections, e.nsec, item)};
+__device__ void visit_misc(const EntropyDev& e, std::uint32_t item, V& v) {
+    const int s{find_section(e.sections, 0, misc_hi(e), item)};
     const Section sec{e.sections[s]};
     const std::uint32_t j{item - sec.first};
     if (sec.kind == kSecDcGlobal) {
@@ -87,47 +95,6 @@ __device__ void visit_item(const EntropyDev& e, std::uint32_t item, V& v) {
         }
         return;
     }
-    if (sec.kind == kSecAcGroup) {
-        const GroupGeom gg{ac_group_geom(e, sec.group)};
-        const int bidx{static_cast<int>(j / 3)};
-        const int c{phys_channel(static_cast<int>(j % 3))};
-        const int bx{gg.bx0 + bidx % gg.gw};
-        const int by{gg.by0 + bidx / gg.gw};
-        const std::size_t blk{static_cast<std::size_t>(by) * e.bw + bx};
-        const int n{e.acs[blk]};
-        if (n == 0) return;
-        const std::size_t cb{static_cast<std::size_t>(c) * e.nblocks};
-        const std::uint32_t nz{e.nzc[cb + blk]};
-        const bool hl{bx > gg.bx0};
-        const bool ht{by > gg.by0};
-        const std::uint32_t top{ht ? e.nzn[cb + blk - e.bw] : 0u};
-        const std::uint32_t left{hl ? e.nzn[cb + blk - 1] : 0u};
-        const int bctx{block_ctx(c, n)};
-        std::uint32_t tok, nb, bits;
-        hybrid_uint(nz, tok, nb, bits);
-        v.token(kTabAc, context_cluster(nonzero_context(predict_nonzeros(hl, ht, top, left), bctx)),
-                tok, nb, bits);
-        if (nz == 0) return;
-        const int side{n >> 3};
-        const std::uint32_t covered{static_cast<std::uint32_t>(side * side)};
-        const std::uint32_t size{static_cast<std::uint32_t>(n * n)};
-        const std::uint32_t l2{n == 16 ? 2u : (n == 32 ? 4u : 0u)};
-        const std::uint16_t* ord{e.order + (n == 8 ? 0 : (n == 16 ? 64 : 320))};
-        const std::int16_t* plane{e.ac + static_cast<std::size_t>(c) * e.nblocks * kCoeffsPerBlock};
-        std::uint32_t remaining{nz};
-        std::uint32_t prev{nz > size / 16 ? 0u : 1u};
-        for (std::uint32_t k{covered}; k < size && remaining > 0; ++k) {
-            const int raw{__ldg(&ord[k])};
-            const std::int32_t val{plane[covered_slot(n, bx, by, e.bw, raw)]};
-            const std::uint32_t ctx{coeff_context(bctx, remaining, k, covered, l2, prev)};
-            hybrid_uint(pack_signed(val), tok, nb, bits);
-            v.token(kTabAc, context_cluster(ctx), tok, nb, bits);
-            prev = val != 0 ? 1u : 0u;
-            remaining -= prev;
-        }
-        return;
-    }
-    // DC group.
     const int g{sec.group};
     const GroupGeom gg{dc_group_geom(e, g)};
     const std::uint32_t n{static_cast<std::uint32_t>(gg.gw * gg.gh)};
@@ -202,12 +169,119 @@ __device__ void visit_item(const EntropyDev& e, std::uint32_t item, V& v) {
     v.token(kTabAm, g, tok, nb, bits);
 }
 
+// ---- AC block-channels, one warp per item ---------------------------------------------
+
+struct AcItem {
+    int n;                 // transform side, 0 for a covered block (no tokens)
+    int c;                 // plane 0=X, 1=Y, 2=B
+    int bx, by;
+    std::uint32_t nz;      // non-zero AC count
+    int nz_cluster;        // cluster of the count token
+    int section;
+};
+
+__device__ __forceinline__ AcItem ac_item(const EntropyDev& e, std::uint32_t item) {
+    AcItem it{};
+    it.section = find_section(e.sections, e.ndc + 2, e.nsec - 1, item);
+    const Section sec{e.sections[it.section]};
+    const std::uint32_t j{item - sec.first};
+    const GroupGeom gg{ac_group_geom(e, sec.group)};
+    const int bidx{static_cast<int>(j / 3)};
+    it.c = phys_channel(static_cast<int>(j % 3));
+    it.bx = gg.bx0 + bidx % gg.gw;
+    it.by = gg.by0 + bidx / gg.gw;
+    const std::size_t blk{static_cast<std::size_t>(it.by) * e.bw + it.bx};
+    it.n = e.acs[blk];
+    if (it.n == 0) return it;
+    const std::size_t cb{static_cast<std::size_t>(it.c) * e.nblocks};
+    it.nz = e.nzc[cb + blk];
+    const bool hl{it.bx > gg.bx0};
+    const bool ht{it.by > gg.by0};
+    const std::uint32_t top{ht ? e.nzn[cb + blk - e.bw] : 0u};
+    const std::uint32_t left{hl ? e.nzn[cb + blk - 1] : 0u};
+    it.nz_cluster = context_cluster(nonzero_context(predict_nonzeros(hl, ht, top, left), block_ctx(it.c, it.n)));
+    return it;
+}
+
+// Calls f(has, cluster, symbol, extra_bits, extra_value) once per step with
+// all 32 lanes (so f may use warp collectives): first the count token on
+// lane 0, then one coefficient token per lane per 32-position chunk of the
+// scan, in stream order. Replicates the sequential loop of
+// src/entropy.cu:653-680: a position is coded while non-zeros remain before it.
+template <class F>
+__device__ void ac_warp_tokens(const EntropyDev& e, const AcItem& it, int lane, F&& f) {
+    {
+        std::uint32_t tok, nb, bits;
+        hybrid_uint(it.nz, tok, nb, bits);
+        f(lane == 0, it.nz_cluster, tok, nb, bits);
+    }
+    if (it.nz == 0) return;
+    const int n{it.n};
+    const int side{n >> 3};
+    const std::uint32_t covered{static_cast<std::uint32_t>(side * side)};
+    const std::uint32_t size{static_cast<std::uint32_t>(n * n)};
+    const std::uint32_t l2{n == 16 ? 2u : (n == 32 ? 4u : 0u)};
+    const int bctx{block_ctx(it.c, n)};
+    const std::uint16_t* ord{e.order + (n == 8 ? 0 : (n == 16 ? 64 : 320))};
+    const std::int16_t* plane{e.ac + static_cast<std::size_t>(it.c) * e.nblocks * kCoeffsPerBlock};
+    std::uint32_t remaining{it.nz};
+    std::uint32_t prev{it.nz > size / 16 ? 0u : 1u};
+    const unsigned below{(1u << lane) - 1u};
+    for (std::uint32_t k0{covered}; k0 < size && remaining > 0; k0 += 32) {
+        const std::uint32_t k{k0 + static_cast<std::uint32_t>(lane)};
+        std::int32_t val{0};
+        if (k < size) val = plane[covered_slot(n, it.bx, it.by, e.bw, __ldg(&ord[k]))];
+        const unsigned nzmask{__ballot_sync(kFull, val != 0)};
+        const std::uint32_t left{remaining - static_cast<std::uint32_t>(__popc(nzmask & below))};
+        const std::uint32_t p{lane == 0 ? prev : ((nzmask >> (lane - 1)) & 1u)};
+        const bool has{k < size && left > 0};
+        std::uint32_t tok{0}, nb{0}, bits{0};
+        int cl{0};
+        if (has) {
+            cl = context_cluster(coeff_context(bctx, left, k, covered, l2, p));
+            hybrid_uint(pack_signed(val), tok, nb, bits);
+        }
+        f(has, cl, tok, nb, bits);
+        remaining -= static_cast<std::uint32_t>(__popc(nzmask));
+        prev = (nzmask >> 31) & 1u;
+    }
+}
+
+constexpr int kAcWarps = 8;
+
+__device__ __forceinline__ std::uint32_t warp_sum(std::uint32_t v) {
+#pragma unroll
+    for (int off{16}; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+    return v;
+}
+
 // ---- pass 1: histograms ---------------------------------------------------------
 
+__global__ void __launch_bounds__(kAcWarps * 32) ac_hist_kernel(EntropyDev e) {
+    __shared__ std::uint32_t sh[kNumClusters * 256];
+    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
+    const std::uint32_t stride{gridDim.x * kAcWarps};
+    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
+        const AcItem it{ac_item(e, item)};
+        if (it.n == 0) continue;
+        ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t, std::uint32_t) {
+            const unsigned key{has ? static_cast<unsigned>(cl * 256 + sym) : 0xffffffffu};
+            const unsigned peers{__match_any_sync(kFull, key)};
+            if (has && (__ffs(peers) - 1) == lane) atomicAdd(&sh[key], static_cast<unsigned>(__popc(peers)));
+        });
+    }
+    __syncthreads();
+    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) {
+        if (sh[i]) atomicAdd(&e.ac_hist[i], sh[i]);
+    }
+}
+
 struct HistVisitor {
-    std::uint32_t* sh_ac;     // [32][256] shared
-    std::uint32_t* sh_g;      // [2][2][256] shared: slot x (dc, am)
-    std::uint32_t* sh_fb;     // [2] shared first-block counts per slot
+    std::uint32_t* sh_g;      // [2 slots][2 tables][256]
+    std::uint32_t* sh_fb;     // [2 slots]
     int g0, g1;
     const EntropyDev* e;
     __device__ void blob(const std::uint8_t*, std::uint32_t) {}
@@ -223,42 +297,33 @@ struct HistVisitor {
             atomicAdd(&e->fb_count[g], 1u);
         }
     }
-    __device__ void token(int tab, int idx, std::uint32_t sym, std::uint32_t, std::uint32_t) {
-        if (tab == kTabAc) {
-            atomicAdd(&sh_ac[idx * 256 + sym], 1u);
-            return;
-        }
+    __device__ void token(int tab, int g, std::uint32_t sym, std::uint32_t, std::uint32_t) {
         const int t{tab == kTabDc ? 0 : 1};
-        if (idx == g0) {
-            atomicAdd(&sh_g[(0 * 2 + t) * 256 + sym], 1u);
-        } else if (idx == g1) {
-            atomicAdd(&sh_g[(1 * 2 + t) * 256 + sym], 1u);
+        if (g == g0) {
+            atomicAdd(&sh_g[t * 256 + sym], 1u);
+        } else if (g == g1) {
+            atomicAdd(&sh_g[(2 + t) * 256 + sym], 1u);
         } else {
-            atomicAdd(&(t == 0 ? e->dc_hist : e->am_hist)[idx * 256 + sym], 1u);
+            atomicAdd(&(t == 0 ? e->dc_hist : e->am_hist)[g * 256 + sym], 1u);
         }
     }
 };
 
-__global__ void __launch_bounds__(256) hist_kernel(EntropyDev e) {
-    __shared__ std::uint32_t sh_ac[kNumClusters * 256];
+__global__ void __launch_bounds__(256) misc_hist_kernel(EntropyDev e) {
     __shared__ std::uint32_t sh_g[4 * 256];
     __shared__ std::uint32_t sh_fb[2];
     if (threadIdx.x < 2) sh_fb[threadIdx.x] = 0;
-    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) sh_ac[i] = 0;
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) sh_g[i] = 0;
     const std::uint32_t first{blockIdx.x * blockDim.x};
-    const std::uint32_t last{min(first + blockDim.x, e.total_items) - 1};
-    const Section s0{e.sections[find_section(e.sections, e.nsec, first)]};
-    const Section s1{e.sections[find_section(e.sections, e.nsec, last)]};
-    HistVisitor v{sh_ac, sh_g, sh_fb, s0.kind == kSecDcGroup ? s0.group : -1,
+    const std::uint32_t last{min(first + blockDim.x, e.ac_first) - 1};
+    const Section s0{e.sections[find_section(e.sections, 0, misc_hi(e), first)]};
+    const Section s1{e.sections[find_section(e.sections, 0, misc_hi(e), last)]};
+    HistVisitor v{sh_g, sh_fb, s0.kind == kSecDcGroup ? s0.group : -1,
                   s1.kind == kSecDcGroup && s1.group != s0.group ? s1.group : -2, &e};
     __syncthreads();
     const std::uint32_t item{first + threadIdx.x};
-    if (item < e.total_items) visit_item(e, item, v);
+    if (item < e.ac_first) visit_misc(e, item, v);
     __syncthreads();
-    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) {
-        if (sh_ac[i]) atomicAdd(&e.ac_hist[i], sh_ac[i]);
-    }
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) {
         const int slot{i >> 9};
         const int t{(i >> 8) & 1};
@@ -279,31 +344,36 @@ struct WarpCodeSmem {
     std::uint8_t level[2 * 256 + 4];
     std::uint8_t depth[256];
     std::uint16_t bits[256];
+    std::uint16_t used[256];   // compacted list of used symbols
+    std::uint8_t desc[kDescBytes];
 };
 
 // Depths for a histogram with at least two used symbols, warp-cooperative:
-// each lane ranks its symbols by (clamped count ascending, symbol descending),
-// which is the order the reference's stable sort produces from leaves pushed
-// in descending symbol order; lane 0 merges and assigns levels.
+// the used symbols are compacted, each lane ranks its share by (clamped count
+// ascending, symbol descending) -- the order the reference's stable sort gives
+// leaves pushed in descending symbol order -- and lane 0 merges and assigns
+// levels (src/bitstream/prefix_code.cc:65-125).
 __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lane) {
+    int n{0};
+    for (int base{0}; base < length; base += 32) {
+        const int sym{base + lane};
+        const bool used{sym < length && s.hist[sym] != 0};
+        const unsigned m{__ballot_sync(kFull, used)};
+        if (used) s.used[n + __popc(m & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(sym);
+        n += __popc(m);
+    }
+    __syncwarp();
     for (std::uint32_t floor{1};; floor *= 2) {
-        int mine{0};
-        for (int sym{lane}; sym < length; sym += 32) {
-            if (s.hist[sym]) ++mine;
-        }
-        int n{mine};
-#pragma unroll
-        for (int off{16}; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
-        for (int sym{lane}; sym < length; sym += 32) {
+        for (int i{lane}; i < n; i += 32) {
+            const int sym{s.used[i]};
             const std::uint32_t h{s.hist[sym]};
-            if (!h) continue;
             const std::uint32_t c{h > floor - 1 ? h : floor - 1};
             int rank{0};
-            for (int t{0}; t < length; ++t) {
-                const std::uint32_t ht{s.hist[t]};
-                if (!ht) continue;
+            for (int t{0}; t < n; ++t) {
+                const int ts{s.used[t]};
+                const std::uint32_t ht{s.hist[ts]};
                 const std::uint32_t ct{ht > floor - 1 ? ht : floor - 1};
-                rank += (ct < c || (ct == c && t > sym)) ? 1 : 0;
+                rank += (ct < c || (ct == c && ts > sym)) ? 1 : 0;
             }
             s.pool[rank].count = c;
             s.pool[rank].left = -1;
@@ -313,28 +383,22 @@ __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lan
         int mx{0};
         if (lane == 0) {
             merge_pool(s.pool, n);
-            for (int i{0}; i < length; ++i) s.depth[i] = 0;
             depths_from_pool(s.pool, n, s.level, s.depth);
-            for (int i{0}; i < length; ++i) mx = s.depth[i] > mx ? s.depth[i] : mx;
+            for (int i{0}; i < n; ++i) mx = max(mx, static_cast<int>(s.depth[s.used[i]]));
         }
-        mx = __shfl_sync(0xffffffffu, mx, 0);
+        mx = __shfl_sync(kFull, mx, 0);
         __syncwarp();
         if (mx <= limit) return;
     }
 }
 
-// build_and_store for histogram s.hist[0..length), warp-cooperative; lane 0
-// writes the header into w. Leaves depth/bits in s.
+// build_and_store for s.hist[0..length) (src/bitstream/prefix_code.cc:387-426);
+// lane 0 writes the header into w.
 __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, int lane) {
-    for (int i{lane}; i < 256; i += 32) {
-        s.depth[i] = 0;
-        s.bits[i] = 0;
-    }
-    __syncwarp();
     int s4[4]{0, 0, 0, 0};
     int count{0};
     if (lane == 0) count = symbol_census(s.hist, length, s4);
-    count = __shfl_sync(0xffffffffu, count, 0);
+    count = __shfl_sync(kFull, count, 0);
     if (count <= 1) {
         if (lane == 0) {
             w.put(4, 1);
@@ -356,7 +420,7 @@ __global__ void __launch_bounds__(512) codes_kernel(EntropyDev e) {
     const int warp{static_cast<int>(threadIdx.x) >> 5};
     const int lane{static_cast<int>(threadIdx.x) & 31};
     WarpCodeSmem& s{reinterpret_cast<WarpCodeSmem*>(code_smem)[warp]};
-    int idx;          // description slot
+    int idx;
     const std::uint32_t* src;
     std::uint8_t* dst_depth;
     std::uint16_t* dst_bits;
@@ -387,48 +451,35 @@ __global__ void __launch_bounds__(512) codes_kernel(EntropyDev e) {
         }
         clustered = false;
     }
-    for (int i{lane}; i < 256; i += 32) s.hist[i] = src[i] + (i == 0 ? extra0 : 0u);
-    std::uint8_t* d{e.desc + idx * kDescBytes};
-    for (int i{lane}; i < kDescBytes; i += 32) d[i] = 0;
+    for (int i{lane}; i < 256; i += 32) {
+        s.hist[i] = src[i] + (i == 0 ? extra0 : 0u);
+        s.depth[i] = 0;
+        s.bits[i] = 0;
+    }
+    for (int i{lane}; i < kDescBytes; i += 32) s.desc[i] = 0;
     __syncwarp();
     int alpha{1};
     for (int i{lane}; i < 256; i += 32) {
         if (s.hist[i]) alpha = i + 1;
     }
 #pragma unroll
-    for (int off{16}; off > 0; off >>= 1) alpha = max(alpha, __shfl_xor_sync(0xffffffffu, alpha, off));
-    BitSink w{d, 0, kDescBytes * 8, false};
-    if (clustered) {
-        if (lane == 0) e.ac_alpha[idx] = static_cast<std::uint32_t>(alpha);
-        if (alpha > 1) {
-            warp_build_and_store(s, alpha, w, lane);
-        } else {
-            for (int i{lane}; i < 256; i += 32) {
-                s.depth[i] = 0;
-                s.bits[i] = 0;
-            }
-            __syncwarp();
-        }
-    } else {
-        // Single-context prefix histogram (src/bitstream/histogram_writer.cc:59-83).
-        if (lane == 0) {
-            w.put(1, 0);
-            w.put(1, 1);
-            put_uint_config(w, 4, 2, 0);
-            put_var_len_u16(w, static_cast<std::uint32_t>(alpha - 1));
-        }
-        w.pos = __shfl_sync(0xffffffffu, w.pos, 0);
-        if (alpha > 1) {
-            warp_build_and_store(s, alpha, w, lane);
-        } else {
-            for (int i{lane}; i < 256; i += 32) {
-                s.depth[i] = 0;
-                s.bits[i] = 0;
-            }
-            __syncwarp();
-        }
+    for (int off{16}; off > 0; off >>= 1) alpha = max(alpha, __shfl_xor_sync(kFull, alpha, off));
+    BitSink w{s.desc, 0, kDescBytes * 8, false};
+    if (!clustered && lane == 0) {
+        // Single-context prefix histogram header (src/bitstream/histogram_writer.cc:59-83).
+        w.put(1, 0);
+        w.put(1, 1);
+        put_uint_config(w, 4, 2, 0);
+        put_var_len_u16(w, static_cast<std::uint32_t>(alpha - 1));
     }
-    if (lane == 0) e.desc_bits[idx] = w.overflow ? 0u : w.pos;
+    if (clustered && lane == 0) e.ac_alpha[idx] = static_cast<std::uint32_t>(alpha);
+    if (alpha > 1) warp_build_and_store(s, alpha, w, lane);
+    __syncwarp();
+    std::uint32_t nbits{w.overflow ? 0u : w.pos};
+    nbits = __shfl_sync(kFull, nbits, 0);
+    if (lane == 0) e.desc_bits[idx] = nbits;
+    std::uint8_t* d{e.desc + idx * kDescBytes};
+    for (int i{lane}; i < kDescBytes; i += 32) d[i] = s.desc[i];
     for (int i{lane}; i < 256; i += 32) {
         dst_depth[i] = s.depth[i];
         dst_bits[i] = s.bits[i];
@@ -437,9 +488,26 @@ __global__ void __launch_bounds__(512) codes_kernel(EntropyDev e) {
 
 // ---- pass 3: bit lengths and scan ----------------------------------------------------
 
+__global__ void __launch_bounds__(kAcWarps * 32) ac_bits_kernel(EntropyDev e) {
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
+    const std::uint32_t stride{gridDim.x * kAcWarps};
+    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
+        const AcItem it{ac_item(e, item)};
+        std::uint32_t total{0};
+        if (it.n != 0) {
+            ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t) {
+                if (has) total += e.ac_depth[cl * 256 + sym] + nb;
+            });
+        }
+        total = warp_sum(total);
+        if (lane == 0) e.item_bits[item] = total;
+    }
+}
+
 struct BitsVisitor {
     const EntropyDev* e;
-    unsigned long long total;
+    std::uint32_t total;
     __device__ void blob(const std::uint8_t*, std::uint32_t nbits) { total += nbits; }
     __device__ void varlen(std::uint32_t v) {
         if (v == 0) {
@@ -453,18 +521,17 @@ struct BitsVisitor {
     __device__ void count_field(int, unsigned nbits) { total += nbits; }
     __device__ void epf(int g) { total += e->am_depth[g * 256]; }
     __device__ void first_block(int) {}
-    __device__ void token(int tab, int idx, std::uint32_t sym, std::uint32_t nb, std::uint32_t) {
-        const std::uint8_t* d{tab == kTabAc ? e->ac_depth : (tab == kTabDc ? e->dc_depth : e->am_depth)};
-        total += d[idx * 256 + sym] + nb;
+    __device__ void token(int tab, int g, std::uint32_t sym, std::uint32_t nb, std::uint32_t) {
+        total += (tab == kTabDc ? e->dc_depth : e->am_depth)[g * 256 + sym] + nb;
     }
 };
 
-__global__ void __launch_bounds__(256) bits_kernel(EntropyDev e) {
+__global__ void __launch_bounds__(256) misc_bits_kernel(EntropyDev e) {
     const std::uint32_t item{blockIdx.x * blockDim.x + threadIdx.x};
-    if (item >= e.total_items) return;
+    if (item >= e.ac_first) return;
     BitsVisitor v{&e, 0};
-    visit_item(e, item, v);
-    e.item_bits[item] = static_cast<std::uint32_t>(v.total);
+    visit_misc(e, item, v);
+    e.item_bits[item] = v.total;
 }
 
 // Exclusive scan of item_bits inside tiles of kScanTile items (1024 threads x 4).
@@ -483,17 +550,17 @@ __global__ void __launch_bounds__(1024) scan_tile_kernel(EntropyDev e) {
     std::uint32_t incl{local};
 #pragma unroll
     for (int off{1}; off < 32; off <<= 1) {
-        const std::uint32_t t{__shfl_up_sync(0xffffffffu, incl, off)};
+        const std::uint32_t t{__shfl_up_sync(kFull, incl, off)};
         if (lane >= off) incl += t;
     }
     if (lane == 31) warp_sums[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        std::uint32_t ws{warp_sums[lane]};
+        const std::uint32_t ws{warp_sums[lane]};
         std::uint32_t wi{ws};
 #pragma unroll
         for (int off{1}; off < 32; off <<= 1) {
-            const std::uint32_t t{__shfl_up_sync(0xffffffffu, wi, off)};
+            const std::uint32_t t{__shfl_up_sync(kFull, wi, off)};
             if (lane >= off) wi += t;
         }
         warp_sums[lane] = wi - ws;
@@ -521,7 +588,7 @@ __global__ void __launch_bounds__(1024) scan_top_kernel(EntropyDev e) {
         unsigned long long incl{x};
 #pragma unroll
         for (int off{1}; off < 32; off <<= 1) {
-            const unsigned long long t{__shfl_up_sync(0xffffffffu, incl, off)};
+            const unsigned long long t{__shfl_up_sync(kFull, incl, off)};
             if (lane >= off) incl += t;
         }
         if (lane == 31) warp_sums[warp] = incl;
@@ -531,7 +598,7 @@ __global__ void __launch_bounds__(1024) scan_top_kernel(EntropyDev e) {
             unsigned long long wi{ws};
 #pragma unroll
             for (int off{1}; off < 32; off <<= 1) {
-                const unsigned long long t{__shfl_up_sync(0xffffffffu, wi, off)};
+                const unsigned long long t{__shfl_up_sync(kFull, wi, off)};
                 if (lane >= off) wi += t;
             }
             warp_sums[lane] = wi - ws;
@@ -583,86 +650,106 @@ __device__ void put_u32(BitSink& w, const U32Dist* d, std::uint32_t value) {
     if (!d[best].direct) w.put(d[best].extra, value - d[best].v);
 }
 
-constexpr int kHeadBytes = 8192;
+constexpr int kLayoutThreads = 256;
 
-// Single thread: sizes the sections, writes the container framing, codestream
-// headers, frame header and TOC (src/bitstream/codestream.cc:57-135,
-// src/bitstream/container.cc:35-62) and places the sections.
-__global__ void layout_kernel(EntropyDev e) {
-    __shared__ __align__(16) std::uint8_t head[kHeadBytes];
-    if (threadIdx.x != 0) return;
-    for (int i{0}; i < kHeadBytes; ++i) head[i] = 0;
-    BitSink w{head, 0, kHeadBytes * 8, false};
-    const U32Dist dim[4]{{false, 1, 9}, {false, 1, 13}, {false, 1, 18}, {false, 1, 30}};
-    const U32Dist toc[4]{{false, 0, 10}, {false, 1024, 14}, {false, 17408, 22}, {false, 4211712, 30}};
-    w.put(8, 0xFF);
-    w.put(8, 0x0A);
-    const std::uint32_t W{static_cast<std::uint32_t>(e.width)};
-    const std::uint32_t H{static_cast<std::uint32_t>(e.height)};
-    const bool small{W % 8 == 0 && H % 8 == 0 && W <= 256 && H <= 256};
-    w.put(1, small ? 1 : 0);
-    if (small) w.put(5, H / 8 - 1); else put_u32(w, dim, H);
-    w.put(3, 0);
-    if (small) w.put(5, W / 8 - 1); else put_u32(w, dim, W);
-    w.put(1, 1);  // ImageMetadata all_default
-    w.put(1, 1);  // transform data all_default
-    w.pos = (w.pos + 7) & ~7u;
-    // FrameHeader: regular VarDCT frame, upsampling 1, x/b qm scale 2, one
-    // pass, no custom size, replace blending, last, unnamed, default loop filter.
-    w.put(1, 0);
-    w.put(2, 0);
-    w.put(1, 0);
-    w.put(2, 0);
-    w.put(2, 0);
-    w.put(3, 2);
-    w.put(3, 2);
-    w.put(2, 0);
-    w.put(1, 0);
-    w.put(2, 0);
-    w.put(1, 1);
-    w.put(2, 0);
-    w.put(1, 1);
-    w.put(2, 0);
-    // TOC without permutation.
-    w.put(1, 0);
-    w.pos = (w.pos + 7) & ~7u;
-    unsigned long long body{0};
-    for (int s{0}; s < e.nsec; ++s) {
+// Sizes the sections in parallel, then one thread writes the container
+// framing, codestream headers, frame header and TOC
+// (src/bitstream/codestream.cc:57-135, src/bitstream/container.cc:35-62) into
+// shared memory; the block copies them out and places the sections. Dynamic
+// shared memory: the section sizes, then the header (layout_head_bytes).
+__global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
+    extern __shared__ __align__(16) unsigned char layout_smem[];
+    __shared__ unsigned long long sh_total, sh_start, sh_status, sh_head;
+    auto* sec_bytes{reinterpret_cast<std::uint32_t*>(layout_smem)};
+    const std::uint32_t head_cap{layout_head_bytes(e.nsec)};
+    std::uint8_t* head{layout_smem + layout_sizes_bytes(e.nsec)};
+    const int tid{static_cast<int>(threadIdx.x)};
+    for (std::uint32_t i{static_cast<std::uint32_t>(tid)}; i < head_cap; i += kLayoutThreads) head[i] = 0;
+    for (int s{tid}; s < e.nsec; s += kLayoutThreads) {
         const Section sec{e.sections[s]};
         const unsigned long long bits{prefix_at(e, sec.first + sec.count) - prefix_at(e, sec.first)};
-        const unsigned long long bytes{(bits + 7) / 8};
-        put_u32(w, toc, static_cast<std::uint32_t>(bytes));
-        e.sec_pos[s] = body;  // relative to the body start for now
-        body += bytes;
+        sec_bytes[s] = static_cast<std::uint32_t>((bits + 7) / 8);
     }
-    w.pos = (w.pos + 7) & ~7u;
-    const unsigned long long head_bytes{w.pos / 8};
-    const unsigned long long cs{head_bytes + body};
-    const bool large{cs >= 0x100000000ull - 8};
-    const unsigned long long framing{32ull + (large ? 16 : 8)};
-    const unsigned long long total{framing + cs};
-    unsigned long long status{w.overflow ? 2ull : 0ull};
-    if (total > e.out_capacity) status = 1;
-    e.result[0] = total;
-    e.result[1] = framing + head_bytes;
-    e.result[2] = status;
-    if (status != 0) return;
-    const std::uint8_t hdr[32]{0, 0, 0, 0x0c, 'J', 'X', 'L', ' ', 0x0d, 0x0a, 0x87, 0x0a, 0, 0, 0, 0x14,
-                               'f', 't', 'y', 'p', 'j', 'x', 'l', ' ', 0, 0, 0, 0, 'j', 'x', 'l', ' '};
-    for (int i{0}; i < 32; ++i) e.out[i] = hdr[i];
-    std::size_t at{32};
-    const unsigned long long box{cs + (large ? 16 : 8)};
-    const std::uint32_t sf{large ? 1u : static_cast<std::uint32_t>(box)};
-    for (int i{0}; i < 4; ++i) e.out[at++] = static_cast<std::uint8_t>(sf >> (8 * (3 - i)));
-    e.out[at++] = 'j';
-    e.out[at++] = 'x';
-    e.out[at++] = 'l';
-    e.out[at++] = 'c';
-    if (large) {
-        for (int i{0}; i < 8; ++i) e.out[at++] = static_cast<std::uint8_t>(box >> (8 * (7 - i)));
+    __syncthreads();
+    if (tid == 0) {
+        BitSink w{head, 0, head_cap * 8, false};
+        const U32Dist dim[4]{{false, 1, 9}, {false, 1, 13}, {false, 1, 18}, {false, 1, 30}};
+        const U32Dist toc[4]{{false, 0, 10}, {false, 1024, 14}, {false, 17408, 22}, {false, 4211712, 30}};
+        w.put(8, 0xFF);
+        w.put(8, 0x0A);
+        const std::uint32_t W{static_cast<std::uint32_t>(e.width)};
+        const std::uint32_t H{static_cast<std::uint32_t>(e.height)};
+        const bool small{W % 8 == 0 && H % 8 == 0 && W <= 256 && H <= 256};
+        w.put(1, small ? 1 : 0);
+        if (small) w.put(5, H / 8 - 1); else put_u32(w, dim, H);
+        w.put(3, 0);
+        if (small) w.put(5, W / 8 - 1); else put_u32(w, dim, W);
+        w.put(1, 1);  // ImageMetadata all_default
+        w.put(1, 1);  // transform data all_default
+        w.pos = (w.pos + 7) & ~7u;
+        // FrameHeader: regular VarDCT frame, upsampling 1, x/b qm scale 2, one
+        // pass, no custom size, replace blending, last, unnamed, default loop filter.
+        w.put(1, 0);
+        w.put(2, 0);
+        w.put(1, 0);
+        w.put(2, 0);
+        w.put(2, 0);
+        w.put(3, 2);
+        w.put(3, 2);
+        w.put(2, 0);
+        w.put(1, 0);
+        w.put(2, 0);
+        w.put(1, 1);
+        w.put(2, 0);
+        w.put(1, 1);
+        w.put(2, 0);
+        w.put(1, 0);  // TOC without permutation
+        w.pos = (w.pos + 7) & ~7u;
+        unsigned long long body{0};
+        for (int s{0}; s < e.nsec; ++s) {
+            put_u32(w, toc, sec_bytes[s]);
+            body += sec_bytes[s];
+        }
+        w.pos = (w.pos + 7) & ~7u;
+        const unsigned long long head_bytes{w.pos / 8};
+        const unsigned long long cs{head_bytes + body};
+        const bool large{cs >= 0x100000000ull - 8};
+        const unsigned long long framing{32ull + (large ? 16 : 8)};
+        sh_total = framing + cs;
+        sh_head = head_bytes;
+        sh_start = framing + head_bytes;
+        sh_status = w.overflow ? 2ull : (sh_total > e.out_capacity ? 1ull : 0ull);
+        e.result[0] = sh_total;
+        e.result[1] = sh_start;
+        e.result[2] = sh_status;
+        if (sh_status == 0) {
+            const std::uint8_t hdr[32]{0, 0, 0, 0x0c, 'J', 'X', 'L', ' ', 0x0d, 0x0a, 0x87, 0x0a, 0, 0, 0, 0x14,
+                                       'f', 't', 'y', 'p', 'j', 'x', 'l', ' ', 0, 0, 0, 0, 'j', 'x', 'l', ' '};
+            for (int i{0}; i < 32; ++i) e.out[i] = hdr[i];
+            std::size_t at{32};
+            const unsigned long long box{cs + (large ? 16 : 8)};
+            const std::uint32_t sf{large ? 1u : static_cast<std::uint32_t>(box)};
+            for (int i{0}; i < 4; ++i) e.out[at++] = static_cast<std::uint8_t>(sf >> (8 * (3 - i)));
+            e.out[at++] = 'j';
+            e.out[at++] = 'x';
+            e.out[at++] = 'l';
+            e.out[at++] = 'c';
+            if (large) {
+                for (int i{0}; i < 8; ++i) e.out[at++] = static_cast<std::uint8_t>(box >> (8 * (7 - i)));
+            }
+            unsigned long long pos{sh_start};
+            for (int s{0}; s < e.nsec; ++s) {
+                e.sec_pos[s] = pos;
+                pos += sec_bytes[s];
+            }
+        }
     }
-    for (unsigned long long i{0}; i < head_bytes; ++i) e.out[at++] = head[i];
-    for (int s{0}; s < e.nsec; ++s) e.sec_pos[s] += framing + head_bytes;
+    __syncthreads();
+    if (sh_status != 0) return;
+    const unsigned long long framing{sh_start - sh_head};
+    for (unsigned long long i{static_cast<unsigned long long>(tid)}; i < sh_head; i += kLayoutThreads) {
+        e.out[framing + i] = head[i];
+    }
 }
 
 __global__ void zero_body_kernel(EntropyDev e) {
@@ -682,6 +769,51 @@ __global__ void zero_body_kernel(EntropyDev e) {
 
 // ---- pass 5: emission ------------------------------------------------------------
 
+// ORs `n` (<= 32) bits of `v` into the zeroed output at bit position `pos`.
+__device__ __forceinline__ void put_bits_at(unsigned int* words, unsigned long long pos, std::uint32_t n,
+                                            std::uint32_t v) {
+    while (n > 0) {
+        const unsigned long long wi{pos >> 5};
+        const std::uint32_t off{static_cast<std::uint32_t>(pos & 31)};
+        const std::uint32_t take{n < 32 - off ? n : 32 - off};
+        const std::uint32_t chunk{take == 32 ? v : (v & ((1u << take) - 1u))};
+        atomicOr(&words[wi], chunk << off);
+        v = take == 32 ? 0 : v >> take;
+        n -= take;
+        pos += take;
+    }
+}
+
+__global__ void __launch_bounds__(kAcWarps * 32) ac_emit_kernel(EntropyDev e) {
+    if (e.result[2] != 0) return;
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
+    const std::uint32_t stride{gridDim.x * kAcWarps};
+    auto* words{reinterpret_cast<unsigned int*>(e.out)};
+    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
+        const AcItem it{ac_item(e, item)};
+        if (it.n == 0) continue;
+        const Section sec{e.sections[it.section]};
+        unsigned long long base{e.sec_pos[it.section] * 8 + (prefix_at(e, item) - prefix_at(e, sec.first))};
+        ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
+            const std::uint32_t d{has ? e.ac_depth[cl * 256 + sym] : 0u};
+            const std::uint32_t tb{has ? d + nb : 0u};
+            std::uint32_t incl{tb};
+#pragma unroll
+            for (int off{1}; off < 32; off <<= 1) {
+                const std::uint32_t t{__shfl_up_sync(kFull, incl, off)};
+                if (lane >= off) incl += t;
+            }
+            if (has) {
+                const unsigned long long at{base + incl - tb};
+                put_bits_at(words, at, d, e.ac_bits[cl * 256 + sym]);
+                if (nb) put_bits_at(words, at + d, nb, bits);
+            }
+            base += __shfl_sync(kFull, incl, 31);
+        });
+    }
+}
+
 struct EmitVisitor {
     const EntropyDev* e;
     unsigned int* words;
@@ -689,19 +821,16 @@ struct EmitVisitor {
     __device__ void put(std::uint32_t n, std::uint32_t v) {
         if (n == 0) return;
         if (n < 32) v &= (1u << n) - 1u;
-        while (n > 0) {
-            const unsigned long long wi{pos >> 5};
-            const std::uint32_t off{static_cast<std::uint32_t>(pos & 31)};
-            const std::uint32_t take{n < 32 - off ? n : 32 - off};
-            const std::uint32_t chunk{take == 32 ? v : (v & ((1u << take) - 1u))};
-            atomicOr(&words[wi], chunk << off);
-            v = take == 32 ? 0 : v >> take;
-            n -= take;
-            pos += take;
-        }
+        put_bits_at(words, pos, n, v);
+        pos += n;
     }
     __device__ void blob(const std::uint8_t* b, std::uint32_t nbits) {
         std::uint32_t i{0};
+        for (; i + 32 <= nbits; i += 32) {
+            put(32, static_cast<std::uint32_t>(b[i >> 3]) | (static_cast<std::uint32_t>(b[(i >> 3) + 1]) << 8) |
+                        (static_cast<std::uint32_t>(b[(i >> 3) + 2]) << 16) |
+                        (static_cast<std::uint32_t>(b[(i >> 3) + 3]) << 24));
+        }
         for (; i + 8 <= nbits; i += 8) put(8, b[i >> 3]);
         if (i < nbits) put(nbits - i, b[i >> 3]);
     }
@@ -719,282 +848,39 @@ struct EmitVisitor {
     __device__ void count_field(int g, unsigned nbits) { put(nbits, e->fb_count[g] - 1); }
     __device__ void epf(int g) { put(e->am_depth[g * 256], e->am_bits[g * 256]); }
     __device__ void first_block(int) {}
-    __device__ void token(int tab, int idx, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
-        const std::uint8_t* d{tab == kTabAc ? e->ac_depth : (tab == kTabDc ? e->dc_depth : e->am_depth)};
-        const std::uint16_t* c{tab == kTabAc ? e->ac_bits : (tab == kTabDc ? e->dc_bits : e->am_bits)};
-        put(d[idx * 256 + sym], c[idx * 256 + sym]);
+    __device__ void token(int tab, int g, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
+        const std::uint8_t* d{tab == kTabDc ? e->dc_depth : e->am_depth};
+        const std::uint16_t* c{tab == kTabDc ? e->dc_bits : e->am_bits};
+        put(d[g * 256 + sym], c[g * 256 + sym]);
         if (nb) put(nb, bits);
     }
 };
 
-__global__ void __launch_bounds__(256) emit_kernel(EntropyDev e) {
+__global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
     if (e.result[2] != 0) return;
     const std::uint32_t item{blockIdx.x * blockDim.x + threadIdx.x};
-    if (item >= e.total_items) return;
-    const int s{find_section(e.sections, e.nsec, item)};
+    if (item >= e.ac_first) return;
+    const int s{find_section(e.sections, 0, misc_hi(e), item)};
     const Section sec{e.sections[s]};
     const unsigned long long rel{prefix_at(e, item) - prefix_at(e, sec.first)};
     EmitVisitor v{&e, reinterpret_cast<unsigned int*>(e.out), e.sec_pos[s] * 8 + rel};
-    visit_item(e, item, v);
+    visit_misc(e, item, v);
 }
 
-// ---- host-side constant blobs ------------------------------------------------------
-
-struct HostBits {
-    std::vector<std::uint8_t> buf;
-    BitSink w;
-    HostBits() : buf(1 << 16, 0), w{nullptr, 0, (1u << 16) * 8, false} { w.buf = buf.data(); }
-    std::vector<std::uint8_t> bytes() const {
-        return std::vector<std::uint8_t>(buf.begin(), buf.begin() + (w.pos + 7) / 8);
+int sm_count() {
+    int dev{0};
+    int sms{0};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        sms = 148;
     }
-};
-
-// Single-histogram description with the serial builder (small alphabets).
-void host_prefix_histograms(BitSink& w, const std::uint32_t* hist, int length, int num_contexts,
-                            std::uint32_t se, std::uint32_t msb, std::uint32_t lsb, std::uint8_t* depth,
-                            std::uint16_t* bits) {
-    w.put(1, 0);
-    if (num_contexts > 1) {
-        w.put(1, 1);
-        w.put(2, 0);
-    }
-    w.put(1, 1);
-    put_uint_config(w, se, msb, lsb);
-    put_var_len_u16(w, static_cast<std::uint32_t>(length - 1));
-    for (int i{0}; i < length; ++i) {
-        depth[i] = 0;
-        bits[i] = 0;
-    }
-    if (length > 1) {
-        std::vector<HuffNode> pool(2 * length + 4);
-        std::vector<std::uint8_t> level(2 * length + 4);
-        build_and_store_serial(hist, length, depth, bits, w, pool.data(), level.data());
-    }
+    return sms;
 }
-
-// Hybrid-uint split with an arbitrary configuration.
-void host_hybrid(std::uint32_t v, std::uint32_t se, std::uint32_t msb, std::uint32_t lsb,
-                 std::uint32_t& tok, std::uint32_t& nb, std::uint32_t& bits) {
-    const std::uint32_t split{1u << se};
-    if (v < split) {
-        tok = v;
-        nb = 0;
-        bits = 0;
-        return;
-    }
-    std::uint32_t n{31};
-    while (!((v >> n) & 1u)) --n;
-    const std::uint32_t m{v - (1u << n)};
-    tok = split + ((n - se) << (msb + lsb)) + ((m >> (n - msb)) << lsb) + (m & ((1u << lsb) - 1u));
-    nb = n - msb - lsb;
-    bits = (v >> lsb) & ((1u << nb) - 1u);
-}
-
-// Complex context map (src/bitstream/context_map.cc:127-164).
-void host_context_map_complex(BitSink& w, const std::vector<std::uint8_t>& map, bool mtf) {
-    std::vector<std::uint8_t> sym(map.size());
-    std::uint8_t order[256];
-    for (int i{0}; i < 256; ++i) order[i] = static_cast<std::uint8_t>(i);
-    for (std::size_t i{0}; i < map.size(); ++i) {
-        if (!mtf) {
-            sym[i] = map[i];
-            continue;
-        }
-        int r{0};
-        while (order[r] != map[i]) ++r;
-        sym[i] = static_cast<std::uint8_t>(r);
-        const std::uint8_t v{order[r]};
-        for (; r > 0; --r) order[r] = order[r - 1];
-        order[0] = v;
-    }
-    std::uint32_t hist[16]{};
-    for (std::uint8_t s : sym) {
-        std::uint32_t t, nb, b;
-        host_hybrid(s, 2, 0, 1, t, nb, b);
-        ++hist[t];
-    }
-    int alpha{1};
-    for (int i{0}; i < 16; ++i) {
-        if (hist[i]) alpha = i + 1;
-    }
-    w.put(1, 0);
-    w.put(1, mtf ? 1 : 0);
-    std::uint8_t depth[16];
-    std::uint16_t bits[16];
-    host_prefix_histograms(w, hist, alpha, 1, 2, 0, 1, depth, bits);
-    for (std::uint8_t s : sym) {
-        std::uint32_t t, nb, b;
-        host_hybrid(s, 2, 0, 1, t, nb, b);
-        w.put(depth[t], bits[t]);
-        if (nb) w.put(nb, b);
-    }
-}
-
-// Modular group header + single-leaf tree (src/bitstream/frame_assembly.cc:150-175).
-void host_modular_tree(BitSink& w, bool gradient) {
-    w.put(1, 0);
-    w.put(1, 1);
-    w.put(2, 0);
-    const std::uint32_t tokens[5]{0, gradient ? 5u : 0u, 0, 0, 0};
-    std::uint32_t hist[16]{};
-    int len{1};
-    for (std::uint32_t t : tokens) {
-        ++hist[t];
-        len = std::max(len, static_cast<int>(t) + 1);
-    }
-    std::uint8_t depth[16];
-    std::uint16_t bits[16];
-    host_prefix_histograms(w, hist, len, 6, 4, 2, 0, depth, bits);
-    for (std::uint32_t t : tokens) w.put(depth[t], bits[t]);
-}
-
-void append_bits(BitSink& dst, const BitSink& src) { dst.put_bits(src.buf, src.pos); }
 
 }  // namespace
 
-std::size_t worst_case_output(std::uint32_t width, std::uint32_t height) {
-    const std::size_t bw{width / 8u};
-    const std::size_t bh{height / 8u};
-    const std::size_t nac{((bw + 31) / 32) * ((bh + 31) / 32)};
-    const std::size_t ndc{((bw + 255) / 256) * ((bh + 255) / 256)};
-    return 3 * bw * bh * 384 + 48 * bw * bh + (nac + ndc) * 2048 + 16384;
-}
-
-std::vector<std::uint8_t> dc_global_bits(std::uint32_t global_scale, std::uint32_t quant_dc,
-                                         std::uint32_t* nbits) {
-    HostBits hb;
-    BitSink& w{hb.w};
-    auto u32 = [&](const std::uint32_t (*d)[3], std::uint32_t value) {
-        std::uint32_t best{0};
-        std::uint32_t best_bits{64};
-        for (std::uint32_t s{0}; s < 4; ++s) {
-            if (d[s][0]) {
-                if (d[s][1] == value) {
-                    best = s;
-                    best_bits = 2;
-                    break;
-                }
-                continue;
-            }
-            if (value < d[s][1] || static_cast<unsigned long long>(value) >=
-                                       static_cast<unsigned long long>(d[s][1]) + (1ull << d[s][2])) {
-                continue;
-            }
-            if (2 + d[s][2] < best_bits) {
-                best = s;
-                best_bits = 2 + d[s][2];
-            }
-        }
-        w.put(2, best);
-        if (!d[best][0]) w.put(d[best][2], value - d[best][1]);
-    };
-    const std::uint32_t gs_enc[4][3]{{0, 1, 11}, {0, 2049, 11}, {0, 4097, 12}, {0, 8193, 16}};
-    const std::uint32_t qdc_enc[4][3]{{1, 16, 0}, {0, 1, 5}, {0, 1, 8}, {0, 1, 16}};
-    w.put(1, 1);
-    u32(gs_enc, global_scale);
-    u32(qdc_enc, quant_dc);
-    w.put(1, 1);
-    w.put(1, 1);
-    w.put(1, 0);
-    w.pos = (w.pos + 7) & ~7u;
-    *nbits = w.pos;
-    return hb.bytes();
-}
-
-EntropyHostPlan entropy_plan(int width, int height) {
-    EntropyHostPlan p;
-    const int bw{width / 8};
-    const int bh{height / 8};
-    const int xg{(bw + 31) / 32};
-    const int yg{(bh + 31) / 32};
-    const int xdg{(bw + 255) / 256};
-    const int ydg{(bh + 255) / 256};
-    std::uint32_t at{0};
-    p.sections.push_back({at, 1, kSecDcGlobal, 0});
-    at += 1;
-    for (int g{0}; g < xdg * ydg; ++g) {
-        const int gw{std::min(256, bw - (g % xdg) * 256)};
-        const int gh{std::min(256, bh - (g / xdg) * 256)};
-        const std::uint32_t n{static_cast<std::uint32_t>(gw * gh)};
-        const std::uint32_t cwch{static_cast<std::uint32_t>(((gw + 7) / 8) * ((gh + 7) / 8))};
-        const std::uint32_t cnt{5 + 6 * n + 2 * cwch};
-        p.sections.push_back({at, cnt, kSecDcGroup, g});
-        at += cnt;
-    }
-    p.sections.push_back({at, 65, kSecAcGlobal, 0});
-    at += 65;
-    for (int g{0}; g < xg * yg; ++g) {
-        const int gw{std::min(32, bw - (g % xg) * 32)};
-        const int gh{std::min(32, bh - (g / xg) * 32)};
-        const std::uint32_t cnt{static_cast<std::uint32_t>(3 * gw * gh)};
-        p.sections.push_back({at, cnt, kSecAcGroup, g});
-        at += cnt;
-    }
-    p.total_items = at;
-
-    {
-        HostBits hb;
-        hb.w.put(2, 0);  // extra_precision
-        host_modular_tree(hb.w, true);
-        p.pre_const = hb.bytes();
-        p.pre_const_bits = hb.w.pos;
-    }
-    {
-        HostBits hb;
-        host_modular_tree(hb.w, false);
-        p.mid_const = hb.bytes();
-        p.mid_const_bits = hb.w.pos;
-    }
-    {
-        HostBits hb;
-        BitSink& w{hb.w};
-        w.put(1, 1);                                                       // dequant all_default
-        w.put(ceil_log2_u(static_cast<std::uint32_t>(xg * yg)), 0);        // num_histograms - 1
-        w.put(2, 2);                                                       // used_orders = 0
-        w.put(1, 0);                                                       // lz77 disabled
-        std::vector<std::uint8_t> map(kNumAcContexts);
-        for (int i{0}; i < kNumAcContexts; ++i) {
-            map[i] = static_cast<std::uint8_t>(context_cluster(static_cast<std::uint32_t>(i)));
-        }
-        HostBits a;
-        HostBits b;
-        host_context_map_complex(a.w, map, false);
-        host_context_map_complex(b.w, map, true);
-        append_bits(w, b.w.pos < a.w.pos ? b.w : a.w);
-        w.put(1, 1);  // use_prefix_code
-        for (int c{0}; c < kNumClusters; ++c) put_uint_config(w, 4, 2, 0);
-        p.ac_prefix = hb.bytes();
-        p.ac_prefix_bits = w.pos;
-    }
-    // Natural coefficient orders (src/coeff_order.cc:10-43), concatenated 8|16|32.
-    for (int n : {8, 16, 32}) {
-        const int cx{n / 8};
-        std::vector<std::uint16_t> out(static_cast<std::size_t>(n) * n);
-        int cur{cx * cx};
-        for (int i{0}; i < n; ++i) {
-            for (int jj{0}; jj <= i; ++jj) {
-                int x{jj};
-                int y{i - jj};
-                if (i & 1) std::swap(x, y);
-                const int val{(x < cx && y < cx) ? y * cx + x : cur++};
-                out[val] = static_cast<std::uint16_t>(y * n + x);
-            }
-        }
-        for (int ip{n - 1}; ip > 0; --ip) {
-            const int i{ip - 1};
-            for (int jj{0}; jj <= i; ++jj) {
-                int x{n - 1 - (i - jj)};
-                int y{n - 1 - jj};
-                if (i & 1) std::swap(x, y);
-                out[cur++] = static_cast<std::uint16_t>(y * n + x);
-            }
-        }
-        p.order.insert(p.order.end(), out.begin(), out.end());
-    }
-    return p;
-}
-
 bool entropy_launch(const EntropyDev& e, void* stream) {
+    if (e.nsec > kMaxSections) return false;
     cudaStream_t st{static_cast<cudaStream_t>(stream)};
     if (cudaMemsetAsync(e.ac_hist, 0, kNumClusters * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
         cudaMemsetAsync(e.dc_hist, 0, static_cast<std::size_t>(e.ndc) * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
@@ -1002,22 +888,33 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
         cudaMemsetAsync(e.fb_count, 0, static_cast<std::size_t>(e.ndc) * sizeof(std::uint32_t), st) != cudaSuccess) {
         return false;
     }
-    const unsigned items{e.total_items};
-    hist_kernel<<<(items + 255) / 256, 256, 0, st>>>(e);
-    const std::size_t code_smem{sizeof(WarpCodeSmem) * 16};
-    codes_kernel<<<2 + e.ndc, 512, code_smem, st>>>(e);
-    bits_kernel<<<(items + 255) / 256, 256, 0, st>>>(e);
+    static thread_local int sms{0};
+    if (sms == 0) sms = sm_count();
+    const unsigned misc{(e.ac_first + 255) / 256};
+    const unsigned ac_items{e.total_items - e.ac_first};
+    const unsigned ac_blocks{(ac_items + kAcWarps - 1) / kAcWarps};
+    const unsigned hist_grid{min(ac_blocks, static_cast<unsigned>(sms) * 4)};
+    const unsigned ac_grid{min(ac_blocks, static_cast<unsigned>(sms) * 8)};
+    const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
+    ac_hist_kernel<<<hist_grid, kAcWarps * 32, 0, st>>>(e);
+    misc_hist_kernel<<<misc, 256, 0, st>>>(e);
+    codes_kernel<<<2 + e.ndc, 512, sizeof(WarpCodeSmem) * 16, st>>>(e);
+    ac_bits_kernel<<<ac_grid, kAcWarps * 32, 0, st>>>(e);
+    misc_bits_kernel<<<misc, 256, 0, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
-    layout_kernel<<<1, 32, 0, st>>>(e);
+    layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
     zero_body_kernel<<<296, 256, 0, st>>>(e);
-    emit_kernel<<<(items + 255) / 256, 256, 0, st>>>(e);
+    ac_emit_kernel<<<ac_grid, kAcWarps * 32, 0, st>>>(e);
+    misc_emit_kernel<<<misc, 256, 0, st>>>(e);
     return cudaGetLastError() == cudaSuccess;
 }
 
 bool entropy_kernels_init() {
     return cudaFuncSetAttribute(codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(WarpCodeSmem) * 16)) == cudaSuccess;
+                                static_cast<int>(sizeof(WarpCodeSmem) * 16)) == cudaSuccess &&
+           cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kLayoutSmemLimit)) == cudaSuccess;
 }
 
 }  // namespace jxb

@@ -13,6 +13,8 @@
 //   4. a layout CTA sizes every section, writes the container, headers and
 //      TOC, and places the sections;
 //   5. an emit pass writes every item's bits at its final position.
+// Passes 1, 3 and 5 run as two kernels each: one warp per AC block-channel
+// (items from ac_first on) and one thread per other item.
 #pragma once
 
 #include <cstddef>
@@ -36,6 +38,7 @@ struct EntropyDev {
     // geometry
     int width, height, bw, bh, nblocks, xg, nac, xdg, ndc, cmw, nsec;
     std::uint32_t total_items;
+    std::uint32_t ac_first;          // first item of the first AcGroup; AC block-channels follow
     std::uint32_t num_tiles;         // scan tiles of kScanTile items
     const Section* sections;
 
@@ -87,11 +90,24 @@ struct EntropyDev {
 constexpr int kDescBytes = 256;
 constexpr int kScanTile = 4096;
 
+// Shared memory of the layout kernel: one 32-bit size per section, then the
+// codestream header, which is at most 64 bytes before the TOC plus 4 bytes
+// per TOC entry.
+__host__ __device__ constexpr std::uint32_t layout_sizes_bytes(int nsec) {
+    return (static_cast<std::uint32_t>(nsec) * 4 + 15) & ~15u;
+}
+__host__ __device__ constexpr std::uint32_t layout_head_bytes(int nsec) {
+    return 64 + static_cast<std::uint32_t>(nsec) * 4;
+}
+constexpr std::uint32_t kLayoutSmemLimit = 200 * 1024;
+constexpr int kMaxSections = static_cast<int>(kLayoutSmemLimit / 8) - 16;
+
 // Builds the constant header blobs and section table for a geometry. Fills the
 // host-side vectors; the caller uploads them.
 struct EntropyHostPlan {
     std::vector<Section> sections;
     std::uint32_t total_items{0};
+    std::uint32_t ac_first{0};
     std::vector<std::uint8_t> pre_const;
     std::uint32_t pre_const_bits{0};
     std::vector<std::uint8_t> mid_const;

@@ -124,6 +124,7 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
     e.cmw = (bw + 7) / 8;
     e.nsec = static_cast<int>(plan.sections.size());
     e.total_items = plan.total_items;
+    e.ac_first = plan.ac_first;
     e.num_tiles = tiles;
     auto* sections{c.take<jxb::Section>(plan.sections.size())};
     auto* order{c.take<std::uint16_t>(plan.order.size())};
