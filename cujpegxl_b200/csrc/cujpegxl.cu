@@ -153,6 +153,7 @@ bool allocate(cujpegxl_encoder* e) {
     const std::size_t o_nzn{a.take(3 * nb)};
     const std::size_t o_nzc{a.take(3 * nb * 2)};
     const std::size_t o_sec{a.take(plan.sections.size() * sizeof(jxb::Section))};
+    const std::size_t o_str{a.take(plan.stripes.size() * sizeof(jxb::Stripe))};
     const std::size_t o_ord{a.take(plan.order.size() * 2)};
     const std::size_t o_pre{a.take(plan.pre_const.size())};
     const std::size_t o_mid{a.take(plan.mid_const.size())};
@@ -222,6 +223,8 @@ bool allocate(cujpegxl_encoder* e) {
     ed.ac_first = plan.ac_first;
     ed.num_tiles = tiles;
     ed.sections = reinterpret_cast<const jxb::Section*>(b + o_sec);
+    ed.stripes = reinterpret_cast<const jxb::Stripe*>(b + o_str);
+    ed.nstripes = static_cast<int>(plan.stripes.size());
     ed.ac = fo.ac;
     ed.dc = fo.dc;
     ed.acs = fo.acs;
@@ -263,6 +266,8 @@ bool allocate(cujpegxl_encoder* e) {
     e->nv12_dev = b + o_nv12;
 
     bool ok{cudaMemcpy(b + o_sec, plan.sections.data(), plan.sections.size() * sizeof(jxb::Section),
+                       cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(b + o_str, plan.stripes.data(), plan.stripes.size() * sizeof(jxb::Stripe),
                        cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(b + o_ord, plan.order.data(), plan.order.size() * 2, cudaMemcpyHostToDevice) ==
                 cudaSuccess &&

@@ -169,68 +169,147 @@ __device__ void visit_misc(const EntropyDev& e, std::uint32_t item, V& v) {
     v.token(kTabAm, g, tok, nb, bits);
 }
 
-// ---- AC block-channels, one warp per item ---------------------------------------------
+// ---- AC block-channels: one CTA per stripe staged in shared memory -------------------
 
-struct AcItem {
-    int n;                 // transform side, 0 for a covered block (no tokens)
-    int c;                 // plane 0=X, 1=Y, 2=B
-    int bx, by;
-    std::uint32_t nz;      // non-zero AC count
-    int nz_cluster;        // cluster of the count token
-    int section;
+constexpr int kAcThreads = 256;
+constexpr int kAcWarps = kAcThreads / 32;
+constexpr int kStripeItems = 3 * kStripeRows * kAcGroupBlocks;  // 384
+constexpr int kRowSlots = kAcGroupBlocks * kCoeffsPerBlock;      // 2048
+// AC token symbols are hybrid-uint (4, 2, 0) tokens of values below 2^16
+// (packed int16 coefficients, counts up to 1008): at most 63.
+constexpr int kAcSymbols = 64;
+constexpr int kWindowWords = 4096;  // 16 KB of output bits assembled per CTA
+
+__device__ __forceinline__ unsigned long long prefix_at(const EntropyDev& e, std::uint32_t i) {
+    if (i >= e.total_items) return e.tile_off[e.num_tiles];
+    return e.tile_off[i / kScanTile] + e.item_pre[i];
+}
+
+// ORs `n` (<= 32) bits of `v` at bit position `pos` of a zeroed word array in
+// shared or global memory.
+__device__ __forceinline__ void put_bits_at(unsigned int* words, unsigned long long pos, std::uint32_t n,
+                                            std::uint32_t v) {
+    while (n > 0) {
+        const unsigned long long wi{pos >> 5};
+        const std::uint32_t off{static_cast<std::uint32_t>(pos & 31)};
+        const std::uint32_t take{n < 32 - off ? n : 32 - off};
+        const std::uint32_t chunk{take == 32 ? v : (v & ((1u << take) - 1u))};
+        if (chunk != 0) atomicOr(&words[wi], chunk << off);
+        v = take == 32 ? 0 : v >> take;
+        n -= take;
+        pos += take;
+    }
+}
+
+// A stripe's inputs in shared memory: the three coefficient planes of its
+// block rows (row stride kRowSlots), the natural orders, strategies and
+// non-zero counts (nzn row 0 is the block row above the stripe).
+struct StripeStage {
+    std::int16_t coef[3][kStripeRows][kRowSlots];
+    std::uint16_t order[64 + 256 + 1024];
+    std::uint16_t nzc[3][kStripeRows][kAcGroupBlocks];
+    std::uint8_t nzn[3][kStripeRows + 1][kAcGroupBlocks];
+    std::int8_t acs[kStripeRows][kAcGroupBlocks];
+    std::uint16_t active[kStripeItems];  // items with coefficient tokens
+    std::uint32_t aux[kStripeItems];     // per-item bits (bits pass) or bit offset (emit pass)
+    int nactive;
 };
 
-__device__ __forceinline__ AcItem ac_item(const EntropyDev& e, std::uint32_t item) {
-    AcItem it{};
-    it.section = find_section(e.sections, e.ndc + 2, e.nsec - 1, item);
-    const Section sec{e.sections[it.section]};
-    const std::uint32_t j{item - sec.first};
-    const GroupGeom gg{ac_group_geom(e, sec.group)};
-    const int bidx{static_cast<int>(j / 3)};
-    it.c = phys_channel(static_cast<int>(j % 3));
-    it.bx = gg.bx0 + bidx % gg.gw;
-    it.by = gg.by0 + bidx / gg.gw;
-    const std::size_t blk{static_cast<std::size_t>(it.by) * e.bw + it.bx};
-    it.n = e.acs[blk];
-    if (it.n == 0) return it;
-    const std::size_t cb{static_cast<std::size_t>(it.c) * e.nblocks};
-    it.nz = e.nzc[cb + blk];
-    const bool hl{it.bx > gg.bx0};
-    const bool ht{it.by > gg.by0};
-    const std::uint32_t top{ht ? e.nzn[cb + blk - e.bw] : 0u};
-    const std::uint32_t left{hl ? e.nzn[cb + blk - 1] : 0u};
-    it.nz_cluster = context_cluster(nonzero_context(predict_nonzeros(hl, ht, top, left), block_ctx(it.c, it.n)));
+__device__ void stage_stripe(const EntropyDev& e, const Stripe& st, const GroupGeom& gg, StripeStage& s) {
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int vpr{gg.gw * (kCoeffsPerBlock * 2 / 16)};  // 16-byte vectors per block row
+    for (int c{0}; c < 3; ++c) {
+        const std::int16_t* plane{e.ac + static_cast<std::size_t>(c) * e.nblocks * kCoeffsPerBlock};
+        for (int r{0}; r < st.rows; ++r) {
+            const std::size_t blk0{static_cast<std::size_t>(gg.by0 + st.r0 + r) * e.bw + gg.bx0};
+            const uint4* src{reinterpret_cast<const uint4*>(plane + blk0 * kCoeffsPerBlock)};
+            uint4* dst{reinterpret_cast<uint4*>(&s.coef[c][r][0])};
+            for (int v{tid}; v < vpr; v += kAcThreads) dst[v] = __ldg(&src[v]);
+        }
+    }
+    for (int i{tid}; i < (64 + 256 + 1024) / 2; i += kAcThreads) {
+        reinterpret_cast<std::uint32_t*>(s.order)[i] = __ldg(&reinterpret_cast<const std::uint32_t*>(e.order)[i]);
+    }
+    const int cells{st.rows * gg.gw};
+    for (int i{tid}; i < cells; i += kAcThreads) {
+        const int r{i / gg.gw};
+        const int x{i - r * gg.gw};
+        const std::size_t blk{static_cast<std::size_t>(gg.by0 + st.r0 + r) * e.bw + gg.bx0 + x};
+        s.acs[r][x] = e.acs[blk];
+        for (int c{0}; c < 3; ++c) {
+            const std::size_t cb{static_cast<std::size_t>(c) * e.nblocks + blk};
+            s.nzc[c][r][x] = e.nzc[cb];
+            s.nzn[c][r + 1][x] = e.nzn[cb];
+            if (r == 0) s.nzn[c][0][x] = st.r0 > 0 ? e.nzn[cb - e.bw] : 0;
+        }
+    }
+    if (tid == 0) s.nactive = 0;
+}
+
+// Stripe-local item j: block (bx, by) of the stripe, plane c.
+struct StripeItem {
+    int c, bx, by, n;
+    std::uint32_t nz;
+};
+
+__device__ __forceinline__ StripeItem stripe_item(const StripeStage& s, int gw, int j) {
+    StripeItem it;
+    const int bidx{j / 3};
+    it.c = phys_channel(j - 3 * bidx);
+    it.by = bidx / gw;
+    it.bx = bidx - it.by * gw;
+    it.n = s.acs[it.by][it.bx];
+    it.nz = it.n != 0 ? s.nzc[it.c][it.by][it.bx] : 0u;
     return it;
 }
 
-// Calls f(has, cluster, symbol, extra_bits, extra_value) once per step with
-// all 32 lanes (so f may use warp collectives): first the count token on
-// lane 0, then one coefficient token per lane per 32-position chunk of the
-// scan, in stream order. Replicates the sequential loop of
-// src/entropy.cu:653-680: a position is coded while non-zeros remain before it.
+// Count token of a non-covered item: cluster from the non-zero prediction of
+// the group-local top and left neighbours (src/entropy.cu:649-652).
+__device__ __forceinline__ void count_token(const StripeStage& s, const Stripe& st, const StripeItem& it, int& cl,
+                                            std::uint32_t& tok, std::uint32_t& nb, std::uint32_t& bits) {
+    const bool hl{it.bx > 0};
+    const bool ht{st.r0 + it.by > 0};
+    const std::uint32_t top{ht ? s.nzn[it.c][it.by][it.bx] : 0u};
+    const std::uint32_t left{hl ? s.nzn[it.c][it.by + 1][it.bx - 1] : 0u};
+    cl = context_cluster(nonzero_context(predict_nonzeros(hl, ht, top, left), block_ctx(it.c, it.n)));
+    hybrid_uint(it.nz, tok, nb, bits);
+}
+
+// Calls f(has, cluster, symbol, extra_bits, extra_value) with all 32 lanes
+// once per 32-position chunk of the item's scan, one coefficient token per
+// lane in stream order. Ballots give each lane the reference's sequential
+// state at its position (src/entropy.cu:653-680): a position is coded while
+// non-zeros remain before it, and its context uses that count and whether the
+// previous coefficient was non-zero.
 template <class F>
-__device__ void ac_warp_tokens(const EntropyDev& e, const AcItem& it, int lane, F&& f) {
-    {
-        std::uint32_t tok, nb, bits;
-        hybrid_uint(it.nz, tok, nb, bits);
-        f(lane == 0, it.nz_cluster, tok, nb, bits);
-    }
-    if (it.nz == 0) return;
+__device__ void coeff_tokens(const StripeStage& s, const StripeItem& it, int lane, F&& f) {
     const int n{it.n};
     const int side{n >> 3};
+    const int lside{side == 1 ? 0 : (side == 2 ? 1 : 2)};
     const std::uint32_t covered{static_cast<std::uint32_t>(side * side)};
     const std::uint32_t size{static_cast<std::uint32_t>(n * n)};
-    const std::uint32_t l2{n == 16 ? 2u : (n == 32 ? 4u : 0u)};
+    const std::uint32_t l2{static_cast<std::uint32_t>(2 * lside)};
     const int bctx{block_ctx(it.c, n)};
-    const std::uint16_t* ord{e.order + (n == 8 ? 0 : (n == 16 ? 64 : 320))};
-    const std::int16_t* plane{e.ac + static_cast<std::size_t>(it.c) * e.nblocks * kCoeffsPerBlock};
+    const std::uint16_t* ord{s.order + (n == 8 ? 0 : (n == 16 ? 64 : 320))};
+    const std::int16_t* plane{&s.coef[it.c][it.by][it.bx * kCoeffsPerBlock]};
     std::uint32_t remaining{it.nz};
     std::uint32_t prev{it.nz > size / 16 ? 0u : 1u};
     const unsigned below{(1u << lane) - 1u};
     for (std::uint32_t k0{covered}; k0 < size && remaining > 0; k0 += 32) {
         const std::uint32_t k{k0 + static_cast<std::uint32_t>(lane)};
         std::int32_t val{0};
-        if (k < size) val = plane[covered_slot(n, it.bx, it.by, e.bw, __ldg(&ord[k]))];
+        if (k < size) {
+            const int raw{ord[k]};
+            const int q{raw >> 6};
+            const int qy{q >> lside};
+            const int qx{q & (side - 1)};
+            // Transforms start at multiples of their size inside the group, so
+            // the covered blocks lie in the stripe; planes that break this
+            // layout read zeros instead of leaving the staged area.
+            if (it.by + qy < kStripeRows && it.bx + qx < kAcGroupBlocks) {
+                val = plane[qy * kRowSlots + qx * kCoeffsPerBlock + (raw & 63)];
+            }
+        }
         const unsigned nzmask{__ballot_sync(kFull, val != 0)};
         const std::uint32_t left{remaining - static_cast<std::uint32_t>(__popc(nzmask & below))};
         const std::uint32_t p{lane == 0 ? prev : ((nzmask >> (lane - 1)) & 1u)};
@@ -247,35 +326,56 @@ __device__ void ac_warp_tokens(const EntropyDev& e, const AcItem& it, int lane, 
     }
 }
 
-constexpr int kAcWarps = 8;
-
 __device__ __forceinline__ std::uint32_t warp_sum(std::uint32_t v) {
 #pragma unroll
     for (int off{16}; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
     return v;
 }
 
+__device__ __forceinline__ std::uint32_t warp_incl_scan(std::uint32_t v, int lane) {
+#pragma unroll
+    for (int off{1}; off < 32; off <<= 1) {
+        const std::uint32_t t{__shfl_up_sync(kFull, v, off)};
+        if (lane >= off) v += t;
+    }
+    return v;
+}
+
 // ---- pass 1: histograms ---------------------------------------------------------
 
-__global__ void __launch_bounds__(kAcWarps * 32) ac_hist_kernel(EntropyDev e) {
-    __shared__ std::uint32_t sh[kNumClusters * 256];
-    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) sh[i] = 0;
+__global__ void __launch_bounds__(kAcThreads) ac_hist_kernel(EntropyDev e) {
+    extern __shared__ __align__(16) unsigned char ac_smem[];
+    StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
+    std::uint32_t* hist{reinterpret_cast<std::uint32_t*>(ac_smem + sizeof(StripeStage))};  // [32][64]
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int lane{tid & 31};
+    const Stripe st{e.stripes[blockIdx.x]};
+    const GroupGeom gg{ac_group_geom(e, st.group)};
+    for (int i{tid}; i < kNumClusters * kAcSymbols; i += kAcThreads) hist[i] = 0;
+    stage_stripe(e, st, gg, s);
     __syncthreads();
-    const int lane{static_cast<int>(threadIdx.x) & 31};
-    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
-    const std::uint32_t stride{gridDim.x * kAcWarps};
-    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
-        const AcItem it{ac_item(e, item)};
+    const int nitems{3 * st.rows * gg.gw};
+    for (int j{tid}; j < nitems; j += kAcThreads) {
+        const StripeItem it{stripe_item(s, gg.gw, j)};
         if (it.n == 0) continue;
-        ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t, std::uint32_t) {
-            const unsigned key{has ? static_cast<unsigned>(cl * 256 + sym) : 0xffffffffu};
+        int cl;
+        std::uint32_t tok, nb, bits;
+        count_token(s, st, it, cl, tok, nb, bits);
+        atomicAdd(&hist[cl * kAcSymbols + tok], 1u);
+        if (it.nz != 0) s.active[atomicAdd(&s.nactive, 1)] = static_cast<std::uint16_t>(j);
+    }
+    __syncthreads();
+    for (int a{tid >> 5}; a < s.nactive; a += kAcWarps) {
+        const StripeItem it{stripe_item(s, gg.gw, s.active[a])};
+        coeff_tokens(s, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t, std::uint32_t) {
+            const unsigned key{has ? static_cast<unsigned>(cl * kAcSymbols + sym) : 0xffffffffu};
             const unsigned peers{__match_any_sync(kFull, key)};
-            if (has && (__ffs(peers) - 1) == lane) atomicAdd(&sh[key], static_cast<unsigned>(__popc(peers)));
+            if (has && (__ffs(peers) - 1) == lane) atomicAdd(&hist[key], static_cast<unsigned>(__popc(peers)));
         });
     }
     __syncthreads();
-    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) {
-        if (sh[i]) atomicAdd(&e.ac_hist[i], sh[i]);
+    for (int i{tid}; i < kNumClusters * kAcSymbols; i += kAcThreads) {
+        if (hist[i]) atomicAdd(&e.ac_hist[(i / kAcSymbols) * 256 + i % kAcSymbols], hist[i]);
     }
 }
 
@@ -488,21 +588,41 @@ __global__ void __launch_bounds__(512) codes_kernel(EntropyDev e) {
 
 // ---- pass 3: bit lengths and scan ----------------------------------------------------
 
-__global__ void __launch_bounds__(kAcWarps * 32) ac_bits_kernel(EntropyDev e) {
-    const int lane{static_cast<int>(threadIdx.x) & 31};
-    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
-    const std::uint32_t stride{gridDim.x * kAcWarps};
-    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
-        const AcItem it{ac_item(e, item)};
-        std::uint32_t total{0};
+__global__ void __launch_bounds__(kAcThreads) ac_bits_kernel(EntropyDev e) {
+    extern __shared__ __align__(16) unsigned char ac_smem[];
+    StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int lane{tid & 31};
+    const Stripe st{e.stripes[blockIdx.x]};
+    const GroupGeom gg{ac_group_geom(e, st.group)};
+    stage_stripe(e, st, gg, s);
+    __syncthreads();
+    const int nitems{3 * st.rows * gg.gw};
+    for (int j{tid}; j < nitems; j += kAcThreads) {
+        const StripeItem it{stripe_item(s, gg.gw, j)};
+        std::uint32_t b{0};
         if (it.n != 0) {
-            ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t) {
-                if (has) total += e.ac_depth[cl * 256 + sym] + nb;
-            });
+            int cl;
+            std::uint32_t tok, nb, bits;
+            count_token(s, st, it, cl, tok, nb, bits);
+            b = __ldg(&e.ac_depth[cl * 256 + tok]) + nb;
+            if (it.nz != 0) s.active[atomicAdd(&s.nactive, 1)] = static_cast<std::uint16_t>(j);
         }
-        total = warp_sum(total);
-        if (lane == 0) e.item_bits[item] = total;
+        s.aux[j] = b;
     }
+    __syncthreads();
+    for (int a{tid >> 5}; a < s.nactive; a += kAcWarps) {
+        const int j{s.active[a]};
+        const StripeItem it{stripe_item(s, gg.gw, j)};
+        std::uint32_t total{0};
+        coeff_tokens(s, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t) {
+            if (has) total += __ldg(&e.ac_depth[cl * 256 + sym]) + nb;
+        });
+        total = warp_sum(total);
+        if (lane == 0) s.aux[j] += total;
+    }
+    __syncthreads();
+    for (int j{tid}; j < nitems; j += kAcThreads) e.item_bits[st.item0 + j] = s.aux[j];
 }
 
 struct BitsVisitor {
@@ -612,10 +732,6 @@ __global__ void __launch_bounds__(1024) scan_top_kernel(EntropyDev e) {
     if (threadIdx.x == 0) e.tile_off[e.num_tiles] = carry;
 }
 
-__device__ __forceinline__ unsigned long long prefix_at(const EntropyDev& e, std::uint32_t i) {
-    if (i >= e.total_items) return e.tile_off[e.num_tiles];
-    return e.tile_off[i / kScanTile] + e.item_pre[i];
-}
 
 // ---- pass 4: layout --------------------------------------------------------------
 
@@ -769,49 +885,91 @@ __global__ void zero_body_kernel(EntropyDev e) {
 
 // ---- pass 5: emission ------------------------------------------------------------
 
-// ORs `n` (<= 32) bits of `v` into the zeroed output at bit position `pos`.
-__device__ __forceinline__ void put_bits_at(unsigned int* words, unsigned long long pos, std::uint32_t n,
-                                            std::uint32_t v) {
-    while (n > 0) {
-        const unsigned long long wi{pos >> 5};
-        const std::uint32_t off{static_cast<std::uint32_t>(pos & 31)};
-        const std::uint32_t take{n < 32 - off ? n : 32 - off};
-        const std::uint32_t chunk{take == 32 ? v : (v & ((1u << take) - 1u))};
-        atomicOr(&words[wi], chunk << off);
-        v = take == 32 ? 0 : v >> take;
-        n -= take;
-        pos += take;
+// Copies a window of `nwords` assembled words to global word w0 onward. The
+// first and last words can share bits with neighbouring items and are ORed
+// in; every word between lies wholly inside the window's bit range and is
+// stored.
+__device__ void flush_window(const unsigned int* win, int nwords, unsigned int* gwords, unsigned long long w0) {
+    for (int i{static_cast<int>(threadIdx.x)}; i < nwords; i += blockDim.x) {
+        const unsigned int v{win[i]};
+        if (i == 0 || i == nwords - 1) {
+            if (v != 0) atomicOr(&gwords[w0 + i], v);
+        } else {
+            gwords[w0 + i] = v;
+        }
     }
 }
 
-__global__ void __launch_bounds__(kAcWarps * 32) ac_emit_kernel(EntropyDev e) {
+// Writes a stripe's tokens. The stripe's bits are contiguous in its section;
+// they are assembled in a shared-memory window and written out with plain
+// stores (global atomics only when the stripe exceeds the window).
+__global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
+    extern __shared__ __align__(16) unsigned char ac_smem[];
+    StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
+    unsigned int* win{reinterpret_cast<unsigned int*>(ac_smem + sizeof(StripeStage))};
+    __shared__ unsigned long long sh_start;
+    __shared__ unsigned long long sh_p0;
+    __shared__ int sh_words;
     if (e.result[2] != 0) return;
-    const int lane{static_cast<int>(threadIdx.x) & 31};
-    const std::uint32_t wid{blockIdx.x * kAcWarps + (threadIdx.x >> 5)};
-    const std::uint32_t stride{gridDim.x * kAcWarps};
-    auto* words{reinterpret_cast<unsigned int*>(e.out)};
-    for (std::uint32_t item{e.ac_first + wid}; item < e.total_items; item += stride) {
-        const AcItem it{ac_item(e, item)};
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int lane{tid & 31};
+    const Stripe st{e.stripes[blockIdx.x]};
+    const GroupGeom gg{ac_group_geom(e, st.group)};
+    const int nitems{3 * st.rows * gg.gw};
+    stage_stripe(e, st, gg, s);
+    if (tid == 0) {
+        const Section sec{e.sections[st.section]};
+        const unsigned long long p0{prefix_at(e, st.item0)};
+        const unsigned long long start{e.sec_pos[st.section] * 8 + (p0 - prefix_at(e, sec.first))};
+        const unsigned long long bits{prefix_at(e, st.item0 + static_cast<std::uint32_t>(nitems)) - p0};
+        const unsigned long long nw{bits == 0 ? 0ull : ((start + bits + 31) >> 5) - (start >> 5)};
+        sh_start = start;
+        sh_p0 = p0;
+        sh_words = nw <= static_cast<unsigned long long>(kWindowWords) ? static_cast<int>(nw) : -1;
+    }
+    __syncthreads();
+    const int nwords{sh_words};
+    for (int i{tid}; i < nwords; i += kAcThreads) win[i] = 0;
+    for (int j{tid}; j < nitems; j += kAcThreads) {
+        s.aux[j] = static_cast<std::uint32_t>(prefix_at(e, st.item0 + static_cast<std::uint32_t>(j)) - sh_p0);
+    }
+    __syncthreads();
+    unsigned int* words{nwords >= 0 ? win : reinterpret_cast<unsigned int*>(e.out)};
+    const unsigned long long base{nwords >= 0 ? (sh_start & 31) : sh_start};
+    for (int j{tid}; j < nitems; j += kAcThreads) {
+        const StripeItem it{stripe_item(s, gg.gw, j)};
         if (it.n == 0) continue;
-        const Section sec{e.sections[it.section]};
-        unsigned long long base{e.sec_pos[it.section] * 8 + (prefix_at(e, item) - prefix_at(e, sec.first))};
-        ac_warp_tokens(e, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
-            const std::uint32_t d{has ? e.ac_depth[cl * 256 + sym] : 0u};
+        int cl;
+        std::uint32_t tok, nb, bits;
+        count_token(s, st, it, cl, tok, nb, bits);
+        const std::uint32_t d{__ldg(&e.ac_depth[cl * 256 + tok])};
+        const unsigned long long at{base + s.aux[j]};
+        put_bits_at(words, at, d, __ldg(&e.ac_bits[cl * 256 + tok]));
+        if (nb) put_bits_at(words, at + d, nb, bits);
+        if (it.nz != 0) {
+            s.active[atomicAdd(&s.nactive, 1)] = static_cast<std::uint16_t>(j);
+            s.aux[j] += d + nb;  // coefficient tokens start after the count token
+        }
+    }
+    __syncthreads();
+    for (int a{tid >> 5}; a < s.nactive; a += kAcWarps) {
+        const int j{s.active[a]};
+        const StripeItem it{stripe_item(s, gg.gw, j)};
+        unsigned long long pos{base + s.aux[j]};
+        coeff_tokens(s, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
+            const std::uint32_t d{has ? __ldg(&e.ac_depth[cl * 256 + sym]) : 0u};
             const std::uint32_t tb{has ? d + nb : 0u};
-            std::uint32_t incl{tb};
-#pragma unroll
-            for (int off{1}; off < 32; off <<= 1) {
-                const std::uint32_t t{__shfl_up_sync(kFull, incl, off)};
-                if (lane >= off) incl += t;
-            }
+            const std::uint32_t incl{warp_incl_scan(tb, lane)};
             if (has) {
-                const unsigned long long at{base + incl - tb};
-                put_bits_at(words, at, d, e.ac_bits[cl * 256 + sym]);
+                const unsigned long long at{pos + incl - tb};
+                put_bits_at(words, at, d, __ldg(&e.ac_bits[cl * 256 + sym]));
                 if (nb) put_bits_at(words, at + d, nb, bits);
             }
-            base += __shfl_sync(kFull, incl, 31);
+            pos += __shfl_sync(kFull, incl, 31);
         });
     }
+    __syncthreads();
+    if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
 }
 
 struct EmitVisitor {
@@ -856,26 +1014,50 @@ struct EmitVisitor {
     }
 };
 
+constexpr int kMiscWindowWords = 2048;
+
+// One thread per non-AC item; the bits of the block's items that share the
+// first item's section are assembled in a shared-memory window.
 __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
+    __shared__ unsigned int win[kMiscWindowWords];
+    __shared__ unsigned long long sh_start;
+    __shared__ std::uint32_t sh_end;
+    __shared__ int sh_words;
     if (e.result[2] != 0) return;
-    const std::uint32_t item{blockIdx.x * blockDim.x + threadIdx.x};
-    if (item >= e.ac_first) return;
-    const int s{find_section(e.sections, 0, misc_hi(e), item)};
-    const Section sec{e.sections[s]};
-    const unsigned long long rel{prefix_at(e, item) - prefix_at(e, sec.first)};
-    EmitVisitor v{&e, reinterpret_cast<unsigned int*>(e.out), e.sec_pos[s] * 8 + rel};
-    visit_misc(e, item, v);
+    const std::uint32_t first{blockIdx.x * blockDim.x};
+    const std::uint32_t item{first + threadIdx.x};
+    if (threadIdx.x == 0) {
+        const int s0{find_section(e.sections, 0, misc_hi(e), first)};
+        const Section sec{e.sections[s0]};
+        const std::uint32_t end{min(min(first + blockDim.x, sec.first + sec.count), e.ac_first)};
+        const unsigned long long p0{prefix_at(e, first)};
+        const unsigned long long start{e.sec_pos[s0] * 8 + (p0 - prefix_at(e, sec.first))};
+        const unsigned long long bits{prefix_at(e, end) - p0};
+        const unsigned long long nw{bits == 0 ? 0ull : ((start + bits + 31) >> 5) - (start >> 5)};
+        sh_start = start;
+        sh_end = end;
+        sh_words = nw <= static_cast<unsigned long long>(kMiscWindowWords) ? static_cast<int>(nw) : -1;
+    }
+    __syncthreads();
+    const int nwords{sh_words};
+    for (int i{static_cast<int>(threadIdx.x)}; i < nwords; i += blockDim.x) win[i] = 0;
+    __syncthreads();
+    if (item < e.ac_first) {
+        const int s{find_section(e.sections, 0, misc_hi(e), item)};
+        const Section sec{e.sections[s]};
+        const unsigned long long pos{e.sec_pos[s] * 8 + (prefix_at(e, item) - prefix_at(e, sec.first))};
+        const bool in_window{nwords >= 0 && item < sh_end};
+        EmitVisitor v{&e, in_window ? win : reinterpret_cast<unsigned int*>(e.out),
+                      in_window ? pos - ((sh_start >> 5) << 5) : pos};
+        visit_misc(e, item, v);
+    }
+    __syncthreads();
+    if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
 }
 
-int sm_count() {
-    int dev{0};
-    int sms{0};
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
-        sms = 148;
-    }
-    return sms;
-}
+constexpr std::size_t kHistSmem{sizeof(StripeStage) + kNumClusters * kAcSymbols * sizeof(std::uint32_t)};
+constexpr std::size_t kBitsSmem{sizeof(StripeStage)};
+constexpr std::size_t kEmitSmem{sizeof(StripeStage) + kWindowWords * sizeof(unsigned int)};
 
 }  // namespace
 
@@ -888,24 +1070,19 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
         cudaMemsetAsync(e.fb_count, 0, static_cast<std::size_t>(e.ndc) * sizeof(std::uint32_t), st) != cudaSuccess) {
         return false;
     }
-    static thread_local int sms{0};
-    if (sms == 0) sms = sm_count();
     const unsigned misc{(e.ac_first + 255) / 256};
-    const unsigned ac_items{e.total_items - e.ac_first};
-    const unsigned ac_blocks{(ac_items + kAcWarps - 1) / kAcWarps};
-    const unsigned hist_grid{min(ac_blocks, static_cast<unsigned>(sms) * 4)};
-    const unsigned ac_grid{min(ac_blocks, static_cast<unsigned>(sms) * 8)};
+    const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
-    ac_hist_kernel<<<hist_grid, kAcWarps * 32, 0, st>>>(e);
+    ac_hist_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(e);
     misc_hist_kernel<<<misc, 256, 0, st>>>(e);
     codes_kernel<<<2 + e.ndc, 512, sizeof(WarpCodeSmem) * 16, st>>>(e);
-    ac_bits_kernel<<<ac_grid, kAcWarps * 32, 0, st>>>(e);
+    ac_bits_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
     misc_bits_kernel<<<misc, 256, 0, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
     layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
     zero_body_kernel<<<296, 256, 0, st>>>(e);
-    ac_emit_kernel<<<ac_grid, kAcWarps * 32, 0, st>>>(e);
+    ac_emit_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(e);
     misc_emit_kernel<<<misc, 256, 0, st>>>(e);
     return cudaGetLastError() == cudaSuccess;
 }
@@ -914,7 +1091,13 @@ bool entropy_kernels_init() {
     return cudaFuncSetAttribute(codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(WarpCodeSmem) * 16)) == cudaSuccess &&
            cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kLayoutSmemLimit)) == cudaSuccess;
+                                static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kHistSmem)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kBitsSmem)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kEmitSmem)) == cudaSuccess;
 }
 
 }  // namespace jxb

@@ -32,6 +32,18 @@ struct Section {
     int group;             // DC or AC group index
 };
 
+// Up to kStripeRows block rows of one AC group: the unit one CTA stages in
+// shared memory for the AC passes. Rows start at multiples of 4 inside the
+// group, so every DCT16/DCT32 transform lies inside one stripe.
+constexpr int kStripeRows = 4;
+struct Stripe {
+    std::uint32_t item0;   // global index of the stripe's first item
+    std::int32_t section;  // section index of the AC group
+    std::uint16_t group;   // AC group index
+    std::uint8_t r0;       // first block row inside the group
+    std::uint8_t rows;     // block rows, 1..kStripeRows
+};
+
 // Geometry and per-frame device state of the entropy stage. All pointers are
 // device memory owned by the encoder.
 struct EntropyDev {
@@ -41,6 +53,8 @@ struct EntropyDev {
     std::uint32_t ac_first;          // first item of the first AcGroup; AC block-channels follow
     std::uint32_t num_tiles;         // scan tiles of kScanTile items
     const Section* sections;
+    const Stripe* stripes;
+    int nstripes;
 
     // inputs (frontend outputs)
     const std::int16_t* ac;
@@ -106,6 +120,7 @@ constexpr int kMaxSections = static_cast<int>(kLayoutSmemLimit / 8) - 16;
 // host-side vectors; the caller uploads them.
 struct EntropyHostPlan {
     std::vector<Section> sections;
+    std::vector<Stripe> stripes;
     std::uint32_t total_items{0};
     std::uint32_t ac_first{0};
     std::vector<std::uint8_t> pre_const;

@@ -207,6 +207,12 @@ EntropyHostPlan entropy_plan(int width, int height) {
         const int gw{std::min(32, bw - (g % xg) * 32)};
         const int gh{std::min(32, bh - (g / xg) * 32)};
         const std::uint32_t cnt{static_cast<std::uint32_t>(3 * gw * gh)};
+        const int sec{static_cast<int>(p.sections.size())};
+        for (int r0{0}; r0 < gh; r0 += kStripeRows) {
+            const int rows{std::min(kStripeRows, gh - r0)};
+            p.stripes.push_back({at + static_cast<std::uint32_t>(3 * gw * r0), sec, static_cast<std::uint16_t>(g),
+                                 static_cast<std::uint8_t>(r0), static_cast<std::uint8_t>(rows)});
+        }
         p.sections.push_back({at, cnt, kSecAcGroup, g});
         at += cnt;
     }

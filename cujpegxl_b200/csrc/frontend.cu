@@ -35,6 +35,13 @@ constexpr int kXplane = kXs * kXs;
 constexpr int kSs = kTile + 1;          // 65: stride of the sharpened tile
 constexpr int kSplane = kTile * kSs;
 constexpr int kRegionAFloats = 3 * kXplane;  // 13872
+// FP16 coefficients of the tile in region A: 64 covered-block slots per block,
+// padded to 66 so that lanes walking different blocks at the same slot hit
+// different shared-memory banks; the final-DCT row scratch follows them.
+constexpr int kCoefBlock = 66;
+constexpr int kCoefPlane = 64 * kCoefBlock;
+constexpr int kDrowsOffset = 3 * kCoefPlane / 2;  // floats
+static_assert(kDrowsOffset + 64 * 72 <= kRegionAFloats, "final-DCT scratch exceeds region A");
 
 // Selection bases: double-precision DCT-II basis narrowed to float
 // (basis[k*n + t], src/transform_select.cu:29-37). Final-DCT bases: the float
@@ -124,6 +131,15 @@ __device__ __forceinline__ void xyb_pixel(const FrontendInputs& in, int gx, int 
     ox = 0.5f * (m0 - m1);
     oy = 0.5f * (m0 + m1);
     ob = m2;
+}
+
+// lrintf((v * qgsf) / w) for a positive weight w (src/frontend_quantize.cu:
+// 165-178). When |v * qgsf| <= w / 2 the rounded quotient is at most 1/2 in
+// magnitude and rounds to zero, so the division is skipped; 0.5f * w is exact.
+__device__ __forceinline__ int quantize(float v, float qgsf, float w) {
+    const float scaled{v * qgsf};
+    if (fabsf(scaled) <= 0.5f * w) return 0;
+    return static_cast<int>(lrintf(scaled / w));
 }
 
 // RatioOfDerivativesOfCubicRootToSimpleGamma (src/adaptive_quant_impl.cuh:44-55).
@@ -266,13 +282,20 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
         float rt{0.0f};
         if (!(fx < N / 8 && fy < N / 8)) {
             const float w{wsel[fx * N + fy]};
-            const float q{rintf((coeff * qgsf) / w)};
-            const float err{(q * w) / qgsf - coeff};
-            d = err * err;
-            if (q != 0.0f) {
-                int a{static_cast<int>(fabsf(q))};
-                a = a < kLog2TableSize ? a : kLog2TableSize - 1;
-                rt = 1.0f + l2t[a];
+            const float scaled{coeff * qgsf};
+            if (fabsf(scaled) <= 0.5f * w) {
+                // |scaled / w| <= 1/2 rounds to a quotient of at most 1/2, so q
+                // is zero and err is -coeff exactly: the same d, no rate.
+                d = coeff * coeff;
+            } else {
+                const float q{rintf(scaled / w)};
+                const float err{(q * w) / qgsf - coeff};
+                d = err * err;
+                if (q != 0.0f) {
+                    int a{static_cast<int>(fabsf(q))};
+                    a = a < kLog2TableSize ? a : kLog2TableSize - 1;
+                    rt = 1.0f + l2t[a];
+                }
             }
         }
         cd_fx[fy] = d;
@@ -302,7 +325,7 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
         const int raw{fx * N + fy};
         const int q{raw >> 6};
         const int lb{(fby + q / side) * 8 + fbx + q % side};
-        coef[lb * 64 + (raw & 63)] = __float2half_rn(coeff);
+        coef[lb * kCoefBlock + (raw & 63)] = __float2half_rn(coeff);
     }
 }
 
@@ -701,53 +724,69 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
     }
     __syncthreads();
-    // 4e. first-block list (largest first) and covering owner of every block.
-    if (tid == 0) {
-        int n[3]{0, 0, 0};
-        for (int lb{0}; lb < 64; ++lb) {
-            sm.owner[lb] = 255;
-        }
-        for (int lb{0}; lb < 64; ++lb) {
-            if (bx0 + (lb & 7) >= bw || by0 + (lb >> 3) >= bh) {
-                continue;
-            }
-            const int side{sm.acs[lb]};
-            if (side == 0) {
-                continue;
-            }
-            n[side == 32 ? 0 : (side == 16 ? 1 : 2)]++;
-            const int s{side >> 3};
-            for (int dy{0}; dy < s; ++dy) {
-                for (int dx{0}; dx < s; ++dx) {
-                    sm.owner[lb + dy * 8 + dx] = static_cast<unsigned char>(lb);
+    // 4e. first-block list (DCT32 first, then DCT16, then DCT8, each in raster
+    // order) with each entry's row-pass scratch offset, and the covering owner
+    // of every block; warp 0, two blocks per lane.
+    if (warp == 0) {
+        int side[2];
+        bool in[2];
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            const int lb{lane + 32 * h};
+            in[h] = bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh;
+            side[h] = in[h] ? sm.acs[lb] : 0;
+            // The owner is the one first block within 3 blocks up and left
+            // whose transform reaches this block.
+            int own{255};
+            for (int dy{0}; dy < 4 && in[h]; ++dy) {
+                for (int dx{0}; dx < 4; ++dx) {
+                    const int fx{(lb & 7) - dx};
+                    const int fy{(lb >> 3) - dy};
+                    if (fx < 0 || fy < 0) continue;
+                    const int s{sm.acs[fy * 8 + fx] >> 3};
+                    if (s > dx && s > dy) own = fy * 8 + fx;
                 }
             }
+            sm.owner[lb] = static_cast<unsigned char>(own);
         }
-        int at[3]{0, n[0], n[0] + n[1]};
-        int off[3]{0, n[0] * 1056, n[0] * 1056 + n[1] * 272};
-        for (int lb{0}; lb < 64; ++lb) {
-            if (bx0 + (lb & 7) >= bw || by0 + (lb >> 3) >= bh || sm.acs[lb] == 0) {
-                continue;
+        int at{0};
+        int off{0};
+        const unsigned below{(1u << lane) - 1u};
+#pragma unroll
+        for (int g{0}; g < 3; ++g) {
+            const int s{32 >> g};
+            const int step{s * (s + 1)};
+            const unsigned m0{__ballot_sync(0xffffffffu, side[0] == s)};
+            const unsigned m1{__ballot_sync(0xffffffffu, side[1] == s)};
+            const int c0{__popc(m0)};
+            if (side[0] == s) {
+                const int r{at + __popc(m0 & below)};
+                sm.fb_list[r] = static_cast<unsigned char>(lane);
+                sm.fb_off[r] = off + (r - at) * step;
             }
-            const int side{sm.acs[lb]};
-            const int g{side == 32 ? 0 : (side == 16 ? 1 : 2)};
-            sm.fb_list[at[g]] = static_cast<unsigned char>(lb);
-            sm.fb_off[at[g]] = off[g];
-            at[g]++;
-            off[g] += side * (side + 1);
+            if (side[1] == s) {
+                const int r{at + c0 + __popc(m1 & below)};
+                sm.fb_list[r] = static_cast<unsigned char>(lane + 32);
+                sm.fb_off[r] = off + (r - at) * step;
+            }
+            const int cnt{c0 + __popc(m1)};
+            if (lane == 0) {
+                if (g == 0) sm.n32 = cnt;
+                if (g == 1) sm.n16 = cnt;
+                if (g == 2) sm.n8 = cnt;
+            }
+            at += cnt;
+            off += cnt * step;
         }
-        sm.n32 = n[0];
-        sm.n16 = n[1];
-        sm.n8 = n[2];
     }
-    if (tid < 192) {
-        sm.nz[tid >> 6][tid & 63] = 0;
+    if (tid >= 64 && tid < 256) {
+        sm.nz[(tid - 64) >> 6][tid & 63] = 0;
     }
     __syncthreads();
 
     // ---- 5. variable DCT of X, Y, B -> FP16 coefficients (src/frontend_transform.cu:190-266).
-    __half* coef{reinterpret_cast<__half*>(smem)};  // [3][64 blocks][64 slots]
-    float* drows{smem + 6144};
+    __half* coef{reinterpret_cast<__half*>(smem)};  // [3][64 blocks][kCoefBlock]
+    float* drows{smem + kDrowsOffset};
     const int n32{sm.n32};
     const int n16{sm.n16};
     const int n8{sm.n8};
@@ -783,7 +822,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
         __syncthreads();
-        __half* cc{coef + c * 4096};
+        __half* cc{coef + c * kCoefPlane};
         for (int k{tid}; k < tall; k += kThreads) {
             if (k < t32) {
                 const int f{k >> 6};
@@ -819,38 +858,89 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (gbx < bw && gby < bh) {
                 out.dbg_coeff[static_cast<std::size_t>(c) * nblocks * 64 +
                               (static_cast<std::size_t>(gby) * bw + gbx) * 64 + (i & 63)] =
-                    __half_as_ushort(coef[i]);
+                    __half_as_ushort(coef[c * kCoefPlane + lb * kCoefBlock + (i & 63)]);
             }
         }
     }
 
-    // ---- 6. chroma from luma over the tile (src/frontend_quantize.cu:49-117).
-    if (tid < 64) {
-        float sxy{0.0f};
-        float syy{0.0f};
-        float sby{0.0f};
-        const int lb{tid};
+    // ---- 6. chroma from luma over the tile (src/frontend_quantize.cu:49-117),
+    // and DC from the low-frequency corners (src/frontend_quantize.cu:180-200,
+    // src/vardct_layout.h:88-111), which needs no CfL result. Warps 0-5: one
+    // of the three per-block CfL sums per thread, each accumulated in raw
+    // order as the reference does. Warps 6-7: one 8x8 DC position per thread.
+    if (tid < 192) {
+        const int which{tid >> 6};  // 0: x*y, 1: y*y, 2: (b - y)*y; warp-uniform
+        const int lb{tid & 63};
+        float acc{0.0f};
         if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
+            // side = n / 8 is 1, 2 or 4: every division below is a shift.
             const int n{sm.acs[lb]};
             const int side{n >> 3};
-            for (int raw{0}; raw < n * n; ++raw) {
-                if ((raw / n) < side && (raw % n) < side) {
-                    continue;
+            const int lside{side == 1 ? 0 : (side == 2 ? 1 : 2)};
+            const int lrow{3 + lside};
+            for (int q{0}; q < side * side; ++q) {
+                const int l{lb + (q >> lside) * 8 + (q & (side - 1))};
+                for (int s{0}; s < 64; ++s) {
+                    const int raw{q * 64 + s};
+                    if ((raw >> lrow) < side && (raw & (n - 1)) < side) {
+                        continue;
+                    }
+                    const int idx{l * kCoefBlock + s};
+                    const float yr{__half2float(coef[kCoefPlane + idx])};
+                    if (which == 0) {
+                        acc = jx_fma(__half2float(coef[idx]), yr, acc);
+                    } else if (which == 1) {
+                        acc = jx_fma(yr, yr, acc);
+                    } else {
+                        acc = jx_fma(__half2float(coef[2 * kCoefPlane + idx]) - yr, yr, acc);
+                    }
                 }
-                const int q{raw >> 6};
-                const int l{lb + (q / side) * 8 + q % side};
-                const int idx{l * 64 + (raw & 63)};
-                const float xr{__half2float(coef[idx])};
-                const float yr{__half2float(coef[4096 + idx])};
-                const float br{__half2float(coef[8192 + idx])};
-                sxy = jx_fma(xr, yr, sxy);
-                syy = jx_fma(yr, yr, syy);
-                sby = jx_fma(br - yr, yr, sby);
             }
         }
-        sm.cfl[0][lb] = sxy;
-        sm.cfl[1][lb] = syy;
-        sm.cfl[2][lb] = sby;
+        sm.cfl[which][lb] = acc;
+    } else {
+        const int p{tid - 192};
+        const int f{sm.owner[p]};
+        if (bx0 + (p & 7) < bw && by0 + (p >> 3) < bh) {
+            const int n{sm.acs[f]};
+            const int m{n >> 3};
+            const int ox{(p & 7) - (f & 7)};
+            const int oy{(p >> 3) - (f >> 3)};
+            float dcv[3];
+            if (m == 1) {
+                for (int c{0}; c < 3; ++c) {
+                    dcv[c] = __half2float(coef[c * kCoefPlane + f * kCoefBlock]);
+                }
+            } else {
+                const double* ob{tb.llf_basis + (m == 2 ? 0 : 16)};
+                const double s16[2]{1.0, 0.901764195028874394};
+                const double s32[4]{1.0, 0.974886821136879522, 0.901764195028874394,
+                                    0.787054918159101335};
+                const double* scl{m == 2 ? s16 : s32};
+                for (int c{0}; c < 3; ++c) {
+                    double sum{0.0};
+                    for (int fx{0}; fx < m; ++fx) {
+                        for (int fy{0}; fy < m; ++fy) {
+                            const int raw{fx * n + fy};
+                            const int q{raw >> 6};
+                            const double cv{__half2float(
+                                coef[c * kCoefPlane + (f + (q >> (m >> 1)) * 8 + (q & (m - 1))) * kCoefBlock + (raw & 63)])};
+                            sum = sum + ob[fx * 4 + ox] * ob[fy * 4 + oy] * cv * scl[fx] * scl[fy];
+                        }
+                    }
+                    dcv[c] = static_cast<float>(static_cast<double>(m) * sum);
+                }
+            }
+            const float dcq_x{4096.0f * sc.dc_scale};
+            const float dcq_y{512.0f * sc.dc_scale};
+            const float dcq_b{256.0f * sc.dc_scale};
+            const std::size_t blk{static_cast<std::size_t>(by0 + (p >> 3)) * bw + bx0 + (p & 7)};
+            const int qdy{static_cast<int>(lrintf(dcv[1] * dcq_y))};
+            const float ydr{static_cast<float>(qdy) / dcq_y};
+            out.dc[nblocks + blk] = qdy;
+            out.dc[blk] = static_cast<int>(lrintf(dcv[0] * dcq_x));
+            out.dc[2 * static_cast<std::size_t>(nblocks) + blk] = static_cast<int>(lrintf((dcv[2] - ydr) * dcq_b));
+        }
     }
     __syncthreads();
     if (warp == 0) {
@@ -891,26 +981,31 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int f{sm.owner[lb]};
         const int n{sm.acs[f]};
         const int side{n >> 3};
+        const int lrow{side == 1 ? 3 : (side == 2 ? 4 : 5)};  // log2(n)
         const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
         const int raw{q * 64 + slot};
         const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
         std::int16_t ax{0};
         std::int16_t ay{0};
         std::int16_t ab{0};
-        if (!((raw / n) < side && (raw % n) < side)) {
+        if (!((raw >> lrow) < side && (raw & (n - 1)) < side)) {
             const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
             const float* wt{tb.dequant + si * 3072};
             const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
-            const float xr{__half2float(coef[k])};
-            const float yr{__half2float(coef[4096 + k])};
-            const float br{__half2float(coef[8192 + k])};
+            const int ci{lb * kCoefBlock + slot};
+            const float xr{__half2float(coef[ci])};
+            const float yr{__half2float(coef[kCoefPlane + ci])};
+            const float br{__half2float(coef[2 * kCoefPlane + ci])};
             const float wy{wt[1024 + raw]};
-            const int qy{static_cast<int>(lrintf((yr * qgsf) / wy))};
-            const float yq{(static_cast<float>(qy) * wy) / qgsf};
+            const int qy{quantize(yr, qgsf, wy)};
+            // A zero Y quantum reconstructs to a signed zero, and fma(-m, +-0, v)
+            // equals v up to the sign of a zero result, which quantises to 0
+            // either way.
+            const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy) / qgsf};
             const float wx{wt[raw]};
-            const int qx{static_cast<int>(lrintf((jx_fma(-ytox, yq, xr) * qgsf) / wx))};
+            const int qx{quantize(jx_fma(-ytox, yq, xr), qgsf, wx)};
             const float wb{wt[2048 + raw]};
-            const int qb{static_cast<int>(lrintf((jx_fma(-ytob, yq, br) * qgsf) / wb))};
+            const int qb{quantize(jx_fma(-ytob, yq, br), qgsf, wb)};
             ax = static_cast<std::int16_t>(qx);
             ay = static_cast<std::int16_t>(qy);
             ab = static_cast<std::int16_t>(qb);
@@ -921,68 +1016,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         out.ac[g] = ax;
         out.ac[cplane + g] = ay;
         out.ac[2 * cplane + g] = ab;
-    }
-    // DC from the low-frequency corner (src/frontend_quantize.cu:180-200,
-    // src/vardct_layout.h:88-111).
-    if (tid < 64) {
-        const int lb{tid};
-        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
-            const int n{sm.acs[lb]};
-            const int m{n >> 3};
-            const float dcq_x{4096.0f * sc.dc_scale};
-            const float dcq_y{512.0f * sc.dc_scale};
-            const float dcq_b{256.0f * sc.dc_scale};
-            float llf[3][16];
-            for (int c{0}; c < 3; ++c) {
-                for (int fx{0}; fx < m; ++fx) {
-                    for (int fy{0}; fy < m; ++fy) {
-                        const int raw{fx * n + fy};
-                        const int q{raw >> 6};
-                        llf[c][fx * m + fy] =
-                            __half2float(coef[c * 4096 + (lb + (q / m) * 8 + q % m) * 64 + (raw & 63)]);
-                    }
-                }
-            }
-            float dcv[3][16];
-            if (m == 1) {
-                for (int c{0}; c < 3; ++c) {
-                    dcv[c][0] = llf[c][0];
-                }
-            } else {
-                const double* ob{tb.llf_basis + (m == 2 ? 0 : 16)};
-                const double s16[2]{1.0, 0.901764195028874394};
-                const double s32[4]{1.0, 0.974886821136879522, 0.901764195028874394,
-                                    0.787054918159101335};
-                const double* scl{m == 2 ? s16 : s32};
-                for (int c{0}; c < 3; ++c) {
-                    for (int oy{0}; oy < m; ++oy) {
-                        for (int ox{0}; ox < m; ++ox) {
-                            double sum{0.0};
-                            for (int fx{0}; fx < m; ++fx) {
-                                for (int fy{0}; fy < m; ++fy) {
-                                    const double cv{llf[c][fx * m + fy]};
-                                    sum = sum + ob[fx * 4 + ox] * ob[fy * 4 + oy] * cv * scl[fx] * scl[fy];
-                                }
-                            }
-                            dcv[c][oy * m + ox] = static_cast<float>(static_cast<double>(m) * sum);
-                        }
-                    }
-                }
-            }
-            for (int oy{0}; oy < m; ++oy) {
-                for (int ox{0}; ox < m; ++ox) {
-                    const int p{oy * m + ox};
-                    const std::size_t blk{static_cast<std::size_t>(by0 + (lb >> 3) + oy) * bw + bx0 +
-                                          (lb & 7) + ox};
-                    const int qdy{static_cast<int>(lrintf(dcv[1][p] * dcq_y))};
-                    const float ydr{static_cast<float>(qdy) / dcq_y};
-                    out.dc[nblocks + blk] = qdy;
-                    out.dc[blk] = static_cast<int>(lrintf(dcv[0][p] * dcq_x));
-                    out.dc[2 * static_cast<std::size_t>(nblocks) + blk] =
-                        static_cast<int>(lrintf((dcv[2][p] - ydr) * dcq_b));
-                }
-            }
-        }
     }
     __syncthreads();
 

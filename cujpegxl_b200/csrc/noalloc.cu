@@ -87,7 +87,7 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
                                                     size_t* out_size, uintptr_t stream) {
     if (planes == nullptr || out_device == nullptr || out_size == nullptr || planes->ac == 0 ||
         planes->dc == 0 || planes->acs == 0 || planes->qf == 0 || planes->ytox == 0 || planes->ytob == 0 ||
-        (reinterpret_cast<std::uintptr_t>(out_device) & 15u) != 0) {
+        (reinterpret_cast<std::uintptr_t>(out_device) & 15u) != 0 || (planes->ac & 15u) != 0) {
         return CUJPEGXL_INVALID_ARGUMENT;
     }
     if (width == 0 || height == 0 || width % 8 != 0 || height % 8 != 0 ||
@@ -127,6 +127,7 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
     e.ac_first = plan.ac_first;
     e.num_tiles = tiles;
     auto* sections{c.take<jxb::Section>(plan.sections.size())};
+    auto* stripes{c.take<jxb::Stripe>(plan.stripes.size())};
     auto* order{c.take<std::uint16_t>(plan.order.size())};
     auto* pre{c.take<std::uint8_t>(plan.pre_const.size())};
     auto* mid{c.take<std::uint8_t>(plan.mid_const.size())};
@@ -156,6 +157,8 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
     if (!c.ok) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
 
     e.sections = sections;
+    e.stripes = stripes;
+    e.nstripes = static_cast<int>(plan.stripes.size());
     e.order = order;
     e.pre_const = pre;
     e.pre_const_bits = plan.pre_const_bits;
@@ -181,6 +184,8 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
     // entropy stage itself.
     const bool uploaded{
         cudaMemcpyAsync(sections, plan.sections.data(), plan.sections.size() * sizeof(jxb::Section),
+                        cudaMemcpyHostToDevice, st) == cudaSuccess &&
+        cudaMemcpyAsync(stripes, plan.stripes.data(), plan.stripes.size() * sizeof(jxb::Stripe),
                         cudaMemcpyHostToDevice, st) == cudaSuccess &&
         cudaMemcpyAsync(order, plan.order.data(), plan.order.size() * 2, cudaMemcpyHostToDevice, st) == cudaSuccess &&
         cudaMemcpyAsync(pre, plan.pre_const.data(), plan.pre_const.size(), cudaMemcpyHostToDevice, st) == cudaSuccess &&

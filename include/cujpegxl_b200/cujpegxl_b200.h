@@ -95,8 +95,9 @@ typedef struct cujpegxl_b200_device_planes {
  * cujpegxl_b200_encode_planes, for callers that cannot allocate device memory
  * while they encode (inside a stream capture, in a real-time loop where
  * cudaMalloc would synchronise the device, or with all device memory held by
- * their own pool). It allocates nothing: the caller passes the planes and a
- * device output buffer (16-byte aligned, `out_capacity` bytes), and every
+ * their own pool). It allocates nothing: the caller passes the planes (the AC
+ * plane 16-byte aligned, as every cudaMalloc'd buffer is) and a device output
+ * buffer (16-byte aligned, `out_capacity` bytes), and every
  * intermediate lives in one fixed 7 MiB array that each GPU loading the
  * library holds until the process exits.
  *  - Frames above 4,194,304 pixels (width*height) are rejected with
