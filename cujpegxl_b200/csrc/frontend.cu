@@ -61,12 +61,18 @@ __device__ __forceinline__ float basis(int i) {
     return N == 8 ? c_dct8[i] : (N == 16 ? c_dct16[i] : c_dct32[i]);
 }
 
+// Rate-proxy table entries kept in shared memory: quantised magnitudes below
+// this are by far the most frequent.
+constexpr int kLog2Cached = 256;
+
 struct Small {
     float pre[256];       // AQ pre-erosion cells, 16x16 over the tile
+    float log2_small[kLog2Cached];  // log2f(1 + i), the first entries of the rate table
     float cost8[64];
     float cost16[16];
     float cost32[4];
     float cfl[3][64];
+    float aq_sums[4][64];  // per block: HF sum, gamma sum, blue sum, eroded mask
     int qf[64];
     int nz[3][64];
     int fb_off[64];       // final-DCT scratch offset of each listed first-block
@@ -79,6 +85,8 @@ struct Small {
 
 constexpr std::size_t kSmemBytes =
     sizeof(float) * (kRegionAFloats + 3 * kSplane) + sizeof(Small);
+// Two CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA.
+static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two frontend CTAs no longer fit on one SM");
 
 __device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
 
@@ -87,15 +95,32 @@ __device__ __forceinline__ float srgb_to_linear(float e) {
     return e <= 0.04045f ? e * (1.0f / 12.92f) : jx_pow24((e + 0.055f) * (1.0f / 1.055f));
 }
 
-// NV12 pixel (gx, gy) -> XYB (src/xyb_impl.cuh:49-70). Chroma is the centred
-// bilinear 2x upsample of the texture path (src/frontend_fused.cu:222), taken
-// exactly: the four taps carry weights {1,3}x{1,3}/16, summed in integers.
-__device__ __forceinline__ void xyb_pixel(const FrontendInputs& in, int gx, int gy, float& ox,
-                                          float& oy, float& ob) {
-    const float yv{static_cast<float>(in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx]) *
-                   kInv255};
-    const int cw{in.width >> 1};
-    const int ch{in.height >> 1};
+// s / 4080.0f correctly rounded for an integer s in [0, 4080], without a
+// division: q0 = s * RN(1/4080), then one Newton correction with the exact
+// residual s - q0 * 4080. Checked against the rounded quotient for every s in
+// the range (the tap sums of the chroma upsample never leave it).
+__device__ __forceinline__ float div4080(int s) {
+    constexpr float kInv{1.0f / 4080.0f};
+    const float sf{static_cast<float>(s)};
+    const float q0{sf * kInv};
+    return jx_fma(jx_fma(-q0, 4080.0f, sf), kInv, q0);
+}
+
+// Chroma window of a tile in shared memory: kChromaWin x kChromaWin (cb, cr)
+// pairs starting kChromaMargin chroma samples before the tile's first.
+constexpr int kChromaMargin = 2;
+constexpr int kChromaWin = kTile / 2 + 2 * kChromaMargin;  // 36
+
+// NV12 pixel (gx, gy) -> XYB (src/xyb_impl.cuh:49-70), from its luma byte and
+// the tile's chroma window whose first pair is chroma sample (cx0, cy0).
+// Chroma is the centred bilinear 2x upsample of the texture path
+// (src/frontend_fused.cu:222), taken exactly: the four taps carry weights
+// {1,3}x{1,3}/16, summed in integers.
+__device__ __forceinline__ void xyb_pixel(int luma, const std::uint8_t* win, int cx0, int cy0, int gx, int gy,
+                                          int width, int height, float& ox, float& oy, float& ob) {
+    const float yv{static_cast<float>(luma) * kInv255};
+    const int cw{width >> 1};
+    const int ch{height >> 1};
     const int jx{gx >> 1};
     const int jy{gy >> 1};
     int xa, xb, wxa, wxb, ya, yb, wya, wyb;
@@ -109,14 +134,14 @@ __device__ __forceinline__ void xyb_pixel(const FrontendInputs& in, int gx, int 
     } else {
         ya = max(jy - 1, 0); yb = jy; wya = 1; wyb = 3;
     }
-    const std::uint8_t* ra{in.chroma + static_cast<std::size_t>(ya) * in.chroma_pitch};
-    const std::uint8_t* rb{in.chroma + static_cast<std::size_t>(yb) * in.chroma_pitch};
-    const int scb{wya * (wxa * ra[2 * xa] + wxb * ra[2 * xb]) +
-                  wyb * (wxa * rb[2 * xa] + wxb * rb[2 * xb])};
-    const int scr{wya * (wxa * ra[2 * xa + 1] + wxb * ra[2 * xb + 1]) +
-                  wyb * (wxa * rb[2 * xa + 1] + wxb * rb[2 * xb + 1])};
-    const float cb{static_cast<float>(scb) / 4080.0f - kChromaCenter};
-    const float cr{static_cast<float>(scr) / 4080.0f - kChromaCenter};
+    const int aa{2 * ((ya - cy0) * kChromaWin + xa - cx0)};
+    const int ab{2 * ((ya - cy0) * kChromaWin + xb - cx0)};
+    const int ba{2 * ((yb - cy0) * kChromaWin + xa - cx0)};
+    const int bb{2 * ((yb - cy0) * kChromaWin + xb - cx0)};
+    const int scb{wya * (wxa * win[aa] + wxb * win[ab]) + wyb * (wxa * win[ba] + wxb * win[bb])};
+    const int scr{wya * (wxa * win[aa + 1] + wxb * win[ab + 1]) + wyb * (wxa * win[ba + 1] + wxb * win[bb + 1])};
+    const float cb{div4080(scb) - kChromaCenter};
+    const float cr{div4080(scr) - kChromaCenter};
 
     const float r{clamp01(srgb_to_linear(clamp01(jx_fma(kCrToR, cr, yv))))};
     const float g{clamp01(srgb_to_linear(clamp01(jx_fma(-kCrToG, cr, jx_fma(-kCbToG, cb, yv)))))};
@@ -265,7 +290,8 @@ __device__ __forceinline__ void row_pass(const float* src, float* dst) {
 // (src/transform_select_impl.cuh:80-106).
 template <int N, int Y0, int Y1>
 __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, float* cr_fx, int fx,
-                                        float qgsf, const float* wsel, const float* l2t) {
+                                        float qgsf, const float* wsel, const float* l2t,
+                                        const float* l2s) {
     float rr[N];
 #pragma unroll
     for (int r{0}; r < N; ++r) {
@@ -294,7 +320,7 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
                 if (q != 0.0f) {
                     int a{static_cast<int>(fabsf(q))};
                     a = a < kLog2TableSize ? a : kLog2TableSize - 1;
-                    rt = 1.0f + l2t[a];
+                    rt = 1.0f + (a < kLog2Cached ? l2s[a] : l2t[a]);
                 }
             }
         }
@@ -329,6 +355,69 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
     }
 }
 
+// One CfL sum of a side-N first block lb over its non-LLF coefficients in raw
+// order, as the reference accumulates it (src/frontend_quantize.cu:63-74):
+// kWhich 0 sums x*y, 1 sums y*y and 2 sums (b - y)*y, each an FMA chain. The
+// chain is sequential; its loads are issued ahead in groups of 16 slots. An
+// LLF slot contributes fma(0, y, acc) instead of being skipped: that adds an
+// exact zero, which can change only the sign of a zero sum, and the quantised
+// CfL maps do not see that sign. Only the first covered block (two for DCT32)
+// holds LLF slots: the first N/8 columns of its first rows.
+template <int N, int kWhich>
+__device__ __forceinline__ float cfl_sum(const __half* coef, int lb) {
+    constexpr int kSide{N / 8};
+    constexpr int kQLlf{kSide == 4 ? 2 : 1};
+    constexpr std::uint64_t kLlf{N == 8 ? 0x1ull : (N == 16 ? 0x30003ull : 0xF0000000Full)};
+    float acc{0.0f};
+#pragma unroll 1
+    for (int q{0}; q < kSide * kSide; ++q) {
+        const int l{lb + (q / kSide) * 8 + q % kSide};
+        const __half2* py{reinterpret_cast<const __half2*>(coef + kCoefPlane + l * kCoefBlock)};
+        const __half2* po{reinterpret_cast<const __half2*>(coef + (kWhich == 2 ? 2 * kCoefPlane : 0) +
+                                                           l * kCoefBlock)};
+        const std::uint64_t skip{q < kQLlf ? kLlf : 0ull};
+#pragma unroll
+        for (int c{0}; c < 4; ++c) {
+            float2 y[8];
+            float2 o[8];
+#pragma unroll
+            for (int j{0}; j < 8; ++j) {
+                y[j] = __half22float2(py[c * 8 + j]);
+                if (kWhich != 1) o[j] = __half22float2(po[c * 8 + j]);
+            }
+#pragma unroll
+            for (int j{0}; j < 16; ++j) {
+                const float yr{(j & 1) ? y[j >> 1].y : y[j >> 1].x};
+                float a;
+                if (kWhich == 0) {
+                    a = (j & 1) ? o[j >> 1].y : o[j >> 1].x;
+                } else if (kWhich == 1) {
+                    a = yr;
+                } else {
+                    a = ((j & 1) ? o[j >> 1].y : o[j >> 1].x) - yr;
+                }
+                if (((kLlf >> (16 * c + j)) & 1ull) != 0) {
+                    a = ((skip >> (16 * c + j)) & 1ull) != 0 ? 0.0f : a;
+                }
+                acc = jx_fma(a, yr, acc);
+            }
+        }
+    }
+    return acc;
+}
+
+// The three sums of every first block of side N, sum kind `which` per warp
+// and one first block per lane (list entries first..first+count-1).
+template <int N>
+__device__ __forceinline__ void cfl_class(const __half* coef, const unsigned char* list, int first, int count,
+                                          int which, int lane, float (*cfl)[64]) {
+    for (int i{lane}; i < count; i += 32) {
+        const int lb{list[first + i]};
+        cfl[which][lb] = which == 0 ? cfl_sum<N, 0>(coef, lb)
+                                    : (which == 1 ? cfl_sum<N, 1>(coef, lb) : cfl_sum<N, 2>(coef, lb));
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
     frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
     extern __shared__ __align__(16) float smem[];
@@ -352,13 +441,38 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int by0{ty * 8};
 
     // ---- 1. NV12 -> XYB over the tile and a 2-pixel halo (clamped coordinates).
+    // 1a. Stage the NV12 window in region B, which is free until gaborish: the
+    // luma of every halo pixel and the chroma pairs of chroma columns and rows
+    // cx0..cx0+35 and cy0..cy0+35, each at its clamped coordinate. All loads
+    // are independent, so their latencies overlap.
+    std::uint8_t* win_luma{reinterpret_cast<std::uint8_t*>(shp)};
+    std::uint8_t* win_chroma{win_luma + kXplane};
+    const int cx0{(px0 >> 1) - kChromaMargin};
+    const int cy0{(py0 >> 1) - kChromaMargin};
+    {
+        const int cw{W >> 1};
+        const int ch{H >> 1};
+        for (int i{tid}; i < kXplane; i += kThreads) {
+            const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
+            const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
+            win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
+        }
+        for (int i{tid}; i < kLog2Cached; i += kThreads) sm.log2_small[i] = tb.log2_1p[i];
+        for (int i{tid}; i < kChromaWin * kChromaWin; i += kThreads) {
+            const int jx{min(max(cx0 + i % kChromaWin, 0), cw - 1)};
+            const int jy{min(max(cy0 + i / kChromaWin, 0), ch - 1)};
+            const std::uint8_t* p{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
+            win_chroma[2 * i] = p[0];
+            win_chroma[2 * i + 1] = p[1];
+        }
+    }
+    __syncthreads();
+    // 1b. XYB of every halo pixel from the window.
     for (int i{tid}; i < kXplane; i += kThreads) {
-        const int lx{i % kXs};
-        const int ly{i / kXs};
-        const int gx{min(max(px0 - kHalo + lx, 0), W - 1)};
-        const int gy{min(max(py0 - kHalo + ly, 0), H - 1)};
+        const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
+        const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
         float x, y, b;
-        xyb_pixel(in, gx, gy, x, y, b);
+        xyb_pixel(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
         xyb[i] = x;
         xyb[kXplane + i] = y;
         xyb[2 * kXplane + i] = b;
@@ -440,24 +554,12 @@ __global__ void __launch_bounds__(kThreads, 2)
             red[half][3] = warp_tree(er);
         }
         if (lane == 0) {
-            const float hf_sum{red[0][0] + red[1][0]};
-            const float gamma_overall{(red[0][1] + red[1][1]) * (0.5f / 64.0f)};
-            float blue_sum{red[0][2] + red[1][2]};
-            const float aq{red[0][3] + red[1][3]};
-            if (blue_sum >= 32.0f * kBlueLimit) {
-                blue_sum = 64.0f * kBlueLimit - blue_sum;
-            }
-            if (blue_sum >= kBlueMaxLimit * kBlueLimit) {
-                blue_sum = kBlueMaxLimit * kBlueLimit;
-            }
-            float ov{compute_mask(aq)};
-            ov = ov + jx_fma(hf_sum, kHfMul, kHfAdd);
-            ov = jx_fma(kGammaLogMul, jx_log2(gamma_overall), ov);
-            ov = jx_fma(blue_sum, kBlueMul, ov);
-            const float qval{jx_fma(jx_exp(ov), sc.mul_pb, sc.add_pb)};
-            int qi{static_cast<int>(jx_fma(qval, sc.inv_global_scale, 0.5f))};
-            qi = qi < 1 ? 1 : (qi > kQuantMax ? kQuantMax : qi);
-            sm.qf[lb] = qi;
+            // The block's quant field is finished from these sums by its own
+            // thread in step 4e, where most warps are otherwise idle.
+            sm.aq_sums[0][lb] = red[0][0] + red[1][0];
+            sm.aq_sums[1][lb] = red[0][1] + red[1][1];
+            sm.aq_sums[2][lb] = red[0][2] + red[1][2];
+            sm.aq_sums[3][lb] = red[0][3] + red[1][3];
         }
     }
 
@@ -520,7 +622,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int fx{k & 7};
         if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
             sel_col<8, 0, 8>(rows + lb * 72 + fx * 9, cdist + lb * 72 + fx * 9,
-                             crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p);
+                             crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p, sm.log2_small);
         }
     }
     __syncthreads();
@@ -553,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh) {
             sel_col<16, 0, 16>(rows + qd * 272 + fx * 17, cdist + qd * 272 + fx * 17,
                                crate + qd * 272 + fx * 17, fx, qg, tb.sel_weight + 1024,
-                               tb.log2_1p);
+                               tb.log2_1p, sm.log2_small);
         }
     }
     __syncthreads();
@@ -611,9 +713,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             float* cd{cdist + ri * 1056 + fx * 33};
             float* cr{crate + ri * 1056 + fx * 33};
             if (hi) {
-                sel_col<32, 16, 32>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p);
+                sel_col<32, 16, 32>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
             } else {
-                sel_col<32, 0, 16>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p);
+                sel_col<32, 0, 16>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
             }
         }
     }
@@ -781,6 +883,31 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     if (tid >= 64 && tid < 256) {
         sm.nz[(tid - 64) >> 6][tid & 63] = 0;
+        sm.cfl[(tid - 64) >> 6][tid & 63] = 0.0f;  // blocks that are not first blocks add zero
+    }
+    if (tid >= 64 && tid < 128) {
+        // Quant field of block lb from its AQ sums (src/frontend_fused.cu:177-201).
+        const int lb{tid - 64};
+        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
+            const float hf_sum{sm.aq_sums[0][lb]};
+            const float gamma_overall{sm.aq_sums[1][lb] * (0.5f / 64.0f)};
+            float blue_sum{sm.aq_sums[2][lb]};
+            const float aq{sm.aq_sums[3][lb]};
+            if (blue_sum >= 32.0f * kBlueLimit) {
+                blue_sum = 64.0f * kBlueLimit - blue_sum;
+            }
+            if (blue_sum >= kBlueMaxLimit * kBlueLimit) {
+                blue_sum = kBlueMaxLimit * kBlueLimit;
+            }
+            float ov{compute_mask(aq)};
+            ov = ov + jx_fma(hf_sum, kHfMul, kHfAdd);
+            ov = jx_fma(kGammaLogMul, jx_log2(gamma_overall), ov);
+            ov = jx_fma(blue_sum, kBlueMul, ov);
+            const float qval{jx_fma(jx_exp(ov), sc.mul_pb, sc.add_pb)};
+            int qi{static_cast<int>(jx_fma(qval, sc.inv_global_scale, 0.5f))};
+            qi = qi < 1 ? 1 : (qi > kQuantMax ? kQuantMax : qi);
+            sm.qf[lb] = qi;
+        }
     }
     __syncthreads();
 
@@ -869,36 +996,16 @@ __global__ void __launch_bounds__(kThreads, 2)
     // of the three per-block CfL sums per thread, each accumulated in raw
     // order as the reference does. Warps 6-7: one 8x8 DC position per thread.
     if (tid < 192) {
-        const int which{tid >> 6};  // 0: x*y, 1: y*y, 2: (b - y)*y; warp-uniform
-        const int lb{tid & 63};
-        float acc{0.0f};
-        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && sm.acs[lb] != 0) {
-            // side = n / 8 is 1, 2 or 4: every division below is a shift.
-            const int n{sm.acs[lb]};
-            const int side{n >> 3};
-            const int lside{side == 1 ? 0 : (side == 2 ? 1 : 2)};
-            const int lrow{3 + lside};
-            for (int q{0}; q < side * side; ++q) {
-                const int l{lb + (q >> lside) * 8 + (q & (side - 1))};
-                for (int s{0}; s < 64; ++s) {
-                    const int raw{q * 64 + s};
-                    if ((raw >> lrow) < side && (raw & (n - 1)) < side) {
-                        continue;
-                    }
-                    const int idx{l * kCoefBlock + s};
-                    const float yr{__half2float(coef[kCoefPlane + idx])};
-                    if (which == 0) {
-                        acc = jx_fma(__half2float(coef[idx]), yr, acc);
-                    } else if (which == 1) {
-                        acc = jx_fma(yr, yr, acc);
-                    } else {
-                        acc = jx_fma(__half2float(coef[2 * kCoefPlane + idx]) - yr, yr, acc);
-                    }
-                }
-            }
+        // Warps 0-2 take the long DCT32 chains, one sum kind each and one
+        // first block per lane; warps 3-5 the DCT16 and then the DCT8 chains
+        // the same way. Every warp's chains have one length.
+        if (warp < 3) {
+            cfl_class<32>(coef, sm.fb_list, 0, sm.n32, warp, lane, sm.cfl);
+        } else {
+            cfl_class<16>(coef, sm.fb_list, sm.n32, sm.n16, warp - 3, lane, sm.cfl);
+            cfl_class<8>(coef, sm.fb_list, sm.n32 + sm.n16, sm.n8, warp - 3, lane, sm.cfl);
         }
-        sm.cfl[which][lb] = acc;
-    } else {
+    } else if (tid >= 192) {
         const int p{tid - 192};
         const int f{sm.owner[p]};
         if (bx0 + (p & 7) < bw && by0 + (p >> 3) < bh) {
