@@ -63,6 +63,22 @@ def test_file_bit_exact(w, h, d, seed):
         assert data == api.ref_encode_frame(r, d)
 
 
+@pytest.mark.parametrize("d", [0.5, 1.0, 2.0, 4.0])
+def test_4k_file_and_planes_bit_exact(d):
+    """The benchmark frame at every distance of the 4K configuration: the
+    quantised planes and the file equal the CPU restatement's."""
+    w, h = 3840, 2160
+    nv = make_nv12(w, h, 0)
+    keep, luma, chroma, lp, cp = device_nv12(nv, w, h)
+    with Encoder(w, h, d) as enc:
+        data = enc.encode_device(luma, chroma, lp, cp)
+        g = enc.read_planes()
+    o = api.frontend(nv, w, h, d)
+    for k in ("qf", "acs", "ytox", "ytob", "ac", "dc"):
+        np.testing.assert_array_equal(g[k], getattr(o, k), err_msg=k)
+    assert data == api.encode(nv, w, h, d)
+
+
 def test_pitched_input_matches_packed():
     w, h = 512, 384
     _, packed, _ = _frontend_and_file(w, h, 1.0, 5)
