@@ -366,6 +366,63 @@ def run_ours(args) -> None:
         pg.destroy_process_group()
 
 
+MIXED64 = ([(1280, 720)] * 16 + [(1920, 1080)] * 16 + [(2560, 1440)] * 16 + [(3840, 2160)] * 8
+           + [(4096, 2160)] * 8)
+
+
+def run_batch(args) -> None:
+    """The 64-frame uneven-resolution batch (16 x 720p, 16 x 1080p, 16 x 1440p,
+    8 x 3840x2160, 8 x 4096x2160; frame i from seed i, d=1.0): one CUDA graph
+    launch per step through cujpegxl_b200_batch_encode."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from cujpegxl_b200 import Batch
+    from cujpegxl_b200.synth import make_nv12
+
+    d = args.distance
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
+        nvs = list(pool.map(lambda i: make_nv12(MIXED64[i][0], MIXED64[i][1], i), range(len(MIXED64))))
+    dev = [torch.from_numpy(nv).cuda() for nv in nvs]
+    torch.cuda.synchronize()
+    inputs = [(t.data_ptr(), t.data_ptr() + w * h, w, w) for t, (w, h) in zip(dev, MIXED64)]
+    batch = Batch([(w, h, d) for w, h in MIXED64], local)
+    for _ in range(args.warmup):
+        batch.encode(inputs)
+        batch.sync()
+    stream = torch.cuda.ExternalStream(batch.stream())
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        batch.encode(inputs)
+    stop.record(stream)
+    sizes = batch.sync()
+    torch.cuda.synchronize()
+    dt = start.elapsed_time(stop) / 1000.0
+    n = args.steps * len(MIXED64)
+    mp = sum(w * h for w, h in MIXED64) * args.steps / 1e6
+    if rank == 0:
+        print(json.dumps({
+            "metric": "mixed-resolution batch frames/s", "value": n / dt, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 frames: 16x1280x720, 16x1920x1080, 16x2560x1440, 8x3840x2160, "
+                                   f"8x4096x2160, frame i seed i, d={d}",
+                       "step": "one CUDA graph launch of the whole batch", "lanes": batch.lanes},
+            "mp_per_s": mp / dt, "bytes_per_step": sum(sizes),
+            "timing": "CUDA events on the batch's stream around K graph launches (each ends with the "
+                      "device-to-host copy of every frame's size)",
+        }), flush=True)
+    torch.cuda.synchronize()
+    del start, stop, stream
+    batch.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,9 +435,13 @@ def main() -> None:
     ap.add_argument("--cpu-runs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--streams", type=int, default=4, help="encoders (CUDA streams) per GPU")
+    ap.add_argument("--workload", default="4k", choices=["4k", "mixed64"],
+                    help="mixed64: the 64-frame uneven-resolution batch in one graph launch per step")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "mixed64":
+        run_batch(args)
     else:
         run_ours(args)
 

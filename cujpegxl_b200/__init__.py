@@ -22,7 +22,7 @@ import numpy as np
 from . import _capi
 from ._capi import CujpegxlError, check
 
-__all__ = ["API_VERSION", "api_version", "query_backend", "encode", "encode_with_stats", "Encoder",
+__all__ = ["API_VERSION", "api_version", "query_backend", "encode", "encode_with_stats", "Encoder", "Batch",
            "CujpegxlError", "max_output_size"]
 
 
@@ -161,6 +161,69 @@ class Encoder:
     def stream(self) -> int:
         s = ctypes.c_size_t(0)
         check("encoder_stream", self._L.cujpegxl_b200_encoder_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+
+class Batch:
+    """Frames of different sizes encoded by one CUDA graph launch
+    (cujpegxl_b200_batch_*). `frames` lists (width, height, distance)."""
+
+    def __init__(self, frames: list[tuple[int, int, float]], device_ordinal: int = 0):
+        self._L = _capi.lib()
+        self.frames = list(frames)
+        cfgs = (_capi.Config * len(self.frames))(*[_capi.Config(w, h, d, device_ordinal) for w, h, d in self.frames])
+        h = ctypes.c_void_p()
+        check("batch_create", self._L.cujpegxl_b200_batch_create(cfgs, len(self.frames), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.cujpegxl_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def encode(self, inputs: list[tuple[int, int, int, int]]) -> None:
+        """Enqueues the batch; inputs[i] = (luma, chroma, luma_pitch, chroma_pitch) device addresses."""
+        arr = (_capi.Nv12Input * len(inputs))(*[_capi.Nv12Input(*x) for x in inputs])
+        check("batch_encode", self._L.cujpegxl_b200_batch_encode(self._h, arr))
+
+    def sync(self) -> list[int]:
+        sizes = (ctypes.c_size_t * len(self.frames))()
+        check("batch_sync", self._L.cujpegxl_b200_batch_sync(self._h, sizes))
+        return list(sizes)
+
+    def frame(self, index: int) -> tuple[int, int]:
+        """(size, device address) of a frame's file after sync."""
+        size = ctypes.c_size_t(0)
+        dev = ctypes.c_size_t(0)
+        check("batch_frame", self._L.cujpegxl_b200_batch_frame(self._h, index, ctypes.byref(size), ctypes.byref(dev)))
+        return size.value, dev.value
+
+    def read(self, index: int) -> bytes:
+        size, _ = self.frame(index)
+        buf = np.empty(max(size, 1), dtype=np.uint8)
+        out = _capi.Output(buf.ctypes.data, 0, buf.size)
+        check("batch_copy", self._L.cujpegxl_b200_batch_copy(self._h, index, ctypes.byref(out)))
+        return buf[:out.size].tobytes()
+
+    @property
+    def lanes(self) -> int:
+        return int(self._L.cujpegxl_b200_batch_lanes(self._h))
+
+    def stream(self) -> int:
+        s = ctypes.c_size_t(0)
+        check("batch_stream", self._L.cujpegxl_b200_batch_stream(self._h, ctypes.byref(s)))
         return s.value
 
 

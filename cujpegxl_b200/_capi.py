@@ -29,6 +29,9 @@ EXPORTS = (
     "cujpegxl_b200_encode_planes", "cujpegxl_b200_encode_host", "cujpegxl_b200_encoder_enqueue",
     "cujpegxl_b200_encoder_enqueue_stages", "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream",
     "cujpegxl_b200_kernels_per_encode", "cujpegxl_b200_encode_planes_noalloc",
+    "cujpegxl_b200_batch_create", "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync",
+    "cujpegxl_b200_batch_frame", "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_lanes",
+    "cujpegxl_b200_batch_destroy", "cujpegxl_b200_batch_stream",
 )
 
 
@@ -91,11 +94,23 @@ def lib() -> ctypes.CDLL:
                                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                                       ctypes.c_size_t, P(ctypes.c_size_t), ctypes.c_size_t]
     L.cujpegxl_b200_encode_planes_noalloc.restype = ctypes.c_int
+    L.cujpegxl_b200_batch_create.argtypes = [P(Config), ctypes.c_size_t, P(E)]
+    L.cujpegxl_b200_batch_encode.argtypes = [E, P(Nv12Input)]
+    L.cujpegxl_b200_batch_sync.argtypes = [E, P(ctypes.c_size_t)]
+    L.cujpegxl_b200_batch_frame.argtypes = [E, ctypes.c_size_t, P(ctypes.c_size_t), P(ctypes.c_size_t)]
+    L.cujpegxl_b200_batch_copy.argtypes = [E, ctypes.c_size_t, P(Output)]
+    L.cujpegxl_b200_batch_stream.argtypes = [E, P(ctypes.c_size_t)]
+    L.cujpegxl_b200_batch_lanes.argtypes = [E]
+    L.cujpegxl_b200_batch_lanes.restype = ctypes.c_uint32
+    L.cujpegxl_b200_batch_destroy.argtypes = [E]
+    L.cujpegxl_b200_batch_destroy.restype = None
     for name in ("cujpegxl_query_backend", "cujpegxl_max_output_size", "cujpegxl_encoder_create",
                  "cujpegxl_encoder_configure", "cujpegxl_encoder_encode", "cujpegxl_b200_encoder_set_debug",
                  "cujpegxl_b200_encoder_read_planes", "cujpegxl_b200_encode_planes",
                  "cujpegxl_b200_encode_host", "cujpegxl_b200_encoder_enqueue", "cujpegxl_b200_encoder_enqueue_stages",
-                 "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream"):
+                 "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream", "cujpegxl_b200_batch_create",
+                 "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync", "cujpegxl_b200_batch_frame",
+                 "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_stream"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -14,6 +14,7 @@
 
 #include "cujpegxl/cujpegxl.h"
 #include "cujpegxl_b200/cujpegxl_b200.h"
+#include "encoder_internal.h"
 #include "entropy.cuh"
 #include "frontend.cuh"
 #include "jxl_constants.cuh"
@@ -312,13 +313,14 @@ bool prepare(cujpegxl_encoder* e) {
 }
 
 bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp, const std::uint8_t* chroma,
-                   std::size_t cp, std::uint32_t stages = 3u) {
+                   std::size_t cp, std::uint32_t stages = 3u, cudaStream_t stream = nullptr) {
     jxb::FrontendTables ft{};
     if (!device_tables(e->device, &ft)) return false;
     const jxb::FrontendInputs in{luma, chroma, lp, cp, static_cast<int>(e->config.width),
                                  static_cast<int>(e->config.height)};
-    if ((stages & 1u) && !jxb::frontend_launch(in, e->fs, ft, e->fo, e->stream)) return false;
-    return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, e->stream);
+    cudaStream_t st{stream != nullptr ? stream : e->stream};
+    if ((stages & 1u) && !jxb::frontend_launch(in, e->fs, ft, e->fo, st)) return false;
+    return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, st);
 }
 
 // Waits for the encode and copies the file into `output`.
@@ -374,6 +376,28 @@ __global__ void nz_kernel(const std::int16_t* ac, const std::int8_t* acs, int bw
 }
 
 }  // namespace
+
+namespace jxb {
+
+bool encoder_prepare(cujpegxl_encoder* e) {
+    DeviceScope scope{e->device};
+    return scope.ok() && prepare(e);
+}
+
+bool encoder_launch(cujpegxl_encoder* e, const cujpegxl_nv12_input& input, cudaStream_t stream) {
+    if (input.luma == 0 || input.chroma == 0 || input.luma_pitch < e->config.width ||
+        input.chroma_pitch < e->config.width) {
+        return false;
+    }
+    return enqueue_frame(e, reinterpret_cast<const std::uint8_t*>(input.luma), input.luma_pitch,
+                         reinterpret_cast<const std::uint8_t*>(input.chroma), input.chroma_pitch, 3u, stream);
+}
+
+const unsigned long long* encoder_result_words(const cujpegxl_encoder* e) { return e->ed.result; }
+
+const std::uint8_t* encoder_output(const cujpegxl_encoder* e) { return e->ed.out; }
+
+}  // namespace jxb
 
 namespace jxb {
 // Launches the non-zero-count kernel above on `stream` (used by entry points

@@ -1,0 +1,28 @@
+// Library-internal access to an encoder for the batch entry points: launch a
+// whole encode on a caller-chosen stream (also inside a stream capture) and
+// find its device-side result words and output bytes.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cujpegxl/cujpegxl.h"
+
+namespace jxb {
+
+// Allocates or refreshes the per-geometry and per-distance state; not
+// capturable (it may allocate and upload tables).
+bool encoder_prepare(cujpegxl_encoder* e);
+
+// Enqueues one full encode (frontend + entropy + assembly) of `input` on
+// `stream`; issues only kernel launches and memsets, so it may be captured.
+bool encoder_launch(cujpegxl_encoder* e, const cujpegxl_nv12_input& input, cudaStream_t stream);
+
+// Device words written by the encode: total bytes, body start, status (0 ok).
+const unsigned long long* encoder_result_words(const cujpegxl_encoder* e);
+
+// Device address of the encoded file.
+const std::uint8_t* encoder_output(const cujpegxl_encoder* e);
+
+}  // namespace jxb

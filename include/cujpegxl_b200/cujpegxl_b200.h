@@ -119,6 +119,46 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
 /* Number of kernels one encode launches. */
 uint32_t cujpegxl_b200_kernels_per_encode(void);
 
+/* ---- Batched encode: frames of different sizes in one CUDA graph launch ----
+ * No reference counterpart (the reference encodes one frame per call). A batch
+ * owns one encoder per frame (each frame may have its own width, height and
+ * distance; all on one device). cujpegxl_b200_batch_encode enqueues the whole
+ * batch as one graph launch: lanes (CUDA streams inside the graph) take the
+ * frames largest first, each frame to the lane with the least work so far.
+ * The first encode times graphs with 1, 2, 4 and 8 lanes and keeps the
+ * fastest; later encodes with the same input addresses relaunch that graph,
+ * new addresses are recaptured and the graph updated in place. The call is
+ * asynchronous: cujpegxl_b200_batch_sync waits and reports every frame's size,
+ * after which each file can be read on the device or copied to the host. */
+typedef struct cujpegxl_b200_batch cujpegxl_b200_batch;
+
+cujpegxl_status cujpegxl_b200_batch_create(const cujpegxl_config* frames, size_t count,
+                                           cujpegxl_b200_batch** out_batch);
+
+/* inputs[count]: device NV12 frames, the same rules as cujpegxl_encoder_encode. */
+cujpegxl_status cujpegxl_b200_batch_encode(cujpegxl_b200_batch* batch, const cujpegxl_nv12_input* inputs);
+
+/* Waits for the last batch_encode; sizes[count] (may be NULL) receives the
+ * file sizes. CUJPEGXL_INTERNAL_ERROR if any frame failed. */
+cujpegxl_status cujpegxl_b200_batch_sync(cujpegxl_b200_batch* batch, size_t* sizes);
+
+/* After batch_sync: size and device address of frame `index`'s file. */
+cujpegxl_status cujpegxl_b200_batch_frame(cujpegxl_b200_batch* batch, size_t index, size_t* size,
+                                          uintptr_t* device_bytes);
+
+/* After batch_sync: copies frame `index`'s file to host memory (BUFFER_TOO_SMALL
+ * sets output->size to the required length). */
+cujpegxl_status cujpegxl_b200_batch_copy(cujpegxl_b200_batch* batch, size_t index, cujpegxl_output* output);
+
+/* The stream the batch's graph is launched on (to order or time caller work
+ * against it). */
+cujpegxl_status cujpegxl_b200_batch_stream(const cujpegxl_b200_batch* batch, uintptr_t* stream);
+
+/* Lanes the batch's graph uses (0 before the first encode). */
+uint32_t cujpegxl_b200_batch_lanes(const cujpegxl_b200_batch* batch);
+
+void cujpegxl_b200_batch_destroy(cujpegxl_b200_batch* batch);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
