@@ -323,6 +323,11 @@ def run_ours(args) -> None:
     in_bytes = BATCH * W * H * 3 // 2
 
     if rank == 0:
+        from cujpegxl_b200.decode import psnr_y
+
+        data = encs[0].encode_device(frames[0][0].data_ptr(), frames[0][1].data_ptr(), W, W)
+        quality = {"psnr_y_db": psnr_y(nv12, data), "bpp": 8.0 * len(data) / (W * H),
+                   "decoder": "in-repo subset decoder, plain dequantisation, BT.709 Y' against the input luma"}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(nv12, W, H, d, args.cpu_runs)
@@ -337,7 +342,7 @@ def run_ours(args) -> None:
                        "width": W, "height": H, "distance": d, "l2": l2,
                        "parallelism": f"{world} independent replica(s), {S} streams each"},
             "mp_per_s": value * W * H / 1e6,
-            "bytes_per_frame": size, "bpp": 8.0 * size / (W * H),
+            "bytes_per_frame": size, "bpp": 8.0 * size / (W * H), "quality": quality,
             "p50_frame_ms": p50, "p99_frame_ms": p99, "latency": "one encoder alone, per frame",
             "frontend_ms": front_ms, "entropy_ms": statistics.mean(frame_ms) - front_ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -68,7 +68,23 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if link.is_symlink() or link.exists():
             link.unlink()
         link.symlink_to(LIB.name)
+    build_decoder(force)
     return LIB
+
+
+DECODER_LIB = OUT_DIR / "libjxlsubset.so"
+
+
+def build_decoder(force: bool = False) -> Path:
+    """The host subset decoder (decodability and PSNR checks), g++ only."""
+    OUT_DIR.mkdir(exist_ok=True)
+    src = CSRC / "subset_decoder.cc"
+    deps = [src, CSRC / "subset_decoder.h", CSRC / "jxl_constants.cuh", CSRC / "jxl_math.cuh",
+            CSRC / "jxl_dequant_tables.inc"]
+    if force or _stale(DECODER_LIB, deps):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", f"-I{CSRC}", str(src), "-o",
+                        str(DECODER_LIB)], check=True)
+    return DECODER_LIB
 
 
 if __name__ == "__main__":

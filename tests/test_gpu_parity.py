@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from cujpegxl_b200 import Encoder
+from cujpegxl_b200.decode import decode_planes, psnr_y
 from cujpegxl_b200.synth import make_nv12
 from oracle import api
 
@@ -77,6 +78,26 @@ def test_4k_file_and_planes_bit_exact(d):
     for k in ("qf", "acs", "ytox", "ytob", "ac", "dc"):
         np.testing.assert_array_equal(g[k], getattr(o, k), err_msg=k)
     assert data == api.encode(nv, w, h, d)
+    # Full-size round trip through the in-repo decoder: the file holds exactly
+    # the planes the GPU computed.
+    back = decode_planes(data)
+    first = g["acs"] != 0
+    for k in ("acs", "dc", "ytox", "ytob", "ac"):
+        np.testing.assert_array_equal(back[k], g[k], err_msg=f"decoded {k}")
+    np.testing.assert_array_equal(back["qf"][first], g["qf"][first])
+
+
+def test_4k_quality_falls_with_distance():
+    w, h = 3840, 2160
+    nv = make_nv12(w, h, 0)
+    keep, luma, chroma, lp, cp = device_nv12(nv, w, h)
+    psnr = []
+    with Encoder(w, h, 0.5) as enc:
+        for d in (0.5, 1.0, 2.0, 4.0):
+            enc.configure(w, h, d)
+            psnr.append(psnr_y(nv, enc.encode_device(luma, chroma, lp, cp)))
+    assert all(a > b for a, b in zip(psnr, psnr[1:])), psnr
+    assert psnr[1] > 40.0, psnr
 
 
 def test_pitched_input_matches_packed():
