@@ -163,6 +163,13 @@ class Encoder:
         check("encoder_stream", self._L.cujpegxl_b200_encoder_stream(self._h, ctypes.byref(s)))
         return s.value
 
+    def memory(self) -> tuple[int, int]:
+        """(device bytes, pinned host bytes) the encoder holds."""
+        d = ctypes.c_size_t(0)
+        p = ctypes.c_size_t(0)
+        check("encoder_memory", self._L.cujpegxl_b200_encoder_memory(self._h, ctypes.byref(d), ctypes.byref(p)))
+        return d.value, p.value
+
 
 class Batch:
     """Frames of different sizes encoded by one CUDA graph launch

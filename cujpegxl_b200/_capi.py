@@ -31,7 +31,7 @@ EXPORTS = (
     "cujpegxl_b200_kernels_per_encode", "cujpegxl_b200_encode_planes_noalloc",
     "cujpegxl_b200_batch_create", "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync",
     "cujpegxl_b200_batch_frame", "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_lanes",
-    "cujpegxl_b200_batch_destroy", "cujpegxl_b200_batch_stream",
+    "cujpegxl_b200_batch_destroy", "cujpegxl_b200_batch_stream", "cujpegxl_b200_encoder_memory",
 )
 
 
@@ -90,6 +90,7 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_encoder_result.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encoder_stream.argtypes = [E, P(ctypes.c_size_t)]
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
+    L.cujpegxl_b200_encoder_memory.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encode_planes_noalloc.argtypes = [P(DevicePlanes), ctypes.c_uint32, ctypes.c_uint32,
                                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                                       ctypes.c_size_t, P(ctypes.c_size_t), ctypes.c_size_t]
@@ -110,7 +111,7 @@ def lib() -> ctypes.CDLL:
                  "cujpegxl_b200_encode_host", "cujpegxl_b200_encoder_enqueue", "cujpegxl_b200_encoder_enqueue_stages",
                  "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream", "cujpegxl_b200_batch_create",
                  "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync", "cujpegxl_b200_batch_frame",
-                 "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_stream"):
+                 "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_stream", "cujpegxl_b200_encoder_memory"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -44,6 +44,7 @@ struct cujpegxl_encoder {
     std::uint8_t* nv12_dev{nullptr};
     std::uint8_t* nv12_pinned{nullptr};
     unsigned long long* result_pinned{nullptr};
+    std::size_t arena_bytes{0};
     bool pending{false};
 };
 
@@ -188,6 +189,7 @@ bool allocate(cujpegxl_encoder* e) {
     void* base{nullptr};
     if (cudaMalloc(&base, a.total) != cudaSuccess) return false;
     e->arena = base;
+    e->arena_bytes = a.total;
     auto* b{static_cast<std::uint8_t*>(base)};
 
     jxb::FrontendOutputs& fo{e->fo};
@@ -692,6 +694,18 @@ cujpegxl_status cujpegxl_b200_encoder_result(cujpegxl_encoder* encoder, size_t* 
 cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_t* out_stream) {
     if (encoder == nullptr || out_stream == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
     *out_stream = reinterpret_cast<uintptr_t>(encoder->stream);
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* device_bytes,
+                                             size_t* pinned_host_bytes) {
+    if (encoder == nullptr || device_bytes == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    *device_bytes = encoder->arena_bytes;
+    if (pinned_host_bytes != nullptr) {
+        *pinned_host_bytes = encoder->nv12_pinned != nullptr
+                                 ? static_cast<std::size_t>(encoder->geo_w) * encoder->geo_h * 3 / 2 + 64
+                                 : 0;
+    }
     return CUJPEGXL_OK;
 }
 

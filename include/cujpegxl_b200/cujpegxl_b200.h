@@ -119,6 +119,13 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
 /* Number of kernels one encode launches. */
 uint32_t cujpegxl_b200_kernels_per_encode(void);
 
+/* Device memory the encoder holds for its current geometry (one arena, all of
+ * it allocated at create/configure) and its pinned host staging buffer
+ * (`pinned_host_bytes` may be NULL), for admission control by callers that
+ * run many encoders. Replaces no reference interface. */
+cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* device_bytes,
+                                             size_t* pinned_host_bytes);
+
 /* ---- Batched encode: frames of different sizes in one CUDA graph launch ----
  * No reference counterpart (the reference encodes one frame per call). A batch
  * owns one encoder per frame (each frame may have its own width, height and
