@@ -65,18 +65,30 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic() -> float | None:
-    """DRAM bytes per frontend launch at 4K from the committed ncu summary."""
+def profiled_value(key: str) -> float | None:
+    """A per-launch figure of the 4K frontend launch from the committed ncu
+    summary (lines `key: value`)."""
     f = REPO / "profiles" / "frontend_kernel_4k.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch_4k:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
                 return None
     return None
+
+
+def profiled_traffic() -> float | None:
+    """DRAM bytes per frontend launch at 4K."""
+    return profiled_value("dram_bytes_per_launch_4k")
+
+
+def sm_count() -> int:
+    import torch
+
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
 
 class ClockSampler:
@@ -247,6 +259,8 @@ def run_ours(args) -> None:
         if pg:
             pg.barrier()
     total_ms = start.elapsed_time(stop)
+    clock_summary = clocks.summary()
+    clocks_mhz = clock_summary.get("sm_mhz")
     n = args.steps * BATCH
     if pg:
         t = torch.tensor([total_ms], device="cuda")
@@ -321,6 +335,17 @@ def run_ours(args) -> None:
     p50 = sorted_ms[len(sorted_ms) // 2]
     p99 = sorted_ms[min(len(sorted_ms) - 1, int(round(0.99 * (len(sorted_ms) - 1))))]
     in_bytes = BATCH * W * H * 3 // 2
+    # The frontend is bound by instruction issue, not HBM: warp instructions
+    # per launch (one-pass ncu count at 4K, committed with the DRAM figure)
+    # over the event-timed duration, against 4 issue slots per SM per clock.
+    inst = profiled_value("warp_instructions_per_launch_4k") if (W, H) == (W_4K, H_4K) else None
+    issue = None
+    if inst is not None and clocks_mhz is not None:
+        peak_issue = sm_count() * 4 * clocks_mhz * 1e6
+        issue = {"achieved": inst / (front_ms / 1000.0), "peak": peak_issue, "unit": "warp instructions/s",
+                 "frac": inst / (front_ms / 1000.0) / peak_issue,
+                 "basis": "smsp__inst_executed.sum per 4K frontend launch / event-timed launch; peak = SMs x 4 "
+                          "schedulers x median SM clock under load"}
 
     if rank == 0:
         from cujpegxl_b200.decode import psnr_y
@@ -348,10 +373,11 @@ def run_ours(args) -> None:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(),
                          "kernel": "frontend_kernel", "algorithmic_bytes": alg, "peak_kind": peak_kind},
+            "sm_issue": issue,
             "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": W * H * 3 // 2,
                     "d2h_bytes_per_step": max(d2h) + 32, "step": f"one frame, {S} host threads"},
             "gpu_launches": kernels * n,
-            "clocks": clocks.summary(),
+            "clocks": clock_summary,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu

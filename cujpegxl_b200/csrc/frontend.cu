@@ -452,18 +452,45 @@ __global__ void __launch_bounds__(kThreads, 2)
     {
         const int cw{W >> 1};
         const int ch{H >> 1};
-        for (int i{tid}; i < kXplane; i += kThreads) {
-            const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
-            const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
-            win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
-        }
         for (int i{tid}; i < kLog2Cached; i += kThreads) sm.log2_small[i] = tb.log2_1p[i];
-        for (int i{tid}; i < kChromaWin * kChromaWin; i += kThreads) {
-            const int jx{min(max(cx0 + i % kChromaWin, 0), cw - 1)};
-            const int jy{min(max(cy0 + i / kChromaWin, 0), ch - 1)};
-            const std::uint8_t* p{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
-            win_chroma[2 * i] = p[0];
-            win_chroma[2 * i + 1] = p[1];
+        // Interior tiles whose window needs no clamping, with 4-byte aligned
+        // rows, load whole 32-bit words: luma bytes px0-4 .. px0+67 of each
+        // row (the window starts 2 bytes in), chroma pairs cx0 .. cx0+35
+        // (bytes px0-4 .. px0+67, word aligned).
+        const bool aligned{((reinterpret_cast<std::uintptr_t>(in.luma) | in.luma_pitch |
+                             reinterpret_cast<std::uintptr_t>(in.chroma) | in.chroma_pitch) & 3u) == 0};
+        if (aligned && px0 >= 4 && py0 >= 4 && px0 + 68 <= W && py0 + 68 <= H) {
+            constexpr int kLumaWords{kXs / 4};        // 17 output words per luma row
+            constexpr int kChromaWords{kChromaWin / 2};  // 18 words per chroma row
+            auto* lw{reinterpret_cast<std::uint32_t*>(win_luma)};
+            for (int i{tid}; i < kXs * kLumaWords; i += kThreads) {
+                const int row{i / kLumaWords};
+                const int w{i - row * kLumaWords};
+                const auto* src{reinterpret_cast<const std::uint32_t*>(
+                    in.luma + static_cast<std::size_t>(py0 - kHalo + row) * in.luma_pitch + px0 - 4)};
+                lw[row * kLumaWords + w] = __funnelshift_r(__ldg(&src[w]), __ldg(&src[w + 1]), 16);
+            }
+            auto* cwd{reinterpret_cast<std::uint32_t*>(win_chroma)};
+            for (int i{tid}; i < kChromaWin * kChromaWords; i += kThreads) {
+                const int row{i / kChromaWords};
+                const int w{i - row * kChromaWords};
+                const auto* src{reinterpret_cast<const std::uint32_t*>(
+                    in.chroma + static_cast<std::size_t>(cy0 + row) * in.chroma_pitch + 2 * cx0)};
+                cwd[row * kChromaWords + w] = __ldg(&src[w]);
+            }
+        } else {
+            for (int i{tid}; i < kXplane; i += kThreads) {
+                const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
+                const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
+                win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
+            }
+            for (int i{tid}; i < kChromaWin * kChromaWin; i += kThreads) {
+                const int jx{min(max(cx0 + i % kChromaWin, 0), cw - 1)};
+                const int jy{min(max(cy0 + i / kChromaWin, 0), ch - 1)};
+                const std::uint8_t* p{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
+                win_chroma[2 * i] = p[0];
+                win_chroma[2 * i + 1] = p[1];
+            }
         }
     }
     __syncthreads();
@@ -1077,52 +1104,61 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float ytox{static_cast<float>(sm.mx) * kCflColorScale};
     const float ytob{jx_fma(static_cast<float>(sm.mb), kCflColorScale, kCflBaseB)};
     const std::size_t cplane{static_cast<std::size_t>(nblocks) * 64};
-    for (int k{tid}; k < 4096; k += kThreads) {
+    for (int k{tid}; k < 4096; k += kThreads) {  // 16 uniform iterations per warp
         const int lb{k >> 6};
         const int slot{k & 63};
         const int lbx{lb & 7};
         const int lby{lb >> 3};
-        if (bx0 + lbx >= bw || by0 + lby >= bh) {
-            continue;
-        }
-        const int f{sm.owner[lb]};
-        const int n{sm.acs[f]};
-        const int side{n >> 3};
-        const int lrow{side == 1 ? 3 : (side == 2 ? 4 : 5)};  // log2(n)
-        const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
-        const int raw{q * 64 + slot};
-        const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
+        const bool inside{bx0 + lbx < bw && by0 + lby < bh};
+        const int f{inside ? static_cast<int>(sm.owner[lb]) : -1};
         std::int16_t ax{0};
         std::int16_t ay{0};
         std::int16_t ab{0};
-        if (!((raw >> lrow) < side && (raw & (n - 1)) < side)) {
-            const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
-            const float* wt{tb.dequant + si * 3072};
-            const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
-            const int ci{lb * kCoefBlock + slot};
-            const float xr{__half2float(coef[ci])};
-            const float yr{__half2float(coef[kCoefPlane + ci])};
-            const float br{__half2float(coef[2 * kCoefPlane + ci])};
-            const float wy{wt[1024 + raw]};
-            const int qy{quantize(yr, qgsf, wy)};
-            // A zero Y quantum reconstructs to a signed zero, and fma(-m, +-0, v)
-            // equals v up to the sign of a zero result, which quantises to 0
-            // either way.
-            const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy) / qgsf};
-            const float wx{wt[raw]};
-            const int qx{quantize(jx_fma(-ytox, yq, xr), qgsf, wx)};
-            const float wb{wt[2048 + raw]};
-            const int qb{quantize(jx_fma(-ytob, yq, br), qgsf, wb)};
-            ax = static_cast<std::int16_t>(qx);
-            ay = static_cast<std::int16_t>(qy);
-            ab = static_cast<std::int16_t>(qb);
-            if (ax != 0) atomicAdd(&sm.nz[0][f], 1);
-            if (ay != 0) atomicAdd(&sm.nz[1][f], 1);
-            if (ab != 0) atomicAdd(&sm.nz[2][f], 1);
+        if (inside) {
+            const int n{sm.acs[f]};
+            const int side{n >> 3};
+            const int lrow{side == 1 ? 3 : (side == 2 ? 4 : 5)};  // log2(n)
+            const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
+            const int raw{q * 64 + slot};
+            if (!((raw >> lrow) < side && (raw & (n - 1)) < side)) {
+                const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
+                const float* wt{tb.dequant + si * 3072};
+                const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
+                const int ci{lb * kCoefBlock + slot};
+                const float xr{__half2float(coef[ci])};
+                const float yr{__half2float(coef[kCoefPlane + ci])};
+                const float br{__half2float(coef[2 * kCoefPlane + ci])};
+                const float wy{wt[1024 + raw]};
+                const int qy{quantize(yr, qgsf, wy)};
+                // A zero Y quantum reconstructs to a signed zero, and
+                // fma(-m, +-0, v) equals v up to the sign of a zero result,
+                // which quantises to 0 either way.
+                const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy) / qgsf};
+                const float wx{wt[raw]};
+                const int qx{quantize(jx_fma(-ytox, yq, xr), qgsf, wx)};
+                const float wb{wt[2048 + raw]};
+                const int qb{quantize(jx_fma(-ytob, yq, br), qgsf, wb)};
+                ax = static_cast<std::int16_t>(qx);
+                ay = static_cast<std::int16_t>(qy);
+                ab = static_cast<std::int16_t>(qb);
+            }
+            const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
+            out.ac[g] = ax;
+            out.ac[cplane + g] = ay;
+            out.ac[2 * cplane + g] = ab;
         }
-        out.ac[g] = ax;
-        out.ac[cplane + g] = ay;
-        out.ac[2 * cplane + g] = ab;
+        // Non-zero counts per first block: one shared-memory add per block
+        // and channel per warp (lanes of a warp mostly share a block).
+        const unsigned peers{__match_any_sync(0xffffffffu, f)};
+        const bool leader{(__ffs(peers) - 1) == lane};
+        const unsigned mx{__ballot_sync(0xffffffffu, ax != 0) & peers};
+        const unsigned my{__ballot_sync(0xffffffffu, ay != 0) & peers};
+        const unsigned mb{__ballot_sync(0xffffffffu, ab != 0) & peers};
+        if (leader && f >= 0) {
+            if (mx) atomicAdd(&sm.nz[0][f], __popc(mx));
+            if (my) atomicAdd(&sm.nz[1][f], __popc(my));
+            if (mb) atomicAdd(&sm.nz[2][f], __popc(mb));
+        }
     }
     __syncthreads();
 
