@@ -141,6 +141,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, pg, device: str) -> float:
+    """The largest `value` over all ranks (each rank's device-timed region; the
+    job lasts as long as its slowest rank). `pg` is torch.distributed or None."""
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, world: int, ms: float) -> float:
+    """Units per second of the whole job: every rank processes the same number
+    of independent units (replicas, weak scaling) within `ms`."""
+    return world * units_per_rank / (ms / 1000.0)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -262,11 +280,8 @@ def run_ours(args) -> None:
     clock_summary = clocks.summary()
     clocks_mhz = clock_summary.get("sm_mhz")
     n = args.steps * BATCH
-    if pg:
-        t = torch.tensor([total_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n / (total_ms / 1000.0)
+    total_ms = max_over_ranks(total_ms, pg, "cuda")
+    value = whole_job_rate(n, world, total_ms)
 
     # Per-frame latency and the frontend/entropy split: one encoder alone,
     # events around each stage of each frame.
@@ -320,12 +335,8 @@ def run_ours(args) -> None:
     for t in workers:
         t.join()
     torch.cuda.synchronize()
-    e2e_ms = max(e0.elapsed_time(dn) for dn in dones)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * (e2e_n // S) * S / (e2e_ms / 1000.0)
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(dn) for dn in dones), pg, "cuda")
+    e2e = whole_job_rate((e2e_n // S) * S, world, e2e_ms)
 
     front_ms = statistics.mean(front)
     alg = frontend_algorithmic_bytes(W, H)

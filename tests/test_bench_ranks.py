@@ -1,0 +1,61 @@
+"""bench.py's multi-rank bookkeeping on CPU: two gloo ranks with different
+timed regions agree on the slowest one, and the whole-job rate counts every
+rank's frames (one replica per rank, no collective on the data path)."""
+
+from __future__ import annotations
+
+import os
+import socket
+import sys
+from pathlib import Path
+
+import torch.multiprocessing as mp
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, out) -> None:
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ms = bench.max_over_ranks(100.0 + 25.0 * rank, dist, "cpu")
+        out.put((rank, ms, bench.whole_job_rate(320, world, ms)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_the_slowest_rank_and_count_all_frames():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in results] == [125.0, 125.0]
+    assert all(abs(r[2] - 2 * 320 / 0.125) < 1e-6 for r in results)
+
+
+def test_single_rank_needs_no_process_group():
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+    assert bench.whole_job_rate(16, 1, 20.0) == 800.0
