@@ -446,6 +446,7 @@ struct WarpCodeSmem {
     std::uint16_t bits[256];
     std::uint16_t used[256];   // compacted list of used symbols
     std::uint8_t desc[kDescBytes];
+    CodeLengthScratch cl;
 };
 
 // Depths for a histogram with at least two used symbols, warp-cooperative:
@@ -510,32 +511,34 @@ __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, in
     warp_create_tree(s, length, 15, lane);
     if (lane == 0) {
         canonical_codes(s.depth, length, s.bits);
-        store_code_header(count, s4, length, s.depth, w);
+        store_code_header(count, s4, length, s.depth, w, s.cl);
     }
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(512) codes_kernel(EntropyDev e) {
+// One single-warp CTA per histogram (the 32 AC clusters, then the DC and the
+// AcMetadata histogram of every DC group): the construction is a long serial
+// chain on lane 0, so each chain gets an SM to itself.
+__global__ void __launch_bounds__(32) codes_kernel(EntropyDev e) {
     extern __shared__ __align__(16) unsigned char code_smem[];
-    const int warp{static_cast<int>(threadIdx.x) >> 5};
     const int lane{static_cast<int>(threadIdx.x) & 31};
-    WarpCodeSmem& s{reinterpret_cast<WarpCodeSmem*>(code_smem)[warp]};
+    WarpCodeSmem& s{*reinterpret_cast<WarpCodeSmem*>(code_smem)};
     int idx;
     const std::uint32_t* src;
     std::uint8_t* dst_depth;
     std::uint16_t* dst_bits;
     bool clustered;
     std::uint32_t extra0{0};
-    if (blockIdx.x < 2) {
-        const int c{static_cast<int>(blockIdx.x) * 16 + warp};
+    if (blockIdx.x < kNumClusters) {
+        const int c{static_cast<int>(blockIdx.x)};
         idx = c;
         src = e.ac_hist + c * 256;
         dst_depth = e.ac_depth + c * 256;
         dst_bits = e.ac_bits + c * 256;
         clustered = true;
     } else {
-        if (warp >= 2) return;
-        const int g{static_cast<int>(blockIdx.x) - 2};
+        const int g{(static_cast<int>(blockIdx.x) - kNumClusters) >> 1};
+        const int warp{(static_cast<int>(blockIdx.x) - kNumClusters) & 1};
         if (warp == 0) {
             idx = 32 + g;
             src = e.dc_hist + g * 256;
@@ -768,19 +771,76 @@ __device__ void put_u32(BitSink& w, const U32Dist* d, std::uint32_t value) {
 
 constexpr int kLayoutThreads = 256;
 
-// Sizes the sections in parallel, then one thread writes the container
-// framing, codestream headers, frame header and TOC
-// (src/bitstream/codestream.cc:57-135, src/bitstream/container.cc:35-62) into
-// shared memory; the block copies them out and places the sections. Dynamic
-// shared memory: the section sizes, then the header (layout_head_bytes).
+// TOC entry of a section of `bytes` bytes: U32 with selectors 0 + 10 bits,
+// 1024 + 14, 17408 + 22, 4211712 + 30 (src/bitstream/codestream.cc:16-18, 91-98);
+// the smallest selector that holds the value, as one LSB-first field.
+__device__ __forceinline__ void toc_entry(std::uint32_t bytes, std::uint32_t& nbits, std::uint32_t& field) {
+    std::uint32_t sel;
+    std::uint32_t base;
+    std::uint32_t extra;
+    if (bytes < 1024u) {
+        sel = 0; base = 0; extra = 10;
+    } else if (bytes < 17408u) {
+        sel = 1; base = 1024; extra = 14;
+    } else if (bytes < 4211712u) {
+        sel = 2; base = 17408; extra = 22;
+    } else {
+        sel = 3; base = 4211712; extra = 30;
+    }
+    nbits = 2 + extra;
+    field = sel | ((bytes - base) << 2);
+}
+
+// Block-wide exclusive scan of one 64-bit value per thread; returns the
+// thread's offset and sets `total`.
+__device__ unsigned long long block_scan(unsigned long long v, unsigned long long* warp_sums,
+                                         unsigned long long& total) {
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const int warp{static_cast<int>(threadIdx.x) >> 5};
+    unsigned long long incl{v};
+#pragma unroll
+    for (int off{1}; off < 32; off <<= 1) {
+        const unsigned long long t{__shfl_up_sync(kFull, incl, off)};
+        if (lane >= off) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw{static_cast<int>(blockDim.x) >> 5};
+        const unsigned long long ws{lane < nw ? warp_sums[lane] : 0ull};
+        unsigned long long wi{ws};
+#pragma unroll
+        for (int off{1}; off < 32; off <<= 1) {
+            const unsigned long long t{__shfl_up_sync(kFull, wi, off)};
+            if (lane >= off) wi += t;
+        }
+        if (lane < nw) warp_sums[lane] = wi - ws;
+        if (lane == nw - 1) warp_sums[32] = wi;
+    }
+    __syncthreads();
+    const unsigned long long off{warp_sums[warp] + incl - v};
+    total = warp_sums[32];
+    __syncthreads();
+    return off;
+}
+
+// Sizes the sections, then writes the codestream headers and frame header
+// (one thread), the TOC (every thread its own entries, placed by a scan of
+// their bit lengths), the container framing and the section positions
+// (src/bitstream/codestream.cc:57-135, src/bitstream/container.cc:35-62).
+// Dynamic shared memory: the section sizes, then the header words
+// (layout_head_bytes).
 __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
     extern __shared__ __align__(16) unsigned char layout_smem[];
-    __shared__ unsigned long long sh_total, sh_start, sh_status, sh_head;
+    __shared__ unsigned long long scan_sums[33];
+    __shared__ unsigned long long sh_start, sh_status, sh_head;
+    __shared__ std::uint32_t sh_toc_start;
     auto* sec_bytes{reinterpret_cast<std::uint32_t*>(layout_smem)};
     const std::uint32_t head_cap{layout_head_bytes(e.nsec)};
     std::uint8_t* head{layout_smem + layout_sizes_bytes(e.nsec)};
+    auto* head_words{reinterpret_cast<unsigned int*>(head)};
     const int tid{static_cast<int>(threadIdx.x)};
-    for (std::uint32_t i{static_cast<std::uint32_t>(tid)}; i < head_cap; i += kLayoutThreads) head[i] = 0;
+    for (std::uint32_t i{static_cast<std::uint32_t>(tid)}; i < head_cap / 4; i += kLayoutThreads) head_words[i] = 0;
     for (int s{tid}; s < e.nsec; s += kLayoutThreads) {
         const Section sec{e.sections[s]};
         const unsigned long long bits{prefix_at(e, sec.first + sec.count) - prefix_at(e, sec.first)};
@@ -790,7 +850,6 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
     if (tid == 0) {
         BitSink w{head, 0, head_cap * 8, false};
         const U32Dist dim[4]{{false, 1, 9}, {false, 1, 13}, {false, 1, 18}, {false, 1, 30}};
-        const U32Dist toc[4]{{false, 0, 10}, {false, 1024, 14}, {false, 17408, 22}, {false, 4211712, 30}};
         w.put(8, 0xFF);
         w.put(8, 0x0A);
         const std::uint32_t W{static_cast<std::uint32_t>(e.width)};
@@ -821,21 +880,47 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
         w.put(2, 0);
         w.put(1, 0);  // TOC without permutation
         w.pos = (w.pos + 7) & ~7u;
-        unsigned long long body{0};
-        for (int s{0}; s < e.nsec; ++s) {
-            put_u32(w, toc, sec_bytes[s]);
-            body += sec_bytes[s];
+        sh_toc_start = w.pos;
+    }
+    __syncthreads();
+    // Each thread takes a contiguous run of sections.
+    const int per{(e.nsec + kLayoutThreads - 1) / kLayoutThreads};
+    const int lo{min(e.nsec, tid * per)};
+    const int hi{min(e.nsec, lo + per)};
+    unsigned long long my_bits{0};
+    unsigned long long my_bytes{0};
+    for (int s{lo}; s < hi; ++s) {
+        std::uint32_t nb, field;
+        toc_entry(sec_bytes[s], nb, field);
+        my_bits += nb;
+        my_bytes += sec_bytes[s];
+    }
+    unsigned long long toc_bits{0};
+    unsigned long long body{0};
+    const unsigned long long bit_off{block_scan(my_bits, scan_sums, toc_bits)};
+    const unsigned long long byte_off{block_scan(my_bytes, scan_sums, body)};
+    {
+        unsigned long long p{sh_toc_start + bit_off};
+        for (int s{lo}; s < hi; ++s) {
+            std::uint32_t nb, field;
+            toc_entry(sec_bytes[s], nb, field);
+            const std::uint32_t off{static_cast<std::uint32_t>(p & 31)};
+            atomicOr(&head_words[p >> 5], field << off);
+            if (off + nb > 32) atomicOr(&head_words[(p >> 5) + 1], field >> (32 - off));
+            p += nb;
         }
-        w.pos = (w.pos + 7) & ~7u;
-        const unsigned long long head_bytes{w.pos / 8};
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const unsigned long long head_bytes{(sh_toc_start + toc_bits + 7) / 8};
         const unsigned long long cs{head_bytes + body};
         const bool large{cs >= 0x100000000ull - 8};
         const unsigned long long framing{32ull + (large ? 16 : 8)};
-        sh_total = framing + cs;
+        const unsigned long long total{framing + cs};
         sh_head = head_bytes;
         sh_start = framing + head_bytes;
-        sh_status = w.overflow ? 2ull : (sh_total > e.out_capacity ? 1ull : 0ull);
-        e.result[0] = sh_total;
+        sh_status = total > e.out_capacity ? 1ull : 0ull;
+        e.result[0] = total;
         e.result[1] = sh_start;
         e.result[2] = sh_status;
         if (sh_status == 0) {
@@ -853,15 +938,17 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
             if (large) {
                 for (int i{0}; i < 8; ++i) e.out[at++] = static_cast<std::uint8_t>(box >> (8 * (7 - i)));
             }
-            unsigned long long pos{sh_start};
-            for (int s{0}; s < e.nsec; ++s) {
-                e.sec_pos[s] = pos;
-                pos += sec_bytes[s];
-            }
         }
     }
     __syncthreads();
     if (sh_status != 0) return;
+    {
+        unsigned long long pos{sh_start + byte_off};
+        for (int s{lo}; s < hi; ++s) {
+            e.sec_pos[s] = pos;
+            pos += sec_bytes[s];
+        }
+    }
     const unsigned long long framing{sh_start - sh_head};
     for (unsigned long long i{static_cast<unsigned long long>(tid)}; i < sh_head; i += kLayoutThreads) {
         e.out[framing + i] = head[i];
@@ -1075,7 +1162,7 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
     ac_hist_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(e);
     misc_hist_kernel<<<misc, 256, 0, st>>>(e);
-    codes_kernel<<<2 + e.ndc, 512, sizeof(WarpCodeSmem) * 16, st>>>(e);
+    codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
     ac_bits_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
     misc_bits_kernel<<<misc, 256, 0, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
@@ -1089,7 +1176,7 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
 
 bool entropy_kernels_init() {
     return cudaFuncSetAttribute(codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(WarpCodeSmem) * 16)) == cudaSuccess &&
+                                static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
            cudaFuncSetAttribute(ac_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

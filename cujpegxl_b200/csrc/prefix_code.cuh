@@ -156,11 +156,22 @@ JX_HD void canonical_codes(const std::uint8_t* depth, int len, std::uint16_t* bi
     }
 }
 
+// Working arrays of the code-length code (kept in shared memory by the
+// device builder, on the stack by host callers).
+struct CodeLengthScratch {
+    std::uint32_t hist[18];
+    std::uint8_t cl_depth[18];
+    std::uint16_t cl_bits[18];
+    HuffNode pool[40];
+    std::uint8_t level[40];
+};
+
 // Header of a code with more than four used symbols (code-length-code form).
-JX_HD void store_complex(const std::uint8_t* depths, int num, BitSink& w) {
+JX_HD void store_complex(const std::uint8_t* depths, int num, BitSink& w, CodeLengthScratch& scr) {
     int new_len{num};
     while (new_len > 0 && depths[new_len - 1] == 0) --new_len;
-    std::uint32_t hist[18]{};
+    std::uint32_t* hist{scr.hist};
+    for (int i{0}; i < 18; ++i) hist[i] = 0;
     for (int i{0}; i < new_len; ++i) ++hist[depths[i]];
     int num_codes{0};
     int code{0};
@@ -175,11 +186,13 @@ JX_HD void store_complex(const std::uint8_t* depths, int num, BitSink& w) {
             }
         }
     }
-    std::uint8_t cl_depth[18]{};
-    std::uint16_t cl_bits[18]{};
-    HuffNode pool[40];
-    std::uint8_t level[40];
-    create_tree_serial(hist, 18, 5, cl_depth, pool, level);
+    std::uint8_t* cl_depth{scr.cl_depth};
+    std::uint16_t* cl_bits{scr.cl_bits};
+    for (int i{0}; i < 18; ++i) {
+        cl_depth[i] = 0;
+        cl_bits[i] = 0;
+    }
+    create_tree_serial(hist, 18, 5, cl_depth, scr.pool, scr.level);
     canonical_codes(cl_depth, 18, cl_bits);
     constexpr std::uint8_t kOrder[18]{1, 2, 3, 4, 0, 5, 17, 6, 16, 7, 8, 9, 10, 11, 12, 13, 14, 15};
     constexpr std::uint8_t kSym[6]{0, 7, 3, 2, 1, 15};
@@ -228,7 +241,8 @@ JX_HD unsigned alphabet_bits(int length) {
 }
 
 // Header for a code whose depths are already built (count >= 2).
-JX_HD void store_code_header(int count, int* s4, int length, const std::uint8_t* depth, BitSink& w) {
+JX_HD void store_code_header(int count, int* s4, int length, const std::uint8_t* depth, BitSink& w,
+                             CodeLengthScratch& scr) {
     const unsigned max_bits{alphabet_bits(length)};
     if (count <= 4) {
         w.put(2, 1);
@@ -245,7 +259,7 @@ JX_HD void store_code_header(int count, int* s4, int length, const std::uint8_t*
         for (int i{0}; i < count; ++i) w.put(max_bits, static_cast<std::uint32_t>(s4[i]));
         if (count == 4) w.put(1, depth[s4[0]] == 1 ? 1 : 0);
     } else {
-        store_complex(depth, length, w);
+        store_complex(depth, length, w, scr);
     }
 }
 
@@ -265,7 +279,8 @@ JX_HD void build_and_store_serial(const std::uint32_t* hist, int length, std::ui
     }
     create_tree_serial(hist, length, 15, depth, pool, level);
     canonical_codes(depth, length, bits);
-    store_code_header(count, s4, length, depth, w);
+    CodeLengthScratch scr;
+    store_code_header(count, s4, length, depth, w, scr);
 }
 
 // Hybrid-uint configuration fields (src/bitstream/histogram_writer.cc:74-81),
