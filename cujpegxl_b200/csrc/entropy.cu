@@ -1059,10 +1059,23 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
 }
 
+// A header blob long enough to be written by the whole CTA (the AcGlobal
+// prefix with its context map runs to tens of thousands of bits).
+struct DeferredBlob {
+    unsigned int* words;
+    unsigned long long pos;
+    const std::uint8_t* src;  // 4-byte aligned, readable in whole words
+    std::uint32_t nbits;
+};
+constexpr int kMaxDeferred = 32;
+constexpr std::uint32_t kDeferBits = 256;
+
 struct EmitVisitor {
     const EntropyDev* e;
     unsigned int* words;
     unsigned long long pos;
+    DeferredBlob* deferred{nullptr};
+    int* ndeferred{nullptr};
     __device__ void put(std::uint32_t n, std::uint32_t v) {
         if (n == 0) return;
         if (n < 32) v &= (1u << n) - 1u;
@@ -1070,6 +1083,14 @@ struct EmitVisitor {
         pos += n;
     }
     __device__ void blob(const std::uint8_t* b, std::uint32_t nbits) {
+        if (deferred != nullptr && nbits > kDeferBits) {
+            const int k{atomicAdd(ndeferred, 1)};
+            if (k < kMaxDeferred) {
+                deferred[k] = DeferredBlob{words, pos, b, nbits};
+                pos += nbits;
+                return;
+            }
+        }
         std::uint32_t i{0};
         for (; i + 32 <= nbits; i += 32) {
             put(32, static_cast<std::uint32_t>(b[i >> 3]) | (static_cast<std::uint32_t>(b[(i >> 3) + 1]) << 8) |
@@ -1107,13 +1128,16 @@ constexpr int kMiscWindowWords = 2048;
 // first item's section are assembled in a shared-memory window.
 __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
     __shared__ unsigned int win[kMiscWindowWords];
+    __shared__ DeferredBlob deferred[kMaxDeferred];
     __shared__ unsigned long long sh_start;
     __shared__ std::uint32_t sh_end;
     __shared__ int sh_words;
+    __shared__ int sh_ndeferred;
     if (e.result[2] != 0) return;
     const std::uint32_t first{blockIdx.x * blockDim.x};
     const std::uint32_t item{first + threadIdx.x};
     if (threadIdx.x == 0) {
+        sh_ndeferred = 0;
         const int s0{find_section(e.sections, 0, misc_hi(e), first)};
         const Section sec{e.sections[s0]};
         const std::uint32_t end{min(min(first + blockDim.x, sec.first + sec.count), e.ac_first)};
@@ -1135,8 +1159,21 @@ __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
         const unsigned long long pos{e.sec_pos[s] * 8 + (prefix_at(e, item) - prefix_at(e, sec.first))};
         const bool in_window{nwords >= 0 && item < sh_end};
         EmitVisitor v{&e, in_window ? win : reinterpret_cast<unsigned int*>(e.out),
-                      in_window ? pos - ((sh_start >> 5) << 5) : pos};
+                      in_window ? pos - ((sh_start >> 5) << 5) : pos, deferred, &sh_ndeferred};
         visit_misc(e, item, v);
+    }
+    __syncthreads();
+    // Long blobs, one 32-bit word of each per thread.
+    const int nd{min(sh_ndeferred, kMaxDeferred)};
+    for (int k{0}; k < nd; ++k) {
+        const DeferredBlob d{deferred[k]};
+        const auto* src{reinterpret_cast<const std::uint32_t*>(d.src)};
+        for (std::uint32_t w{threadIdx.x}; 32 * w < d.nbits; w += blockDim.x) {
+            const std::uint32_t n{min(32u, d.nbits - 32 * w)};
+            std::uint32_t v{src[w]};
+            if (n < 32) v &= (1u << n) - 1u;
+            put_bits_at(d.words, d.pos + 32ull * w, n, v);
+        }
     }
     __syncthreads();
     if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
