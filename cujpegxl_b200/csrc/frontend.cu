@@ -288,6 +288,23 @@ __device__ __forceinline__ void row_pass(const float* src, float* dst) {
 // sampled at the coefficient's frequency and stores its distortion and rate
 // contributions (zero for the low-frequency corner), as in block_ac_cost
 // (src/transform_select_impl.cuh:80-106).
+// Distortion and rate of a selection coefficient whose quantum may be non-zero
+// (block_ac_cost, src/transform_select_impl.cuh:80-106). Kept out of line:
+// the unrolled column passes call it from hundreds of sites, and one shared
+// body keeps their code small enough for the instruction caches.
+__device__ __noinline__ float2 sel_cost_nonzero(float coeff, float scaled, float w, float qgsf, const float* l2t,
+                                                const float* l2s) {
+    const float q{rintf(scaled / w)};
+    const float err{(q * w) / qgsf - coeff};
+    float rt{0.0f};
+    if (q != 0.0f) {
+        int a{static_cast<int>(fabsf(q))};
+        a = a < kLog2TableSize ? a : kLog2TableSize - 1;
+        rt = 1.0f + (a < kLog2Cached ? l2s[a] : l2t[a]);
+    }
+    return make_float2(err * err, rt);
+}
+
 template <int N, int Y0, int Y1>
 __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, float* cr_fx, int fx,
                                         float qgsf, const float* wsel, const float* l2t,
@@ -314,14 +331,9 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
                 // is zero and err is -coeff exactly: the same d, no rate.
                 d = coeff * coeff;
             } else {
-                const float q{rintf(scaled / w)};
-                const float err{(q * w) / qgsf - coeff};
-                d = err * err;
-                if (q != 0.0f) {
-                    int a{static_cast<int>(fabsf(q))};
-                    a = a < kLog2TableSize ? a : kLog2TableSize - 1;
-                    rt = 1.0f + (a < kLog2Cached ? l2s[a] : l2t[a]);
-                }
+                const float2 dr{sel_cost_nonzero(coeff, scaled, w, qgsf, l2t, l2s)};
+                d = dr.x;
+                rt = dr.y;
             }
         }
         cd_fx[fy] = d;
