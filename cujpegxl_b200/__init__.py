@@ -59,6 +59,7 @@ class Encoder:
         check("encoder_create", self._L.cujpegxl_encoder_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self.width, self.height, self.distance, self.device_ordinal = width, height, distance, device_ordinal
         self._buf = np.zeros(max_output_size(width, height, distance, device_ordinal), np.uint8)
+        self._net = None
 
     def close(self) -> None:
         if self._h:
@@ -162,6 +163,21 @@ class Encoder:
         s = ctypes.c_size_t(0)
         check("encoder_stream", self._L.cujpegxl_b200_encoder_stream(self._h, ctypes.byref(s)))
         return s.value
+
+    def set_acsnet(self, net, margin: float = 0.2, flags: int = 1) -> None:
+        """Attach a transform-decision network (cujpegxl_b200.acsnet.AcsNet;
+        None detaches). flags: 1 = split only, 3 = split and quant field."""
+        check("encoder_set_acsnet", self._L.cujpegxl_b200_encoder_set_acsnet(
+            self._h, None if net is None else net.handle, margin, flags))
+        self._net = net
+
+    def acsnet_stats(self) -> tuple[int, int]:
+        """(regions the network decided, full 32x32 regions) of the last encode."""
+        d = ctypes.c_uint32(0)
+        r = ctypes.c_uint32(0)
+        check("encoder_acsnet_stats", self._L.cujpegxl_b200_encoder_acsnet_stats(self._h, ctypes.byref(d),
+                                                                                 ctypes.byref(r)))
+        return d.value, r.value
 
     def memory(self) -> tuple[int, int]:
         """(device bytes, pinned host bytes) the encoder holds."""

@@ -32,6 +32,11 @@ EXPORTS = (
     "cujpegxl_b200_batch_create", "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync",
     "cujpegxl_b200_batch_frame", "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_lanes",
     "cujpegxl_b200_batch_destroy", "cujpegxl_b200_batch_stream", "cujpegxl_b200_encoder_memory",
+    "cujpegxl_b200_acsnet_param_count", "cujpegxl_b200_acsnet_check_blob", "cujpegxl_b200_acsnet_create",
+    "cujpegxl_b200_acsnet_destroy", "cujpegxl_b200_encoder_set_acsnet", "cujpegxl_b200_encoder_acsnet_stats",
+    "cujpegxl_b200_acsnet_trainer_create", "cujpegxl_b200_acsnet_trainer_destroy",
+    "cujpegxl_b200_acsnet_trainer_forward", "cujpegxl_b200_acsnet_trainer_gradient",
+    "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params",
 )
 
 
@@ -51,6 +56,11 @@ class Output(ctypes.Structure):
 
 class Planes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("ac", "dc", "acs", "qf", "ytox", "ytob", "xyb", "sharp", "coeff")]
+
+
+class NetBatch(ctypes.Structure):
+    _fields_ = [("tiles", ctypes.c_size_t), ("tile_index", ctypes.c_size_t), ("log2_distance", ctypes.c_size_t),
+                ("label_class", ctypes.c_size_t), ("label_qf", ctypes.c_size_t), ("n", ctypes.c_uint32)]
 
 
 class DevicePlanes(ctypes.Structure):
@@ -105,13 +115,34 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_batch_lanes.restype = ctypes.c_uint32
     L.cujpegxl_b200_batch_destroy.argtypes = [E]
     L.cujpegxl_b200_batch_destroy.restype = None
+    F = ctypes.c_float
+    L.cujpegxl_b200_acsnet_param_count.restype = ctypes.c_uint32
+    L.cujpegxl_b200_acsnet_check_blob.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
+    L.cujpegxl_b200_acsnet_create.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, P(E)]
+    L.cujpegxl_b200_acsnet_destroy.argtypes = [E]
+    L.cujpegxl_b200_acsnet_destroy.restype = None
+    L.cujpegxl_b200_encoder_set_acsnet.argtypes = [E, E, F, ctypes.c_uint32]
+    L.cujpegxl_b200_encoder_acsnet_stats.argtypes = [E, P(ctypes.c_uint32), P(ctypes.c_uint32)]
+    L.cujpegxl_b200_acsnet_trainer_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                      ctypes.c_int32, P(E)]
+    L.cujpegxl_b200_acsnet_trainer_destroy.argtypes = [E]
+    L.cujpegxl_b200_acsnet_trainer_destroy.restype = None
+    L.cujpegxl_b200_acsnet_trainer_forward.argtypes = [E, P(NetBatch), ctypes.c_size_t, ctypes.c_size_t]
+    L.cujpegxl_b200_acsnet_trainer_gradient.argtypes = [E, P(NetBatch), F, ctypes.c_size_t, ctypes.c_size_t,
+                                                        ctypes.c_size_t]
+    L.cujpegxl_b200_acsnet_trainer_step.argtypes = [E, P(NetBatch), F, F, ctypes.c_size_t, ctypes.c_size_t]
+    L.cujpegxl_b200_acsnet_trainer_params.argtypes = [E, ctypes.c_void_p]
     for name in ("cujpegxl_query_backend", "cujpegxl_max_output_size", "cujpegxl_encoder_create",
                  "cujpegxl_encoder_configure", "cujpegxl_encoder_encode", "cujpegxl_b200_encoder_set_debug",
                  "cujpegxl_b200_encoder_read_planes", "cujpegxl_b200_encode_planes",
                  "cujpegxl_b200_encode_host", "cujpegxl_b200_encoder_enqueue", "cujpegxl_b200_encoder_enqueue_stages",
                  "cujpegxl_b200_encoder_result", "cujpegxl_b200_encoder_stream", "cujpegxl_b200_batch_create",
                  "cujpegxl_b200_batch_encode", "cujpegxl_b200_batch_sync", "cujpegxl_b200_batch_frame",
-                 "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_stream", "cujpegxl_b200_encoder_memory"):
+                 "cujpegxl_b200_batch_copy", "cujpegxl_b200_batch_stream", "cujpegxl_b200_encoder_memory",
+                 "cujpegxl_b200_acsnet_check_blob", "cujpegxl_b200_acsnet_create", "cujpegxl_b200_encoder_set_acsnet",
+                 "cujpegxl_b200_encoder_acsnet_stats", "cujpegxl_b200_acsnet_trainer_create",
+                 "cujpegxl_b200_acsnet_trainer_forward", "cujpegxl_b200_acsnet_trainer_gradient",
+                 "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -1,0 +1,1163 @@
+// Transform-decision network: inference inside an encode, and the training
+// kernels (forward, backward-data, weight gradients, Adam) behind the C ABI.
+//
+// Every contraction is a BF16 x BF16 -> FP32 warp MMA (m16n8k16) fed by
+// ldmatrix from shared memory. Convolutions are implicit GEMMs: the im2col
+// row of an output position and eight consecutive reduction columns (one
+// tap, eight input channels) is one 16-byte chunk of the [pixel][channel]
+// activation buffer, or a zero chunk where the tap falls into the padding.
+// The same chunk addressing serves the three products of training:
+//   forward        Y[p][co]  = im2col(X)[p][k]  . W[co][k]^T
+//   data gradient  dX[q][ci] = sum over (tap, co) of dY[p(q, tap)][co] . W[co][tap, ci]
+//                  (a gather per input pixel, grouped by pixel parity for
+//                  stride 2, so no scatter or atomics are needed)
+//   weight grad.   dW[co][k] = dY[p][co]^T . im2col(X)[p][k]
+// Reductions run in a fixed order, so training is deterministic.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "acsnet.cuh"
+#include "cujpegxl/cujpegxl.h"
+#include "cujpegxl_b200/cujpegxl_b200.h"
+#include "frontend.cuh"
+#include "jxl_constants.cuh"
+#include "xyb.cuh"
+
+namespace jxb {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kNetThreads = 128;   // inference and training forward/backward CTAs
+constexpr int kGradThreads = 256;  // weight-gradient CTAs
+constexpr int kW1S = 88;           // shared-memory row stride of W1 (BF16)
+constexpr int kWS = 296;           // row stride of W2..W4
+constexpr int kActS = 40;          // pixel stride of 32-channel activations
+
+// Weights and one region's activations. Row strides of 88/296/40 BF16 put the
+// eight rows of every ldmatrix on distinct bank groups (stride-1 access).
+struct NetSmem {
+    bf16 w1[kNetC * kW1S];
+    bf16 w[3][kNetC * kWS];
+    float bias[4][kNetC];
+    bf16 zero[8];
+    bf16 x1[1024 * kNetIn];
+    bf16 x2[256 * kActS];
+    bf16 x3[64 * kActS];
+    bf16 x4[16 * kActS];
+    float out[16 * kNetC];
+};
+
+struct TrainSmem {
+    NetSmem n;
+    bf16 g1[256 * kActS];
+    bf16 g2[64 * kActS];
+    bf16 g3[16 * kActS];
+    bf16 g4[16 * kActS];
+};
+
+static_assert(sizeof(NetSmem) % 16 == 0 && sizeof(TrainSmem) % 16 == 0, "16-byte shared-memory layout");
+// Two inference CTAs per SM.
+static_assert(2 * (sizeof(NetSmem) + 1024) <= 228 * 1024, "inference CTA too large");
+
+__device__ __forceinline__ unsigned saddr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], unsigned a) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], unsigned a) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ldsm_x2(unsigned (&r)[2], unsigned a) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0, %1}, [%2];\n"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(a)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ldsm_x2_t(unsigned (&r)[2], unsigned a) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0, %1}, [%2];\n"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(a)
+                 : "memory");
+}
+
+// D += A . B for one 16x8x16 tile (A row-major 16x16, B column-major 16x8).
+__device__ __forceinline__ void mma(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void store_pair(bf16* dst, float lo, float hi) {
+    *reinterpret_cast<__nv_bfloat162*>(dst) = __floats2bfloat162_rn(lo, hi);
+}
+
+// Shared-memory address of im2col row p, reduction columns k0..k0+7, for a
+// 3x3 convolution with padding 1 over a kInW x kInW input of kCin channels
+// stored kInS apart; the zero chunk where the tap is padding.
+template <int kInW, int kStride, int kCin, int kInS>
+__device__ __forceinline__ unsigned im2col_row(unsigned in, unsigned zero, int p, int k0) {
+    constexpr int kOutW{kInW / kStride};
+    const int tap{k0 / kCin};
+    const int ci{k0 - tap * kCin};
+    const int oy{p / kOutW};
+    const int ox{p - oy * kOutW};
+    const int iy{oy * kStride + tap / 3 - 1};
+    const int ix{ox * kStride + tap % 3 - 1};
+    const bool ok{tap < 9 && iy >= 0 && iy < kInW && ix >= 0 && ix < kInW};
+    return ok ? in + 2u * static_cast<unsigned>((iy * kInW + ix) * kInS + ci) : zero;
+}
+
+// Forward of a layer with at least four 16-row position tiles (L1, L2): warp w
+// takes position tiles w, w+4, ... and all four 8-channel output tiles.
+template <int kInW, int kStride, int kCin, int kInS, int kK, int kWStr>
+__device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* out,
+                                         int warp, int lane) {
+    constexpr int kOutW{kInW / kStride};
+    constexpr int kMW{kOutW * kOutW / 64};
+    float acc[kMW][4][4];
+#pragma unroll
+    for (int i{0}; i < kMW; ++i) {
+#pragma unroll
+        for (int n{0}; n < 4; ++n) {
+#pragma unroll
+            for (int j{0}; j < 4; ++j) acc[i][n][j] = 0.0f;
+        }
+    }
+#pragma unroll 2
+    for (int k0{0}; k0 < kK; k0 += 16) {
+        unsigned b[4][2];
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            unsigned r[4];
+            ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kWStr + k0 +
+                                                      ((lane >> 3) & 1) * 8));
+            b[2 * h][0] = r[0];
+            b[2 * h][1] = r[1];
+            b[2 * h + 1][0] = r[2];
+            b[2 * h + 1][1] = r[3];
+        }
+#pragma unroll
+        for (int i{0}; i < kMW; ++i) {
+            unsigned a[4];
+            ldsm_x4(a, im2col_row<kInW, kStride, kCin, kInS>(in, zero, (warp + 4 * i) * 16 + (lane & 15),
+                                                             k0 + (lane >> 4) * 8));
+#pragma unroll
+            for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
+        }
+    }
+#pragma unroll
+    for (int i{0}; i < kMW; ++i) {
+        const int p{(warp + 4 * i) * 16 + (lane >> 2)};
+#pragma unroll
+        for (int n{0}; n < 4; ++n) {
+            const int c{n * 8 + 2 * (lane & 3)};
+            const float b0{bias[c]};
+            const float b1{bias[c + 1]};
+            store_pair(out + p * kActS + c, fmaxf(acc[i][n][0] + b0, 0.0f), fmaxf(acc[i][n][1] + b1, 0.0f));
+            store_pair(out + (p + 8) * kActS + c, fmaxf(acc[i][n][2] + b0, 0.0f), fmaxf(acc[i][n][3] + b1, 0.0f));
+        }
+    }
+}
+
+// Forward of a layer with one 16-row position tile (L3, L4): warp w takes
+// output channels 8w..8w+7. kRelu: BF16 activations; else FP32 outputs.
+template <int kInW, int kStride, bool kRelu>
+__device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* outb,
+                                         float* outf, int warp, int lane) {
+    float acc[4]{0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 3
+    for (int k0{0}; k0 < kNetK; k0 += 16) {
+        unsigned a[4];
+        ldsm_x4(a, im2col_row<kInW, kStride, kNetC, kActS>(in, zero, lane & 15, k0 + (lane >> 4) * 8));
+        unsigned b[2];
+        ldsm_x2(b, w + 2u * static_cast<unsigned>((8 * warp + (lane & 7)) * kWS + k0 + ((lane >> 3) & 1) * 8));
+        mma(acc, a, b[0], b[1]);
+    }
+    const int p{lane >> 2};
+    const int c{8 * warp + 2 * (lane & 3)};
+    const float v0{acc[0] + bias[c]};
+    const float v1{acc[1] + bias[c + 1]};
+    const float v2{acc[2] + bias[c]};
+    const float v3{acc[3] + bias[c + 1]};
+    if (kRelu) {
+        store_pair(outb + p * kActS + c, fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+        store_pair(outb + (p + 8) * kActS + c, fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
+    } else {
+        outf[p * kNetC + c] = v0;
+        outf[p * kNetC + c + 1] = v1;
+        outf[(p + 8) * kNetC + c] = v2;
+        outf[(p + 8) * kNetC + c + 1] = v3;
+    }
+}
+
+// Gradient into a BF16 buffer, zero where the layer input (post-ReLU) is zero.
+__device__ __forceinline__ void store_masked(bf16* g, const bf16* x, int at, float v0, float v1) {
+    const __nv_bfloat162 xv{*reinterpret_cast<const __nv_bfloat162*>(x + at)};
+    const float m0{__bfloat162float(xv.x) > 0.0f ? v0 : 0.0f};
+    const float m1{__bfloat162float(xv.y) > 0.0f ? v1 : 0.0f};
+    store_pair(g + at, m0, m1);
+}
+
+// Data gradient of L4 (stride 1, 4x4): g3 = mask(x4) * convT(g4, W4). Warp w
+// takes input channels 8w..8w+7 of the 16 pixels.
+__device__ __forceinline__ void bwd_l4(unsigned gout, unsigned zero, unsigned w, const bf16* xin, bf16* gin,
+                                       int warp, int lane) {
+    float acc[4]{0.0f, 0.0f, 0.0f, 0.0f};
+    const int q{lane & 15};
+    const int qy{q >> 2};
+    const int qx{q & 3};
+#pragma unroll 2
+    for (int s{0}; s < 18; ++s) {
+        const int tap{s >> 1};
+        const int co0{(s & 1) * 16};
+        const int oy{qy - tap / 3 + 1};
+        const int ox{qx - tap % 3 + 1};
+        const bool ok{oy >= 0 && oy < 4 && ox >= 0 && ox < 4};
+        unsigned a[4];
+        ldsm_x4(a, ok ? gout + 2u * static_cast<unsigned>((oy * 4 + ox) * kActS + co0 + (lane >> 4) * 8) : zero);
+        unsigned b[2];
+        ldsm_x2_t(b, w + 2u * static_cast<unsigned>((co0 + (lane & 15)) * kWS + tap * kNetC + 8 * warp));
+        mma(acc, a, b[0], b[1]);
+    }
+    const int p{lane >> 2};
+    const int c{8 * warp + 2 * (lane & 3)};
+    store_masked(gin, xin, p * kActS + c, acc[0], acc[1]);
+    store_masked(gin, xin, (p + 8) * kActS + c, acc[2], acc[3]);
+}
+
+// Data gradient of a stride-2 layer over a kInW x kInW input. Input pixel
+// (iy, ix) collects output position ((iy + 1 - ky) / 2, (ix + 1 - kx) / 2)
+// for the taps whose offsets are even: ky = 1 for even iy, ky in {0, 2} for
+// odd iy (the same in x). Pixels are processed in four parity classes, each
+// a (kInW/2)^2 grid with its own tap list.
+template <int kInW>
+__device__ __forceinline__ void bwd_s2(unsigned gout, unsigned zero, unsigned w, const bf16* xin, bf16* gin,
+                                       int warp, int lane) {
+    constexpr int kOutW{kInW / 2};
+    constexpr int kCW{kInW / 2};
+    constexpr int kCM{kCW * kCW / 16};  // 16-pixel tiles per class
+    static_assert(kCM == 1 || kCM == 4, "layer geometry");
+#pragma unroll 1
+    for (int cls{0}; cls < 4; ++cls) {
+        const int py{cls >> 1};
+        const int px{cls & 1};
+        const int ntx{1 + px};
+        const int nsteps{2 * (1 + py) * (1 + px)};
+        // kCM == 4: warp w takes pixel tile w and all 32 channels; kCM == 1:
+        // the single tile and channels 8w..8w+7.
+        const int r{(kCM == 4 ? warp * 16 : 0) + (lane & 15)};
+        const int iy{2 * (r / kCW) + py};
+        const int ix{2 * (r % kCW) + px};
+        float acc[4][4];
+#pragma unroll
+        for (int n{0}; n < 4; ++n) {
+#pragma unroll
+            for (int j{0}; j < 4; ++j) acc[n][j] = 0.0f;
+        }
+#pragma unroll 1
+        for (int s{0}; s < nsteps; ++s) {
+            const int j{s >> 1};
+            const int co0{(s & 1) * 16};
+            const int ky{py ? 2 * (j / ntx) : 1};
+            const int kx{px ? 2 * (j % ntx) : 1};
+            const int oy{(iy + 1 - ky) >> 1};
+            const int ox{(ix + 1 - kx) >> 1};
+            const bool ok{oy < kOutW && ox < kOutW};
+            unsigned a[4];
+            ldsm_x4(a, ok ? gout + 2u * static_cast<unsigned>((oy * kOutW + ox) * kActS + co0 + (lane >> 4) * 8)
+                          : zero);
+            const int col{(ky * 3 + kx) * kNetC};
+            if (kCM == 4) {
+#pragma unroll
+                for (int h{0}; h < 2; ++h) {
+                    unsigned bb[4];
+                    ldsm_x4_t(bb, w + 2u * static_cast<unsigned>((co0 + (lane & 7) + ((lane >> 3) & 1) * 8) * kWS +
+                                                                 col + h * 16 + (lane >> 4) * 8));
+                    mma(acc[2 * h], a, bb[0], bb[1]);
+                    mma(acc[2 * h + 1], a, bb[2], bb[3]);
+                }
+            } else {
+                unsigned b[2];
+                ldsm_x2_t(b, w + 2u * static_cast<unsigned>((co0 + (lane & 15)) * kWS + col + 8 * warp));
+                mma(acc[0], a, b[0], b[1]);
+            }
+        }
+        const int r0{(kCM == 4 ? warp * 16 : 0) + (lane >> 2)};
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            const int rr{r0 + 8 * h};
+            const int pix{(2 * (rr / kCW) + py) * kInW + 2 * (rr % kCW) + px};
+            if (kCM == 4) {
+#pragma unroll
+                for (int n{0}; n < 4; ++n) {
+                    store_masked(gin, xin, pix * kActS + n * 8 + 2 * (lane & 3), acc[n][2 * h], acc[n][2 * h + 1]);
+                }
+            } else {
+                store_masked(gin, xin, pix * kActS + 8 * warp + 2 * (lane & 3), acc[0][2 * h], acc[0][2 * h + 1]);
+            }
+        }
+    }
+}
+
+// Copies the weights into shared memory (rows padded to kW1S / kWS).
+__device__ void load_net(NetSmem& s, const NetParamsDev& p, int tid, int nthreads) {
+    const uint4* g{reinterpret_cast<const uint4*>(p.w)};
+    for (int i{tid}; i < kNetC * (kNetK1 / 8); i += nthreads) {
+        const int r{i / (kNetK1 / 8)};
+        const int c{i - r * (kNetK1 / 8)};
+        *reinterpret_cast<uint4*>(&s.w1[r * kW1S + c * 8]) = __ldg(&g[i]);
+    }
+    for (int l{0}; l < 3; ++l) {
+        const uint4* gl{reinterpret_cast<const uint4*>(p.w + kNetW2 + l * kNetC * kNetK)};
+        for (int i{tid}; i < kNetC * (kNetK / 8); i += nthreads) {
+            const int r{i / (kNetK / 8)};
+            const int c{i - r * (kNetK / 8)};
+            *reinterpret_cast<uint4*>(&s.w[l][r * kWS + c * 8]) = __ldg(&gl[i]);
+        }
+    }
+    for (int i{tid}; i < 4 * kNetC; i += nthreads) s.bias[i / kNetC][i % kNetC] = p.bias[i];
+    if (tid < 8) s.zero[tid] = __float2bfloat16_rn(0.0f);
+}
+
+// One input pixel's eight stored channels: normalised X, Y, B and log2
+// distance rounded to BF16, then four zeros.
+__device__ __forceinline__ uint4 input_pixel(const NetParamsDev& p, float x, float y, float b, float l2d) {
+    const float v0{(x - p.shift[0]) * p.scale[0]};
+    const float v1{(y - p.shift[1]) * p.scale[1]};
+    const float v2{(b - p.shift[2]) * p.scale[2]};
+    const float v3{(l2d - p.shift[3]) * p.scale[3]};
+    const __nv_bfloat162 lo{__floats2bfloat162_rn(v0, v1)};
+    const __nv_bfloat162 hi{__floats2bfloat162_rn(v2, v3)};
+    uint4 r;
+    r.x = *reinterpret_cast<const unsigned*>(&lo);
+    r.y = *reinterpret_cast<const unsigned*>(&hi);
+    r.z = 0u;
+    r.w = 0u;
+    return r;
+}
+
+// The four layers over the region in s.x1; ends with s.out filled.
+__device__ __forceinline__ void net_forward(NetSmem& s, int warp, int lane) {
+    const unsigned zero{saddr(s.zero)};
+    fwd_rows<32, 2, kNetIn, kNetIn, kNetK1, kW1S>(saddr(s.x1), zero, saddr(s.w1), s.bias[0], s.x2, warp, lane);
+    __syncthreads();
+    fwd_rows<16, 2, kNetC, kActS, kNetK, kWS>(saddr(s.x2), zero, saddr(s.w[0]), s.bias[1], s.x3, warp, lane);
+    __syncthreads();
+    fwd_cols<8, 2, true>(saddr(s.x3), zero, saddr(s.w[1]), s.bias[2], s.x4, nullptr, warp, lane);
+    __syncthreads();
+    fwd_cols<4, 1, false>(saddr(s.x4), zero, saddr(s.w[2]), s.bias[3], nullptr, s.out, warp, lane);
+    __syncthreads();
+}
+
+// Split logit of `lane` (0..16; -inf elsewhere): channel 1 + lane averaged
+// over the 16 positions, summed in position order.
+__device__ __forceinline__ float split_logit(const float* out, int lane) {
+    if (lane >= kNetClasses) return -INFINITY;
+    float acc{0.0f};
+#pragma unroll
+    for (int p{0}; p < 16; ++p) acc = acc + out[p * kNetC + 1 + lane];
+    return acc * 0.0625f;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o{16}; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o{16}; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Lowest lane holding the warp maximum of v.
+__device__ __forceinline__ int warp_argmax(float v, float mx) {
+    return __ffs(__ballot_sync(0xffffffffu, v == mx)) - 1;
+}
+
+// Softmax statistics of the split logits held one per lane.
+struct SplitHead {
+    float prob;    // this lane's probability
+    int top;       // arg-max class
+    float margin;  // top probability minus the runner-up
+    float lse;     // log-sum-exp of the logits
+};
+
+__device__ __forceinline__ SplitHead split_head(float logit) {
+    const int lane{static_cast<int>(threadIdx.x & 31)};
+    const float mx{warp_max(logit)};
+    const float e{logit == -INFINITY ? 0.0f : expf(logit - mx)};
+    const float sum{warp_sum(e)};
+    SplitHead h;
+    h.prob = e / sum;
+    h.top = warp_argmax(logit, mx);
+    const float second{warp_max(lane == h.top ? 0.0f : e)};
+    h.margin = (__shfl_sync(0xffffffffu, e, h.top) - second) / sum;
+    h.lse = logf(sum) + mx;
+    return h;
+}
+
+// ---- Inference inside an encode ----
+
+constexpr int kRegionWin = 16 + 4;  // chroma window of one 32x32 region (2-sample margins)
+
+__global__ void __launch_bounds__(kNetThreads, 2)
+    acsnet_infer_kernel(FrontendInputs in, NetParamsDev p, float log2_distance, float margin,
+                        NetDecisionsDev out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    NetSmem& s{*reinterpret_cast<NetSmem*>(smem_raw)};
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int warp{tid >> 5};
+    const int lane{tid & 31};
+    load_net(s, p, tid, kNetThreads);
+    const int W{in.width};
+    const int H{in.height};
+    const int bw{W >> 3};
+    const int rw{(bw + 3) >> 2};
+    const int rh{((H >> 3) + 3) >> 2};
+    const int tw{(W + 63) >> 6};
+    const int ntiles{tw * ((H + 63) >> 6)};
+    std::uint8_t* win_luma{reinterpret_cast<std::uint8_t*>(s.x2)};
+    std::uint8_t* win_chroma{win_luma + 1024};
+    for (int t{static_cast<int>(blockIdx.x)}; t < ntiles; t += static_cast<int>(gridDim.x)) {
+#pragma unroll 1
+        for (int ri{0}; ri < 4; ++ri) {
+            const int rx{2 * (t % tw) + (ri & 1)};
+            const int ry{2 * (t / tw) + (ri >> 1)};
+            if (rx >= rw || ry >= rh) continue;  // block-uniform
+            const int px0{rx * 32};
+            const int py0{ry * 32};
+            if (px0 + 32 > W || py0 + 32 > H) {
+                if (tid == 0) out.cls[ry * rw + rx] = -1;
+                continue;
+            }
+            __syncthreads();  // the previous region is done with x2 and out
+            const int cx0{(px0 >> 1) - 2};
+            const int cy0{(py0 >> 1) - 2};
+            for (int i{tid}; i < 1024; i += kNetThreads) {
+                win_luma[i] = in.luma[static_cast<std::size_t>(py0 + (i >> 5)) * in.luma_pitch + px0 + (i & 31)];
+            }
+            for (int i{tid}; i < kRegionWin * kRegionWin; i += kNetThreads) {
+                const int jx{min(max(cx0 + i % kRegionWin, 0), (W >> 1) - 1)};
+                const int jy{min(max(cy0 + i / kRegionWin, 0), (H >> 1) - 1)};
+                const std::uint8_t* c{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
+                win_chroma[2 * i] = c[0];
+                win_chroma[2 * i + 1] = c[1];
+            }
+            __syncthreads();
+            for (int i{tid}; i < 1024; i += kNetThreads) {
+                float x, y, b;
+                xyb_pixel<kRegionWin>(win_luma[i], win_chroma, cx0, cy0, px0 + (i & 31), py0 + (i >> 5), W, H, x,
+                                      y, b);
+                *reinterpret_cast<uint4*>(&s.x1[i * kNetIn]) = input_pixel(p, x, y, b, log2_distance);
+            }
+            __syncthreads();
+            net_forward(s, warp, lane);
+            if (warp == 0) {
+                const SplitHead h{split_head(split_logit(s.out, lane))};
+                const int cls{h.margin >= margin ? h.top : -1};
+                if (lane == 0) out.cls[ry * rw + rx] = static_cast<std::int8_t>(cls);
+                if (cls >= 0 && out.qf != nullptr && lane < 16) {
+                    // fmaxf maps a NaN to 1.
+                    const float q{fminf(fmaxf(rintf(exp2f(s.out[lane * kNetC])), 1.0f),
+                                        static_cast<float>(kQuantMax))};
+                    const int qi{static_cast<int>(q)};
+                    out.qf[static_cast<std::size_t>(ry * 4 + (lane >> 2)) * bw + rx * 4 + (lane & 3)] =
+                        static_cast<std::int16_t>(qi);
+                }
+            }
+        }
+    }
+}
+
+// ---- Training ----
+
+// Forward (and with labels the loss and the data gradients) of one sample per
+// iteration; stores the activations and gradients the weight-gradient kernel
+// needs. out[n][33] and stats[n][4] are optional.
+__global__ void __launch_bounds__(kNetThreads)
+    acsnet_train_kernel(NetParamsDev p, NetBatchDev b, float inv_batch, float qf_weight, bf16* act,
+                        float* outv, float* stats) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& ts{*reinterpret_cast<TrainSmem*>(smem_raw)};
+    NetSmem& s{ts.n};
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int warp{tid >> 5};
+    const int lane{tid & 31};
+    load_net(s, p, tid, kNetThreads);
+    const unsigned zero{saddr(s.zero)};
+    for (std::uint32_t i{blockIdx.x}; i < b.n; i += gridDim.x) {
+        __syncthreads();
+        const float* tile{b.tiles + static_cast<std::size_t>(b.tile_index[i]) * 3072};
+        const float l2d{b.log2_distance[i]};
+        for (int px{tid}; px < 1024; px += kNetThreads) {
+            *reinterpret_cast<uint4*>(&s.x1[px * kNetIn]) =
+                input_pixel(p, tile[px], tile[1024 + px], tile[2048 + px], l2d);
+        }
+        __syncthreads();
+        net_forward(s, warp, lane);
+        if (outv != nullptr && warp == 0) {
+            float* o{outv + static_cast<std::size_t>(i) * kNetOut};
+            const float lg{split_logit(s.out, lane)};
+            if (lane < kNetClasses) o[lane] = lg;
+            if (lane < 16) o[kNetClasses + lane] = s.out[lane * kNetC];
+        }
+        if (b.label_class == nullptr) continue;  // block-uniform
+        if (warp == 0) {
+            // Loss and its gradient at the L4 outputs.
+            const int label{b.label_class[i]};
+            const float lg{split_logit(s.out, lane)};
+            const SplitHead h{split_head(lg)};
+            const float dlogit{(h.prob - (lane == label ? 1.0f : 0.0f)) * inv_batch};
+            const float ce{h.lse - __shfl_sync(0xffffffffu, lg, label)};
+            float d{0.0f};
+            if (lane < 16) d = s.out[lane * kNetC] - b.label_qf[static_cast<std::size_t>(i) * 16 + lane];
+            const float sq{warp_sum(d * d)};
+            const float dq{2.0f * qf_weight * d * inv_batch * 0.0625f};
+            const float dl_c{__shfl_sync(0xffffffffu, dlogit, (lane + 31) & 31) * 0.0625f};
+#pragma unroll 1
+            for (int pp{0}; pp < 16; ++pp) {
+                const float dqp{__shfl_sync(0xffffffffu, dq, pp)};
+                const float v{lane == 0 ? dqp : (lane <= kNetClasses ? dl_c : 0.0f)};
+                ts.g4[pp * kActS + lane] = __float2bfloat16_rn(v);
+            }
+            if (stats != nullptr && lane == 0) {
+                float* st{stats + static_cast<std::size_t>(i) * 4};
+                st[0] = ce;
+                st[1] = sq * 0.0625f;
+                st[2] = h.top == label ? 1.0f : 0.0f;
+                st[3] = h.margin;
+            }
+        }
+        __syncthreads();
+        bwd_l4(saddr(ts.g4), zero, saddr(s.w[2]), s.x4, ts.g3, warp, lane);
+        __syncthreads();
+        bwd_s2<8>(saddr(ts.g3), zero, saddr(s.w[1]), s.x3, ts.g2, warp, lane);
+        __syncthreads();
+        bwd_s2<16>(saddr(ts.g2), zero, saddr(s.w[0]), s.x2, ts.g1, warp, lane);
+        __syncthreads();
+        // Compact copies for the weight-gradient kernel (8 BF16 per uint4).
+        bf16* a{act + static_cast<std::size_t>(i) * kNetActPerSample};
+        auto put = [&](int dst, const bf16* src, int pixels, int stride, int ch) {
+            const int per{ch / 8};
+            for (int k{tid}; k < pixels * per; k += kNetThreads) {
+                const int px{k / per};
+                const int c{k - px * per};
+                *reinterpret_cast<uint4*>(a + dst + px * ch + c * 8) =
+                    *reinterpret_cast<const uint4*>(src + px * stride + c * 8);
+            }
+        };
+        put(kNetActX1, s.x1, 1024, kNetIn, kNetIn);
+        put(kNetActX2, s.x2, 256, kActS, kNetC);
+        put(kNetActX3, s.x3, 64, kActS, kNetC);
+        put(kNetActX4, s.x4, 16, kActS, kNetC);
+        put(kNetActG1, ts.g1, 256, kActS, kNetC);
+        put(kNetActG2, ts.g2, 64, kActS, kNetC);
+        put(kNetActG3, ts.g3, 16, kActS, kNetC);
+        put(kNetActG4, ts.g4, 16, kActS, kNetC);
+    }
+}
+
+// Geometry of layer L (1..4) for the weight gradient.
+template <int L>
+struct LayerGeo {
+    static constexpr int kInW = L == 1 ? 32 : (L == 2 ? 16 : (L == 3 ? 8 : 4));
+    static constexpr int kStride = L == 4 ? 1 : 2;
+    static constexpr int kCin = L == 1 ? kNetIn : kNetC;
+    static constexpr int kInS = L == 1 ? kNetIn : kActS;
+    static constexpr int kK = L == 1 ? kNetK1 : kNetK;
+    static constexpr int kP = (kInW / kStride) * (kInW / kStride);
+    static constexpr int kXOff = L == 1 ? kNetActX1 : (L == 2 ? kNetActX2 : (L == 3 ? kNetActX3 : kNetActX4));
+    static constexpr int kGOff = L == 1 ? kNetActG1 : (L == 2 ? kNetActG2 : (L == 3 ? kNetActG3 : kNetActG4));
+    static constexpr int kWOff = L == 1 ? kNetW1 : (L == 2 ? kNetW2 : (L == 3 ? kNetW3 : kNetW4));
+};
+
+// dW_L = sum over the split's samples and positions of g[p][co] x im2col(x)[p][k],
+// and the bias gradient; written to partial[blockIdx.x][...] in fixed order.
+template <int L>
+__global__ void __launch_bounds__(kGradThreads) acsnet_wgrad_kernel(const bf16* act, std::uint32_t n, float* partial) {
+    using G = LayerGeo<L>;
+    constexpr int kPairs{G::kK / 16};   // pairs of 8-column tiles
+    constexpr int kPW{(kPairs + 7) / 8};  // pairs per warp
+    __shared__ __align__(16) bf16 xs[G::kInW * G::kInW * G::kInS];
+    __shared__ __align__(16) bf16 gs[G::kP * kActS];
+    __shared__ __align__(16) bf16 zs[8];
+    const int tid{static_cast<int>(threadIdx.x)};
+    const int warp{tid >> 5};
+    const int lane{tid & 31};
+    if (tid < 8) zs[tid] = __float2bfloat16_rn(0.0f);
+    float acc[kPW][2][2][4];
+#pragma unroll
+    for (int i{0}; i < kPW; ++i) {
+#pragma unroll
+        for (int m{0}; m < 2; ++m) {
+#pragma unroll
+            for (int nn{0}; nn < 2; ++nn) {
+#pragma unroll
+                for (int j{0}; j < 4; ++j) acc[i][m][nn][j] = 0.0f;
+            }
+        }
+    }
+    float db{0.0f};
+    const unsigned xa{saddr(xs)};
+    const unsigned ga{saddr(gs)};
+    const unsigned za{saddr(zs)};
+    for (std::uint32_t i{blockIdx.x}; i < n; i += gridDim.x) {
+        __syncthreads();
+        const bf16* a{act + static_cast<std::size_t>(i) * kNetActPerSample};
+        constexpr int kXPer{G::kCin / 8};
+        for (int k{tid}; k < G::kInW * G::kInW * kXPer; k += kGradThreads) {
+            const int px{k / kXPer};
+            const int c{k - px * kXPer};
+            *reinterpret_cast<uint4*>(&xs[px * G::kInS + c * 8]) =
+                *reinterpret_cast<const uint4*>(a + G::kXOff + px * G::kCin + c * 8);
+        }
+        for (int k{tid}; k < G::kP * 4; k += kGradThreads) {
+            const int px{k >> 2};
+            const int c{k & 3};
+            *reinterpret_cast<uint4*>(&gs[px * kActS + c * 8]) =
+                *reinterpret_cast<const uint4*>(a + G::kGOff + px * kNetC + c * 8);
+        }
+        __syncthreads();
+        if (tid < kNetC) {
+            for (int pp{0}; pp < G::kP; ++pp) db = db + __bfloat162float(gs[pp * kActS + tid]);
+        }
+#pragma unroll 1
+        for (int kp{0}; kp < G::kP; kp += 16) {
+            unsigned am[2][4];
+#pragma unroll
+            for (int m{0}; m < 2; ++m) {
+                ldsm_x4_t(am[m], ga + 2u * static_cast<unsigned>((kp + (lane & 7) + ((lane >> 4) << 3)) * kActS +
+                                                                 m * 16 + ((lane >> 3) & 1) * 8));
+            }
+#pragma unroll
+            for (int pi{0}; pi < kPW; ++pi) {
+                const int pair{warp + 8 * pi};
+                if (pair < kPairs) {
+                    unsigned bb[4];
+                    ldsm_x4_t(bb, im2col_row<G::kInW, G::kStride, G::kCin, G::kInS>(
+                                      xa, za, kp + (lane & 7) + ((lane >> 3) & 1) * 8, pair * 16 + (lane >> 4) * 8));
+#pragma unroll
+                    for (int m{0}; m < 2; ++m) {
+                        mma(acc[pi][m][0], am[m], bb[0], bb[1]);
+                        mma(acc[pi][m][1], am[m], bb[2], bb[3]);
+                    }
+                }
+            }
+        }
+    }
+    float* out{partial + static_cast<std::size_t>(blockIdx.x) * kNetParams};
+#pragma unroll
+    for (int pi{0}; pi < kPW; ++pi) {
+        const int pair{warp + 8 * pi};
+        if (pair >= kPairs) continue;
+#pragma unroll
+        for (int m{0}; m < 2; ++m) {
+#pragma unroll
+            for (int nn{0}; nn < 2; ++nn) {
+                const int co{m * 16 + (lane >> 2)};
+                const int k{pair * 16 + nn * 8 + 2 * (lane & 3)};
+                out[G::kWOff + co * G::kK + k] = acc[pi][m][nn][0];
+                out[G::kWOff + co * G::kK + k + 1] = acc[pi][m][nn][1];
+                out[G::kWOff + (co + 8) * G::kK + k] = acc[pi][m][nn][2];
+                out[G::kWOff + (co + 8) * G::kK + k + 1] = acc[pi][m][nn][3];
+            }
+        }
+    }
+    if (tid < kNetC) out[kNetBias + (L - 1) * kNetC + tid] = db;
+}
+
+struct AdamArgs {
+    float* theta;
+    float* m;
+    float* v;
+    std::uint16_t* wbf;
+    float lr_t;     // learning rate with both bias corrections folded in
+    float eps_t;    // epsilon scaled by the second-moment correction
+    int update;
+};
+
+// Sums the per-split partial gradients in split order; optionally one Adam
+// update of the FP32 master weights and their BF16 copy.
+__global__ void acsnet_reduce_kernel(const float* partial, int nsplit, float* grad, AdamArgs a) {
+    const int i{static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x)};
+    if (i >= kNetParams) return;
+    float g{0.0f};
+    for (int sp{0}; sp < nsplit; ++sp) g = g + partial[static_cast<std::size_t>(sp) * kNetParams + i];
+    if (grad != nullptr) grad[i] = g;
+    if (!a.update) return;
+    const float m{0.9f * a.m[i] + 0.1f * g};
+    const float v{0.999f * a.v[i] + 0.001f * (g * g)};
+    a.m[i] = m;
+    a.v[i] = v;
+    const float t{a.theta[i] - a.lr_t * m / (sqrtf(v) + a.eps_t)};
+    a.theta[i] = t;
+    if (i < kNetWeights) a.wbf[i] = __bfloat16_as_ushort(__float2bfloat16_rn(t));
+}
+
+int sm_count() {
+    int dev{0};
+    int n{0};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                                   cudaSuccess) {
+        return 148;
+    }
+    return n;
+}
+
+}  // namespace
+
+bool acsnet_kernels_init() {
+    return cudaFuncSetAttribute(acsnet_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(NetSmem))) == cudaSuccess &&
+           cudaFuncSetAttribute(acsnet_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(TrainSmem))) == cudaSuccess;
+}
+
+bool acsnet_infer_launch(const FrontendInputs& in, const NetParamsDev& p, float log2_distance, float margin,
+                         const NetDecisionsDev& out, void* stream) {
+    const int ntiles{((in.width + 63) >> 6) * ((in.height + 63) >> 6)};
+    const int grid{ntiles < 2 * sm_count() ? ntiles : 2 * sm_count()};
+    acsnet_infer_kernel<<<grid, kNetThreads, sizeof(NetSmem), static_cast<cudaStream_t>(stream)>>>(
+        in, p, log2_distance, margin, out);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+// Host BF16 rounding (nearest, ties to even), as __float2bfloat16_rn.
+std::uint16_t host_bf16(float f) {
+    std::uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0u;
+    return static_cast<std::uint16_t>((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+
+}  // namespace jxb
+
+// ---- SHA-256 (FIPS 180-4), for the weights blob ----
+namespace {
+
+class Sha256 {
+public:
+    void update(const std::uint8_t* d, std::size_t n) {
+        for (std::size_t i{0}; i < n; ++i) {
+            buf_[fill_++] = d[i];
+            if (fill_ == 64) {
+                block();
+                fill_ = 0;
+            }
+        }
+        len_ += n;
+    }
+
+    void finish(std::uint8_t out[32]) {
+        const std::uint64_t bits{len_ * 8};
+        const std::uint8_t one{0x80};
+        update(&one, 1);
+        const std::uint8_t z{0};
+        while (fill_ != 56) update(&z, 1);
+        for (int i{7}; i >= 0; --i) {
+            const std::uint8_t b{static_cast<std::uint8_t>(bits >> (8 * i))};
+            update(&b, 1);
+        }
+        for (int i{0}; i < 8; ++i) {
+            for (int j{0}; j < 4; ++j) out[4 * i + j] = static_cast<std::uint8_t>(h_[i] >> (24 - 8 * j));
+        }
+    }
+
+private:
+    static std::uint32_t rotr(std::uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+
+    void block() {
+        static constexpr std::uint32_t k[64]{
+            0x428a2f98u, 0x71374491u, 0xb5c0fbcfu, 0xe9b5dba5u, 0x3956c25bu, 0x59f111f1u, 0x923f82a4u, 0xab1c5ed5u,
+            0xd807aa98u, 0x12835b01u, 0x243185beu, 0x550c7dc3u, 0x72be5d74u, 0x80deb1feu, 0x9bdc06a7u, 0xc19bf174u,
+            0xe49b69c1u, 0xefbe4786u, 0x0fc19dc6u, 0x240ca1ccu, 0x2de92c6fu, 0x4a7484aau, 0x5cb0a9dcu, 0x76f988dau,
+            0x983e5152u, 0xa831c66du, 0xb00327c8u, 0xbf597fc7u, 0xc6e00bf3u, 0xd5a79147u, 0x06ca6351u, 0x14292967u,
+            0x27b70a85u, 0x2e1b2138u, 0x4d2c6dfcu, 0x53380d13u, 0x650a7354u, 0x766a0abbu, 0x81c2c92eu, 0x92722c85u,
+            0xa2bfe8a1u, 0xa81a664bu, 0xc24b8b70u, 0xc76c51a3u, 0xd192e819u, 0xd6990624u, 0xf40e3585u, 0x106aa070u,
+            0x19a4c116u, 0x1e376c08u, 0x2748774cu, 0x34b0bcb5u, 0x391c0cb3u, 0x4ed8aa4au, 0x5b9cca4fu, 0x682e6ff3u,
+            0x748f82eeu, 0x78a5636fu, 0x84c87814u, 0x8cc70208u, 0x90befffau, 0xa4506cebu, 0xbef9a3f7u, 0xc67178f2u};
+        std::uint32_t w[64];
+        for (int i{0}; i < 16; ++i) {
+            w[i] = (static_cast<std::uint32_t>(buf_[4 * i]) << 24) | (static_cast<std::uint32_t>(buf_[4 * i + 1]) << 16) |
+                   (static_cast<std::uint32_t>(buf_[4 * i + 2]) << 8) | buf_[4 * i + 3];
+        }
+        for (int i{16}; i < 64; ++i) {
+            const std::uint32_t s0{rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3)};
+            const std::uint32_t s1{rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10)};
+            w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+        }
+        std::uint32_t a{h_[0]}, b{h_[1]}, c{h_[2]}, d{h_[3]}, e{h_[4]}, f{h_[5]}, g{h_[6]}, h{h_[7]};
+        for (int i{0}; i < 64; ++i) {
+            const std::uint32_t s1{rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)};
+            const std::uint32_t ch{(e & f) ^ (~e & g)};
+            const std::uint32_t t1{h + s1 + ch + k[i] + w[i]};
+            const std::uint32_t s0{rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)};
+            const std::uint32_t mj{(a & b) ^ (a & c) ^ (b & c)};
+            const std::uint32_t t2{s0 + mj};
+            h = g;
+            g = f;
+            f = e;
+            e = d + t1;
+            d = c;
+            c = b;
+            b = a;
+            a = t1 + t2;
+        }
+        h_[0] += a;
+        h_[1] += b;
+        h_[2] += c;
+        h_[3] += d;
+        h_[4] += e;
+        h_[5] += f;
+        h_[6] += g;
+        h_[7] += h;
+    }
+
+    std::uint32_t h_[8]{0x6a09e667u, 0xbb67ae85u, 0x3c6ef372u, 0xa54ff53au,
+                        0x510e527fu, 0x9b05688cu, 0x1f83d9abu, 0x5be0cd19u};
+    std::uint8_t buf_[64]{};
+    std::size_t fill_{0};
+    std::uint64_t len_{0};
+};
+
+constexpr std::size_t kBlobHeader = 4 + 6 * 4 + 8 * 4;  // magic, six uint32, scale[4], shift[4]
+constexpr std::size_t kBlobBytes = kBlobHeader + 4 * static_cast<std::size_t>(jxb::kNetParams) + 32;
+
+std::uint32_t rd32(const std::uint8_t* p) {
+    return static_cast<std::uint32_t>(p[0]) | (static_cast<std::uint32_t>(p[1]) << 8) |
+           (static_cast<std::uint32_t>(p[2]) << 16) | (static_cast<std::uint32_t>(p[3]) << 24);
+}
+
+float rdf(const std::uint8_t* p) {
+    const std::uint32_t u{rd32(p)};
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+bool blob_ok(const void* blob, std::size_t size) {
+    if (blob == nullptr || size != kBlobBytes) return false;
+    const auto* b{static_cast<const std::uint8_t*>(blob)};
+    if (std::memcmp(b, "JXBN", 4) != 0 || rd32(b + 4) != 1u || rd32(b + 8) != static_cast<std::uint32_t>(jxb::kNetParams) ||
+        rd32(b + 12) != 32u || rd32(b + 16) != 17u || rd32(b + 20) != 80u || rd32(b + 24) != 288u) {
+        return false;
+    }
+    Sha256 h;
+    h.update(b, size - 32);
+    std::uint8_t d[32];
+    h.finish(d);
+    if (std::memcmp(d, b + size - 32, 32) != 0) return false;
+    for (std::size_t i{28}; i < size - 32; i += 4) {
+        if (!std::isfinite(rdf(b + i))) return false;
+    }
+    return true;
+}
+
+class DeviceScope {
+public:
+    explicit DeviceScope(int device) {
+        ok_ = cudaGetDevice(&prev_) == cudaSuccess && cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceScope() { cudaSetDevice(prev_); }
+    bool ok() const { return ok_; }
+
+private:
+    int prev_{0};
+    bool ok_{false};
+};
+
+std::mutex g_init_mutex;
+bool g_init[64]{};
+
+bool init_device(int device) {
+    if (device < 0 || device >= 64) return false;
+    std::lock_guard<std::mutex> lock(g_init_mutex);
+    if (!g_init[device]) {
+        if (!jxb::acsnet_kernels_init()) return false;
+        g_init[device] = true;
+    }
+    return true;
+}
+
+bool valid_device(int device) {
+    int n{0};
+    return cudaGetDeviceCount(&n) == cudaSuccess && device >= 0 && device < n;
+}
+
+}  // namespace
+
+struct cujpegxl_b200_acsnet {
+    int device{0};
+    void* mem{nullptr};
+    jxb::NetParamsDev p{};
+};
+
+struct cujpegxl_b200_acsnet_trainer {
+    int device{0};
+    std::uint32_t max_batch{0};
+    int nsplit{0};
+    void* mem{nullptr};
+    float* theta{nullptr};
+    float* m{nullptr};
+    float* v{nullptr};
+    std::uint16_t* wbf{nullptr};
+    float* partial{nullptr};
+    __nv_bfloat16* act{nullptr};
+    jxb::NetParamsDev p{};
+    std::uint32_t steps{0};
+};
+
+namespace jxb {
+
+const NetParamsDev* acsnet_params(const cujpegxl_b200_acsnet* net) { return net == nullptr ? nullptr : &net->p; }
+int acsnet_device(const cujpegxl_b200_acsnet* net) { return net->device; }
+
+}  // namespace jxb
+
+namespace {
+
+bool batch_dev(const cujpegxl_b200_acsnet_batch* b, std::uint32_t max_batch, bool labels, jxb::NetBatchDev* out) {
+    if (b == nullptr || b->n == 0 || b->n > max_batch || b->tiles == nullptr || b->tile_index == nullptr ||
+        b->log2_distance == nullptr) {
+        return false;
+    }
+    if (labels && (b->label_class == nullptr || b->label_qf == nullptr)) return false;
+    *out = jxb::NetBatchDev{b->tiles, b->tile_index, b->log2_distance, labels ? b->label_class : nullptr,
+                            labels ? b->label_qf : nullptr, b->n};
+    return true;
+}
+
+int train_grid(std::uint32_t n) {
+    const int g{2 * jxb::sm_count()};
+    return static_cast<int>(n) < g ? static_cast<int>(n) : g;
+}
+
+// Forward + backward-data, the four weight-gradient kernels and the reduction
+// (with an Adam update when `lr` > 0).
+bool run_gradient(cujpegxl_b200_acsnet_trainer* t, const jxb::NetBatchDev& b, float qf_weight, float* grad,
+                  float* stats, float lr, cudaStream_t st) {
+    const float inv_batch{1.0f / static_cast<float>(b.n)};
+    jxb::acsnet_train_kernel<<<train_grid(b.n), jxb::kNetThreads, sizeof(jxb::TrainSmem), st>>>(
+        t->p, b, inv_batch, qf_weight, t->act, nullptr, stats);
+    const int ns{static_cast<int>(b.n) < t->nsplit ? static_cast<int>(b.n) : t->nsplit};
+    jxb::acsnet_wgrad_kernel<1><<<ns, jxb::kGradThreads, 0, st>>>(t->act, b.n, t->partial);
+    jxb::acsnet_wgrad_kernel<2><<<ns, jxb::kGradThreads, 0, st>>>(t->act, b.n, t->partial);
+    jxb::acsnet_wgrad_kernel<3><<<ns, jxb::kGradThreads, 0, st>>>(t->act, b.n, t->partial);
+    jxb::acsnet_wgrad_kernel<4><<<ns, jxb::kGradThreads, 0, st>>>(t->act, b.n, t->partial);
+    jxb::AdamArgs a{t->theta, t->m, t->v, t->wbf, 0.0f, 0.0f, 0};
+    if (lr > 0.0f) {
+        ++t->steps;
+        const double c1{1.0 - std::pow(0.9, static_cast<double>(t->steps))};
+        const double c2{1.0 - std::pow(0.999, static_cast<double>(t->steps))};
+        // theta -= lr * (m / c1) / (sqrt(v / c2) + 1e-8), rewritten with
+        // lr_t = lr * sqrt(c2) / c1 and eps_t = 1e-8 * sqrt(c2).
+        a.lr_t = static_cast<float>(lr * std::sqrt(c2) / c1);
+        a.eps_t = static_cast<float>(1e-8 * std::sqrt(c2));
+        a.update = 1;
+    }
+    jxb::acsnet_reduce_kernel<<<(jxb::kNetParams + 255) / 256, 256, 0, st>>>(t->partial, ns, grad, a);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t cujpegxl_b200_acsnet_param_count(void) { return static_cast<uint32_t>(jxb::kNetParams); }
+
+cujpegxl_status cujpegxl_b200_acsnet_check_blob(const void* blob, size_t size) {
+    return blob_ok(blob, size) ? CUJPEGXL_OK : CUJPEGXL_INVALID_ARGUMENT;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_create(const void* blob, size_t size, int32_t device_ordinal,
+                                            cujpegxl_b200_acsnet** out_net) {
+    if (out_net == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    *out_net = nullptr;
+    if (!blob_ok(blob, size)) return CUJPEGXL_INVALID_ARGUMENT;
+    if (!valid_device(device_ordinal)) return CUJPEGXL_NO_DEVICE;
+    DeviceScope scope{device_ordinal};
+    if (!scope.ok() || !init_device(device_ordinal)) return CUJPEGXL_INTERNAL_ERROR;
+    const auto* b{static_cast<const std::uint8_t*>(blob)};
+    auto* net{new (std::nothrow) cujpegxl_b200_acsnet};
+    if (net == nullptr) return CUJPEGXL_INTERNAL_ERROR;
+    net->device = device_ordinal;
+    std::vector<std::uint16_t> w(jxb::kNetWeights);
+    std::vector<float> bias(4 * jxb::kNetC);
+    const std::uint8_t* params{b + kBlobHeader};
+    for (int i{0}; i < jxb::kNetWeights; ++i) w[i] = jxb::host_bf16(rdf(params + 4 * i));
+    for (int i{0}; i < 4 * jxb::kNetC; ++i) bias[i] = rdf(params + 4 * (jxb::kNetBias + i));
+    for (int i{0}; i < 4; ++i) {
+        net->p.scale[i] = rdf(b + 28 + 4 * i);
+        net->p.shift[i] = rdf(b + 44 + 4 * i);
+    }
+    const std::size_t wbytes{(w.size() * 2 + 255) & ~static_cast<std::size_t>(255)};
+    if (cudaMalloc(&net->mem, wbytes + bias.size() * 4) != cudaSuccess) {
+        delete net;
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    auto* m{static_cast<std::uint8_t*>(net->mem)};
+    if (cudaMemcpy(m, w.data(), w.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m + wbytes, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(net->mem);
+        delete net;
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    net->p.w = reinterpret_cast<const std::uint16_t*>(m);
+    net->p.bias = reinterpret_cast<const float*>(m + wbytes);
+    *out_net = net;
+    return CUJPEGXL_OK;
+}
+
+void cujpegxl_b200_acsnet_destroy(cujpegxl_b200_acsnet* net) {
+    if (net == nullptr) return;
+    DeviceScope scope{net->device};
+    cudaFree(net->mem);
+    delete net;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_trainer_create(const float* params, const float* norm, uint32_t max_batch,
+                                                    int32_t device_ordinal,
+                                                    cujpegxl_b200_acsnet_trainer** out_trainer) {
+    if (out_trainer == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    *out_trainer = nullptr;
+    if (params == nullptr || norm == nullptr || max_batch == 0 || max_batch > (1u << 20)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    for (int i{0}; i < jxb::kNetParams; ++i) {
+        if (!std::isfinite(params[i])) return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    if (!valid_device(device_ordinal)) return CUJPEGXL_NO_DEVICE;
+    DeviceScope scope{device_ordinal};
+    if (!scope.ok() || !init_device(device_ordinal)) return CUJPEGXL_INTERNAL_ERROR;
+    auto* t{new (std::nothrow) cujpegxl_b200_acsnet_trainer};
+    if (t == nullptr) return CUJPEGXL_INTERNAL_ERROR;
+    t->device = device_ordinal;
+    t->max_batch = max_batch;
+    t->nsplit = 2 * jxb::sm_count();
+    auto a256 = [](std::size_t v) { return (v + 255) & ~static_cast<std::size_t>(255); };
+    const std::size_t np{static_cast<std::size_t>(jxb::kNetParams)};
+    const std::size_t o_theta{0};
+    const std::size_t o_m{o_theta + a256(np * 4)};
+    const std::size_t o_v{o_m + a256(np * 4)};
+    const std::size_t o_w{o_v + a256(np * 4)};
+    const std::size_t o_part{o_w + a256(np * 2)};
+    const std::size_t o_act{o_part + a256(np * 4 * static_cast<std::size_t>(t->nsplit))};
+    const std::size_t total{o_act + a256(static_cast<std::size_t>(max_batch) * jxb::kNetActPerSample * 2)};
+    if (cudaMalloc(&t->mem, total) != cudaSuccess) {
+        delete t;
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    auto* m{static_cast<std::uint8_t*>(t->mem)};
+    t->theta = reinterpret_cast<float*>(m + o_theta);
+    t->m = reinterpret_cast<float*>(m + o_m);
+    t->v = reinterpret_cast<float*>(m + o_v);
+    t->wbf = reinterpret_cast<std::uint16_t*>(m + o_w);
+    t->partial = reinterpret_cast<float*>(m + o_part);
+    t->act = reinterpret_cast<__nv_bfloat16*>(m + o_act);
+    std::vector<std::uint16_t> w(jxb::kNetWeights);
+    for (int i{0}; i < jxb::kNetWeights; ++i) w[i] = jxb::host_bf16(params[i]);
+    if (cudaMemcpy(t->theta, params, np * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(t->m, 0, np * 4) != cudaSuccess || cudaMemset(t->v, 0, np * 4) != cudaSuccess ||
+        cudaMemcpy(t->wbf, w.data(), w.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(t->mem);
+        delete t;
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    t->p.w = t->wbf;
+    t->p.bias = t->theta + jxb::kNetBias;
+    for (int i{0}; i < 4; ++i) {
+        t->p.scale[i] = norm[i];
+        t->p.shift[i] = norm[4 + i];
+    }
+    *out_trainer = t;
+    return CUJPEGXL_OK;
+}
+
+void cujpegxl_b200_acsnet_trainer_destroy(cujpegxl_b200_acsnet_trainer* trainer) {
+    if (trainer == nullptr) return;
+    DeviceScope scope{trainer->device};
+    cudaFree(trainer->mem);
+    delete trainer;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_trainer_forward(cujpegxl_b200_acsnet_trainer* trainer,
+                                                     const cujpegxl_b200_acsnet_batch* batch, float* out,
+                                                     uintptr_t stream) {
+    jxb::NetBatchDev b{};
+    if (trainer == nullptr || out == nullptr || !batch_dev(batch, trainer->max_batch, false, &b)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{trainer->device};
+    if (!scope.ok()) return CUJPEGXL_INTERNAL_ERROR;
+    jxb::acsnet_train_kernel<<<train_grid(b.n), jxb::kNetThreads, sizeof(jxb::TrainSmem),
+                               reinterpret_cast<cudaStream_t>(stream)>>>(trainer->p, b, 0.0f, 0.0f, trainer->act, out,
+                                                                         nullptr);
+    return cudaGetLastError() == cudaSuccess ? CUJPEGXL_OK : CUJPEGXL_INTERNAL_ERROR;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_trainer_gradient(cujpegxl_b200_acsnet_trainer* trainer,
+                                                      const cujpegxl_b200_acsnet_batch* batch, float qf_weight,
+                                                      float* grad, float* stats, uintptr_t stream) {
+    jxb::NetBatchDev b{};
+    if (trainer == nullptr || grad == nullptr || !(qf_weight >= 0.0f) ||
+        !batch_dev(batch, trainer->max_batch, true, &b)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{trainer->device};
+    if (!scope.ok()) return CUJPEGXL_INTERNAL_ERROR;
+    return run_gradient(trainer, b, qf_weight, grad, stats, 0.0f, reinterpret_cast<cudaStream_t>(stream))
+               ? CUJPEGXL_OK
+               : CUJPEGXL_INTERNAL_ERROR;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_trainer_step(cujpegxl_b200_acsnet_trainer* trainer,
+                                                  const cujpegxl_b200_acsnet_batch* batch, float qf_weight,
+                                                  float learning_rate, float* stats, uintptr_t stream) {
+    jxb::NetBatchDev b{};
+    if (trainer == nullptr || !(qf_weight >= 0.0f) || !(learning_rate > 0.0f) ||
+        !batch_dev(batch, trainer->max_batch, true, &b)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{trainer->device};
+    if (!scope.ok()) return CUJPEGXL_INTERNAL_ERROR;
+    return run_gradient(trainer, b, qf_weight, nullptr, stats, learning_rate, reinterpret_cast<cudaStream_t>(stream))
+               ? CUJPEGXL_OK
+               : CUJPEGXL_INTERNAL_ERROR;
+}
+
+cujpegxl_status cujpegxl_b200_acsnet_trainer_params(cujpegxl_b200_acsnet_trainer* trainer, float* params) {
+    if (trainer == nullptr || params == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    DeviceScope scope{trainer->device};
+    if (!scope.ok() || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(params, trainer->theta, static_cast<std::size_t>(jxb::kNetParams) * 4, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    return CUJPEGXL_OK;
+}
+
+}  // extern "C"

@@ -15,6 +15,7 @@
 #include "cujpegxl/cujpegxl.h"
 #include "cujpegxl_b200/cujpegxl_b200.h"
 #include "encoder_internal.h"
+#include "acsnet.cuh"
 #include "entropy.cuh"
 #include "frontend.cuh"
 #include "jxl_constants.cuh"
@@ -46,6 +47,13 @@ struct cujpegxl_encoder {
     unsigned long long* result_pinned{nullptr};
     std::size_t arena_bytes{0};
     bool pending{false};
+    // Learned decisions: the attached network (not owned), its margin and
+    // flags, and the per-frame decision buffers in the arena.
+    const cujpegxl_b200_acsnet* net{nullptr};
+    float net_margin{0.2f};
+    std::uint32_t net_flags{0};
+    std::int8_t* net_class{nullptr};
+    std::int16_t* net_qf{nullptr};
 };
 
 namespace {
@@ -77,7 +85,9 @@ bool device_tables(int device, jxb::FrontendTables* out) {
     std::lock_guard<std::mutex> lock(g_mutex);
     DeviceTables& t{g_tables[device]};
     if (!t.ready) {
-        if (!jxb::frontend_tables_init(&t.ft) || !jxb::entropy_kernels_init()) return false;
+        if (!jxb::frontend_tables_init(&t.ft) || !jxb::entropy_kernels_init() || !jxb::acsnet_kernels_init()) {
+            return false;
+        }
         t.ready = true;
     }
     *out = t.ft;
@@ -182,6 +192,8 @@ bool allocate(cujpegxl_encoder* e) {
     const std::size_t o_res{a.take(4 * 8)};
     const std::size_t o_out{a.take(out_cap)};
     const std::size_t o_nv12{a.take(static_cast<std::size_t>(W) * H * 3 / 2)};
+    const std::size_t o_ncls{a.take(((bw + 3) / 4) * ((bh + 3) / 4))};
+    const std::size_t o_nqf{a.take(nb * 2)};
     std::size_t o_dbg{0};
     if (e->debug) {
         o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2);
@@ -267,6 +279,8 @@ bool allocate(cujpegxl_encoder* e) {
     ed.out = b + o_out;
     ed.out_capacity = out_cap;
     e->nv12_dev = b + o_nv12;
+    e->net_class = reinterpret_cast<std::int8_t*>(b + o_ncls);
+    e->net_qf = reinterpret_cast<std::int16_t*>(b + o_nqf);
 
     bool ok{cudaMemcpy(b + o_sec, plan.sections.data(), plan.sections.size() * sizeof(jxb::Section),
                        cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -318,9 +332,18 @@ bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp
                    std::size_t cp, std::uint32_t stages = 3u, cudaStream_t stream = nullptr) {
     jxb::FrontendTables ft{};
     if (!device_tables(e->device, &ft)) return false;
-    const jxb::FrontendInputs in{luma, chroma, lp, cp, static_cast<int>(e->config.width),
-                                 static_cast<int>(e->config.height)};
+    jxb::FrontendInputs in{luma, chroma, lp, cp, static_cast<int>(e->config.width),
+                           static_cast<int>(e->config.height), nullptr, nullptr};
     cudaStream_t st{stream != nullptr ? stream : e->stream};
+    if ((stages & 1u) && e->net != nullptr) {
+        const jxb::NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr};
+        if (!jxb::acsnet_infer_launch(in, *jxb::acsnet_params(e->net), std::log2(e->config.distance),
+                                      e->net_margin, dec, st)) {
+            return false;
+        }
+        in.net_class = dec.cls;
+        in.net_qf = dec.qf;
+    }
     if ((stages & 1u) && !jxb::frontend_launch(in, e->fs, ft, e->fo, st)) return false;
     return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, st);
 }
@@ -499,6 +522,7 @@ cujpegxl_status cujpegxl_encoder_configure(cujpegxl_encoder* encoder, const cujp
         encoder->stream = nullptr;
         release(encoder);
         encoder->device = config->device_ordinal;
+        encoder->net = nullptr;  // a network lives on one device
         DeviceScope scope{encoder->device};
         if (cudaStreamCreateWithFlags(&encoder->stream, cudaStreamNonBlocking) != cudaSuccess) {
             return CUJPEGXL_INTERNAL_ERROR;
@@ -710,5 +734,44 @@ cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* 
 }
 
 uint32_t cujpegxl_b200_kernels_per_encode(void) { return 12u; }
+
+cujpegxl_status cujpegxl_b200_encoder_set_acsnet(cujpegxl_encoder* encoder, const cujpegxl_b200_acsnet* net,
+                                                 float margin, uint32_t flags) {
+    if (encoder == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    if (net == nullptr) {
+        encoder->net = nullptr;
+        encoder->net_flags = 0;
+        return CUJPEGXL_OK;
+    }
+    if (!(margin >= 0.0f && margin <= 1.0f) || (flags & CUJPEGXL_B200_ACSNET_SPLIT) == 0 ||
+        (flags & ~(CUJPEGXL_B200_ACSNET_SPLIT | CUJPEGXL_B200_ACSNET_QF)) != 0 ||
+        jxb::acsnet_device(net) != encoder->device) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    encoder->net = net;
+    encoder->net_margin = margin;
+    encoder->net_flags = flags;
+    return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_acsnet_stats(cujpegxl_encoder* encoder, uint32_t* decided,
+                                                   uint32_t* regions) {
+    if (encoder == nullptr || decided == nullptr || regions == nullptr || encoder->arena == nullptr) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    const std::size_t rw{(encoder->geo_w / 8 + 3) / 4};
+    const std::size_t rh{(encoder->geo_h / 8 + 3) / 4};
+    std::vector<std::int8_t> cls(rw * rh);
+    if (!scope.ok() || cudaStreamSynchronize(encoder->stream) != cudaSuccess ||
+        cudaMemcpy(cls.data(), encoder->net_class, cls.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    std::uint32_t d{0};
+    for (const std::int8_t c : cls) d += c >= 0 ? 1u : 0u;
+    *decided = encoder->net != nullptr ? d : 0u;
+    *regions = static_cast<std::uint32_t>((encoder->geo_w / 32) * (encoder->geo_h / 32));
+    return CUJPEGXL_OK;
+}
 
 }  // extern "C"

@@ -8,8 +8,15 @@
 #include <cstdint>
 
 #include "cujpegxl/cujpegxl.h"
+#include "cujpegxl_b200/cujpegxl_b200.h"
 
 namespace jxb {
+
+struct NetParamsDev;
+
+// Device weights and device ordinal of a transform-decision network.
+const NetParamsDev* acsnet_params(const cujpegxl_b200_acsnet* net);
+int acsnet_device(const cujpegxl_b200_acsnet* net);
 
 // Allocates or refreshes the per-geometry and per-distance state; not
 // capturable (it may allocate and upload tables).

@@ -21,6 +21,7 @@
 #include "frontend.cuh"
 #include "jxl_constants.cuh"
 #include "jxl_math.cuh"
+#include "xyb.cuh"
 
 namespace jxb {
 namespace {
@@ -81,82 +82,21 @@ struct Small {
     signed char acs[64];
     int n32, n16, n8;
     int mx, mb;
+    signed char net[4];   // learned split class of each 32x32 region, -1 = RD heuristic
 };
+
+// Region (0..3, raster) of the tile that holds tile block lb.
+__device__ __forceinline__ int region_of_block(int lb) { return ((lb >> 5) << 1) | ((lb & 7) >> 2); }
 
 constexpr std::size_t kSmemBytes =
     sizeof(float) * (kRegionAFloats + 3 * kSplane) + sizeof(Small);
 // Two CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA.
 static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two frontend CTAs no longer fit on one SM");
 
-__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
-
-// sRGB transfer function to linear (src/xyb_impl.cuh:37-40).
-__device__ __forceinline__ float srgb_to_linear(float e) {
-    return e <= 0.04045f ? e * (1.0f / 12.92f) : jx_pow24((e + 0.055f) * (1.0f / 1.055f));
-}
-
-// s / 4080.0f correctly rounded for an integer s in [0, 4080], without a
-// division: q0 = s * RN(1/4080), then one Newton correction with the exact
-// residual s - q0 * 4080. Checked against the rounded quotient for every s in
-// the range (the tap sums of the chroma upsample never leave it).
-__device__ __forceinline__ float div4080(int s) {
-    constexpr float kInv{1.0f / 4080.0f};
-    const float sf{static_cast<float>(s)};
-    const float q0{sf * kInv};
-    return jx_fma(jx_fma(-q0, 4080.0f, sf), kInv, q0);
-}
-
 // Chroma window of a tile in shared memory: kChromaWin x kChromaWin (cb, cr)
 // pairs starting kChromaMargin chroma samples before the tile's first.
 constexpr int kChromaMargin = 2;
 constexpr int kChromaWin = kTile / 2 + 2 * kChromaMargin;  // 36
-
-// NV12 pixel (gx, gy) -> XYB (src/xyb_impl.cuh:49-70), from its luma byte and
-// the tile's chroma window whose first pair is chroma sample (cx0, cy0).
-// Chroma is the centred bilinear 2x upsample of the texture path
-// (src/frontend_fused.cu:222), taken exactly: the four taps carry weights
-// {1,3}x{1,3}/16, summed in integers.
-__device__ __forceinline__ void xyb_pixel(int luma, const std::uint8_t* win, int cx0, int cy0, int gx, int gy,
-                                          int width, int height, float& ox, float& oy, float& ob) {
-    const float yv{static_cast<float>(luma) * kInv255};
-    const int cw{width >> 1};
-    const int ch{height >> 1};
-    const int jx{gx >> 1};
-    const int jy{gy >> 1};
-    int xa, xb, wxa, wxb, ya, yb, wya, wyb;
-    if (gx & 1) {
-        xa = jx; xb = min(jx + 1, cw - 1); wxa = 3; wxb = 1;
-    } else {
-        xa = max(jx - 1, 0); xb = jx; wxa = 1; wxb = 3;
-    }
-    if (gy & 1) {
-        ya = jy; yb = min(jy + 1, ch - 1); wya = 3; wyb = 1;
-    } else {
-        ya = max(jy - 1, 0); yb = jy; wya = 1; wyb = 3;
-    }
-    const int aa{2 * ((ya - cy0) * kChromaWin + xa - cx0)};
-    const int ab{2 * ((ya - cy0) * kChromaWin + xb - cx0)};
-    const int ba{2 * ((yb - cy0) * kChromaWin + xa - cx0)};
-    const int bb{2 * ((yb - cy0) * kChromaWin + xb - cx0)};
-    const int scb{wya * (wxa * win[aa] + wxb * win[ab]) + wyb * (wxa * win[ba] + wxb * win[bb])};
-    const int scr{wya * (wxa * win[aa + 1] + wxb * win[ab + 1]) + wyb * (wxa * win[ba + 1] + wxb * win[bb + 1])};
-    const float cb{div4080(scb) - kChromaCenter};
-    const float cr{div4080(scr) - kChromaCenter};
-
-    const float r{clamp01(srgb_to_linear(clamp01(jx_fma(kCrToR, cr, yv))))};
-    const float g{clamp01(srgb_to_linear(clamp01(jx_fma(-kCrToG, cr, jx_fma(-kCbToG, cb, yv)))))};
-    const float b{clamp01(srgb_to_linear(clamp01(jx_fma(kCbToB, cb, yv))))};
-
-    float m0{jx_fma(kM02, b, jx_fma(kM01, g, kM00 * r)) + kOpsinBias};
-    float m1{jx_fma(kM12, b, jx_fma(kM11, g, kM10 * r)) + kOpsinBias};
-    float m2{jx_fma(kM22, b, jx_fma(kM21, g, kM20 * r)) + kOpsinBias};
-    m0 = jx_cbrt(fmaxf(m0, 0.0f)) + kNegCbrtBias;
-    m1 = jx_cbrt(fmaxf(m1, 0.0f)) + kNegCbrtBias;
-    m2 = jx_cbrt(fmaxf(m2, 0.0f)) + kNegCbrtBias;
-    ox = 0.5f * (m0 - m1);
-    oy = 0.5f * (m0 + m1);
-    ob = m2;
-}
 
 // lrintf((v * qgsf) / w) for a positive weight w (src/frontend_quantize.cu:
 // 165-178). When |v * qgsf| <= w / 2 the rounded quotient is at most 1/2 in
@@ -465,6 +405,13 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int cw{W >> 1};
         const int ch{H >> 1};
         for (int i{tid}; i < kLog2Cached; i += kThreads) sm.log2_small[i] = tb.log2_1p[i];
+        if (tid < 4) {
+            const int rw{(bw + 3) >> 2};
+            const int rx{2 * tx + (tid & 1)};
+            const int ry{2 * ty + (tid >> 1)};
+            sm.net[tid] = in.net_class != nullptr && rx < rw && ry < ((bh + 3) >> 2) ? in.net_class[ry * rw + rx]
+                                                                                    : static_cast<signed char>(-1);
+        }
         // Interior tiles whose window needs no clamping, with 4-byte aligned
         // rows, load whole 32-bit words: luma bytes px0-4 .. px0+67 of each
         // row (the window starts 2 bytes in), chroma pairs cx0 .. cx0+35
@@ -506,12 +453,18 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
     }
     __syncthreads();
+    // Regions whose transform split (and, with net_qf, quant field) the
+    // network decided; zero without a network.
+    unsigned dmask{0};
+#pragma unroll
+    for (int ri{0}; ri < 4; ++ri) dmask |= (sm.net[ri] >= 0 ? 1u : 0u) << ri;
+    const unsigned qmask{in.net_qf != nullptr ? dmask : 0u};
     // 1b. XYB of every halo pixel from the window.
     for (int i{tid}; i < kXplane; i += kThreads) {
         const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
         const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
         float x, y, b;
-        xyb_pixel(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
+        xyb_pixel<kChromaWin>(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
         xyb[i] = x;
         xyb[kXplane + i] = y;
         xyb[2 * kXplane + i] = b;
@@ -559,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int lby{lb >> 3};
         const int gbx{bx0 + lbx};
         const int gby{by0 + lby};
-        if (gbx >= bw || gby >= bh) {
+        if (gbx >= bw || gby >= bh || ((qmask >> region_of_block(lb)) & 1u) != 0) {
             continue;  // warp-uniform
         }
         const int fx{lane & 7};
@@ -645,155 +598,171 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* cdist{smem + 4608};     // per-coefficient distortion contributions
     float* crate{smem + 9216};     // per-coefficient rate contributions
     const float qg{sc.qgsf_select};
-    // 4a. DCT8 candidates: one per block inside the image.
-    for (int k{tid}; k < 512; k += kThreads) {
-        const int lb{k >> 3};
-        const int r{k & 7};
-        const int lbx{lb & 7};
-        const int lby{lb >> 3};
-        if (bx0 + lbx < bw && by0 + lby < bh) {
-            row_pass<8, 0, 8, true>(SY + (lby * 8 + r) * kSs + lbx * 8, rows + lb * 72 + r);
-        }
-    }
-    __syncthreads();
-    for (int k{tid}; k < 512; k += kThreads) {
-        const int lb{k >> 3};
-        const int fx{k & 7};
-        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
-            sel_col<8, 0, 8>(rows + lb * 72 + fx * 9, cdist + lb * 72 + fx * 9,
-                             crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p, sm.log2_small);
-        }
-    }
-    __syncthreads();
-    for (int lb{warp}; lb < 64; lb += kThreads / 32) {
-        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
-            const int i0{lb * 72 + (lane >> 3) * 9 + (lane & 7)};
-            const int i1{lb * 72 + ((lane + 32) >> 3) * 9 + (lane & 7)};
-            const float D{warp_tree(cdist[i0] + cdist[i1])};
-            const float R{warp_tree(crate[i0] + crate[i1])};
-            if (lane == 0) {
-                sm.cost8[lb] = 64.0f * D + kSelectLambda * R;
-            }
-        }
-    }
-    __syncthreads();
-    // 4b. DCT16 candidates: the 16 quads of the tile that fit in the image.
-    for (int k{tid}; k < 256; k += kThreads) {
-        const int qd{k >> 4};
-        const int r{k & 15};
-        const int qx{qd & 3};
-        const int qy{qd >> 2};
-        if (bx0 + 2 * qx + 2 <= bw && by0 + 2 * qy + 2 <= bh) {
-            row_pass<16, 0, 16, true>(SY + (qy * 16 + r) * kSs + qx * 16, rows + qd * 272 + r);
-        }
-    }
-    __syncthreads();
-    for (int k{tid}; k < 256; k += kThreads) {
-        const int qd{k >> 4};
-        const int fx{k & 15};
-        if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh) {
-            sel_col<16, 0, 16>(rows + qd * 272 + fx * 17, cdist + qd * 272 + fx * 17,
-                               crate + qd * 272 + fx * 17, fx, qg, tb.sel_weight + 1024,
-                               tb.log2_1p, sm.log2_small);
-        }
-    }
-    __syncthreads();
-    for (int qd{warp}; qd < 16; qd += kThreads / 32) {
-        if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh) {
-            float pd[8];
-            float pr[8];
+    // Regions inside the image that the network did not decide need the RD
+    // costs; when there are none the cost passes are skipped altogether.
+    unsigned inimg{0};
 #pragma unroll
-            for (int j{0}; j < 8; ++j) {
-                const int t{lane + 32 * j};
-                pd[j] = cdist[qd * 272 + (t >> 4) * 17 + (t & 15)];
-                pr[j] = crate[qd * 272 + (t >> 4) * 17 + (t & 15)];
-            }
-#pragma unroll
-            for (int j{0}; j < 4; ++j) {
-                pd[j] = pd[j] + pd[j + 4];
-                pr[j] = pr[j] + pr[j + 4];
-            }
-            pd[0] = pd[0] + pd[2];
-            pd[1] = pd[1] + pd[3];
-            pr[0] = pr[0] + pr[2];
-            pr[1] = pr[1] + pr[3];
-            const float D{warp_tree(pd[0] + pd[1])};
-            const float R{warp_tree(pr[0] + pr[1])};
-            if (lane == 0) {
-                sm.cost16[qd] = 256.0f * D + kSelectLambda * R;
+    for (int ri{0}; ri < 4; ++ri) {
+        inimg |= (bx0 + 4 * (ri & 1) < bw && by0 + 4 * (ri >> 1) < bh ? 1u : 0u) << ri;
+    }
+    if ((inimg & ~dmask) != 0u) {
+        // 4a. DCT8 candidates: one per block inside the image.
+        for (int k{tid}; k < 512; k += kThreads) {
+            const int lb{k >> 3};
+            const int r{k & 7};
+            const int lbx{lb & 7};
+            const int lby{lb >> 3};
+            if (bx0 + lbx < bw && by0 + lby < bh && ((dmask >> region_of_block(lb)) & 1u) == 0) {
+                row_pass<8, 0, 8, true>(SY + (lby * 8 + r) * kSs + lbx * 8, rows + lb * 72 + r);
             }
         }
-    }
-    __syncthreads();
-    // 4c. DCT32 candidates: the 4 regions of the tile that fit in the image.
-    for (int k{tid}; k < 256; k += kThreads) {
-        const int ri{k >> 6};
-        const int r{k & 31};
-        const bool hi{(k & 32) != 0};
-        const int rx{ri & 1};
-        const int ry{ri >> 1};
-        if (bx0 + 4 * rx + 4 <= bw && by0 + 4 * ry + 4 <= bh) {
-            const float* src{SY + (ry * 32 + r) * kSs + rx * 32};
-            float* dst{rows + ri * 1056 + r};
-            if (hi) {
-                row_pass<32, 16, 32, true>(src, dst);
-            } else {
-                row_pass<32, 0, 16, true>(src, dst);
+        __syncthreads();
+        for (int k{tid}; k < 512; k += kThreads) {
+            const int lb{k >> 3};
+            const int fx{k & 7};
+            if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh &&
+                ((dmask >> region_of_block(lb)) & 1u) == 0) {
+                sel_col<8, 0, 8>(rows + lb * 72 + fx * 9, cdist + lb * 72 + fx * 9,
+                                 crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p, sm.log2_small);
             }
         }
-    }
-    __syncthreads();
-    for (int k{tid}; k < 256; k += kThreads) {
-        const int ri{k >> 6};
-        const int fx{k & 31};
-        const bool hi{(k & 32) != 0};
-        if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh) {
-            const float* src{rows + ri * 1056 + fx * 33};
-            float* cd{cdist + ri * 1056 + fx * 33};
-            float* cr{crate + ri * 1056 + fx * 33};
-            if (hi) {
-                sel_col<32, 16, 32>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
-            } else {
-                sel_col<32, 0, 16>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
-            }
-        }
-    }
-    __syncthreads();
-    if (warp < 4) {
-        const int ri{warp};
-        if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh) {
-            float pd[8];
-            float pr[8];
-#pragma unroll
-            for (int j{0}; j < 8; ++j) {
-                float d{0.0f};
-                float r{0.0f};
-#pragma unroll
-                for (int m{0}; m < 4; ++m) {
-                    const int e{lane + 32 * j + 256 * m};
-                    d = d + cdist[ri * 1056 + (e >> 5) * 33 + (e & 31)];
-                    r = r + crate[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+        __syncthreads();
+        for (int lb{warp}; lb < 64; lb += kThreads / 32) {
+            if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh &&
+                ((dmask >> region_of_block(lb)) & 1u) == 0) {
+                const int i0{lb * 72 + (lane >> 3) * 9 + (lane & 7)};
+                const int i1{lb * 72 + ((lane + 32) >> 3) * 9 + (lane & 7)};
+                const float D{warp_tree(cdist[i0] + cdist[i1])};
+                const float R{warp_tree(crate[i0] + crate[i1])};
+                if (lane == 0) {
+                    sm.cost8[lb] = 64.0f * D + kSelectLambda * R;
                 }
-                pd[j] = d;
-                pr[j] = r;
-            }
-#pragma unroll
-            for (int j{0}; j < 4; ++j) {
-                pd[j] = pd[j] + pd[j + 4];
-                pr[j] = pr[j] + pr[j + 4];
-            }
-            pd[0] = pd[0] + pd[2];
-            pd[1] = pd[1] + pd[3];
-            pr[0] = pr[0] + pr[2];
-            pr[1] = pr[1] + pr[3];
-            const float D{warp_tree(pd[0] + pd[1])};
-            const float R{warp_tree(pr[0] + pr[1])};
-            if (lane == 0) {
-                sm.cost32[ri] = 1024.0f * D + kSelectLambda * R;
             }
         }
+        __syncthreads();
+        // 4b. DCT16 candidates: the 16 quads of the tile that fit in the image.
+        for (int k{tid}; k < 256; k += kThreads) {
+            const int qd{k >> 4};
+            const int r{k & 15};
+            const int qx{qd & 3};
+            const int qy{qd >> 2};
+            if (bx0 + 2 * qx + 2 <= bw && by0 + 2 * qy + 2 <= bh &&
+                ((dmask >> (((qy >> 1) << 1) | (qx >> 1))) & 1u) == 0) {
+                row_pass<16, 0, 16, true>(SY + (qy * 16 + r) * kSs + qx * 16, rows + qd * 272 + r);
+            }
+        }
+        __syncthreads();
+        for (int k{tid}; k < 256; k += kThreads) {
+            const int qd{k >> 4};
+            const int fx{k & 15};
+            if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh &&
+                ((dmask >> (((qd >> 3) << 1) | ((qd & 3) >> 1))) & 1u) == 0) {
+                sel_col<16, 0, 16>(rows + qd * 272 + fx * 17, cdist + qd * 272 + fx * 17,
+                                   crate + qd * 272 + fx * 17, fx, qg, tb.sel_weight + 1024,
+                                   tb.log2_1p, sm.log2_small);
+            }
+        }
+        __syncthreads();
+        for (int qd{warp}; qd < 16; qd += kThreads / 32) {
+            if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh &&
+                ((dmask >> (((qd >> 3) << 1) | ((qd & 3) >> 1))) & 1u) == 0) {
+                float pd[8];
+                float pr[8];
+#pragma unroll
+                for (int j{0}; j < 8; ++j) {
+                    const int t{lane + 32 * j};
+                    pd[j] = cdist[qd * 272 + (t >> 4) * 17 + (t & 15)];
+                    pr[j] = crate[qd * 272 + (t >> 4) * 17 + (t & 15)];
+                }
+#pragma unroll
+                for (int j{0}; j < 4; ++j) {
+                    pd[j] = pd[j] + pd[j + 4];
+                    pr[j] = pr[j] + pr[j + 4];
+                }
+                pd[0] = pd[0] + pd[2];
+                pd[1] = pd[1] + pd[3];
+                pr[0] = pr[0] + pr[2];
+                pr[1] = pr[1] + pr[3];
+                const float D{warp_tree(pd[0] + pd[1])};
+                const float R{warp_tree(pr[0] + pr[1])};
+                if (lane == 0) {
+                    sm.cost16[qd] = 256.0f * D + kSelectLambda * R;
+                }
+            }
+        }
+        __syncthreads();
+        // 4c. DCT32 candidates: the 4 regions of the tile that fit in the image.
+        for (int k{tid}; k < 256; k += kThreads) {
+            const int ri{k >> 6};
+            const int r{k & 31};
+            const bool hi{(k & 32) != 0};
+            const int rx{ri & 1};
+            const int ry{ri >> 1};
+            if (bx0 + 4 * rx + 4 <= bw && by0 + 4 * ry + 4 <= bh && ((dmask >> ri) & 1u) == 0) {
+                const float* src{SY + (ry * 32 + r) * kSs + rx * 32};
+                float* dst{rows + ri * 1056 + r};
+                if (hi) {
+                    row_pass<32, 16, 32, true>(src, dst);
+                } else {
+                    row_pass<32, 0, 16, true>(src, dst);
+                }
+            }
+        }
+        __syncthreads();
+        for (int k{tid}; k < 256; k += kThreads) {
+            const int ri{k >> 6};
+            const int fx{k & 31};
+            const bool hi{(k & 32) != 0};
+            if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh &&
+                ((dmask >> ri) & 1u) == 0) {
+                const float* src{rows + ri * 1056 + fx * 33};
+                float* cd{cdist + ri * 1056 + fx * 33};
+                float* cr{crate + ri * 1056 + fx * 33};
+                if (hi) {
+                    sel_col<32, 16, 32>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
+                } else {
+                    sel_col<32, 0, 16>(src, cd, cr, fx, qg, tb.sel_weight + 2048, tb.log2_1p, sm.log2_small);
+                }
+            }
+        }
+        __syncthreads();
+        if (warp < 4) {
+            const int ri{warp};
+            if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh &&
+                ((dmask >> ri) & 1u) == 0) {
+                float pd[8];
+                float pr[8];
+#pragma unroll
+                for (int j{0}; j < 8; ++j) {
+                    float d{0.0f};
+                    float r{0.0f};
+#pragma unroll
+                    for (int m{0}; m < 4; ++m) {
+                        const int e{lane + 32 * j + 256 * m};
+                        d = d + cdist[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+                        r = r + crate[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+                    }
+                    pd[j] = d;
+                    pr[j] = r;
+                }
+#pragma unroll
+                for (int j{0}; j < 4; ++j) {
+                    pd[j] = pd[j] + pd[j + 4];
+                    pr[j] = pr[j] + pr[j + 4];
+                }
+                pd[0] = pd[0] + pd[2];
+                pd[1] = pd[1] + pd[3];
+                pr[0] = pr[0] + pr[2];
+                pr[1] = pr[1] + pr[3];
+                const float D{warp_tree(pd[0] + pd[1])};
+                const float R{warp_tree(pr[0] + pr[1])};
+                if (lane == 0) {
+                    sm.cost32[ri] = 1024.0f * D + kSelectLambda * R;
+                }
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
     // 4d. RD decision per region (src/transform_select_impl.cuh:130-201).
     if (tid < 4) {
         const int ri{tid};
@@ -801,7 +770,26 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int rly{(ri >> 1) * 4};
         const int rbx{bx0 + rlx};
         const int rby{by0 + rly};
-        if (rbx < bw && rby < bh) {
+        if (((dmask >> ri) & 1u) != 0) {
+            // Network split of a full region: class 0 is one DCT32, class
+            // 1 + m has quadrant q as four DCT8 when bit q of m is set, else
+            // as one DCT16.
+            const int cls{sm.net[ri]};
+            for (int dy{0}; dy < 4; ++dy) {
+                for (int dx{0}; dx < 4; ++dx) {
+                    const int q{(dy >> 1) * 2 + (dx >> 1)};
+                    signed char a;
+                    if (cls == 0) {
+                        a = (dx == 0 && dy == 0) ? 32 : 0;
+                    } else if ((((cls - 1) >> q) & 1) != 0) {
+                        a = 8;
+                    } else {
+                        a = ((dx & 1) == 0 && (dy & 1) == 0) ? 16 : 0;
+                    }
+                    sm.acs[(rly + dy) * 8 + rlx + dx] = a;
+                }
+            }
+        } else if (rbx < bw && rby < bh) {
             constexpr float kInf{1.0e30f};
             const bool fit32{rbx + 4 <= bw && rby + 4 <= bh};
             const float c32{fit32 ? sm.cost32[ri] : kInf};
@@ -927,7 +915,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (tid >= 64 && tid < 128) {
         // Quant field of block lb from its AQ sums (src/frontend_fused.cu:177-201).
         const int lb{tid - 64};
-        if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
+        if (((qmask >> region_of_block(lb)) & 1u) != 0) {
+            sm.qf[lb] = in.net_qf[static_cast<std::size_t>(by0 + (lb >> 3)) * bw + bx0 + (lb & 7)];
+        } else if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
             const float hf_sum{sm.aq_sums[0][lb]};
             const float gamma_overall{sm.aq_sums[1][lb] * (0.5f / 64.0f)};
             float blue_sum{sm.aq_sums[2][lb]};

@@ -48,6 +48,12 @@ struct FrontendInputs {
     std::size_t chroma_pitch;
     int width;
     int height;
+    // Learned decisions (both null without a network): the split class of
+    // every 32x32 region ([ceil(bh/4)][ceil(bw/4)], -1 where the RD heuristic
+    // decides) and, if net_qf is set, the quant field of the blocks of
+    // decided regions ([bh][bw]).
+    const std::int8_t* net_class;
+    const std::int16_t* net_qf;
 };
 
 // Read-only tables in device memory (built once per device by

@@ -166,6 +166,91 @@ uint32_t cujpegxl_b200_batch_lanes(const cujpegxl_b200_batch* batch);
 
 void cujpegxl_b200_batch_destroy(cujpegxl_b200_batch* batch);
 
+/* ---- Learned transform decisions ----
+ * No reference counterpart. A 4-layer BF16 convolutional network over each
+ * 32x32 region of XYB pixels predicts the region's DCT32/DCT16/DCT8 split and
+ * the quant field of its 16 blocks. Regions whose softmax margin (top
+ * probability minus the runner-up) is below a threshold keep the RD
+ * heuristic, as do regions that are not a full 32x32 inside the image. The
+ * decisions only steer the encoder: the stream stays conformant and its
+ * entropy coding exact.
+ *
+ * Weights blob (little-endian): "JXBN", uint32 version 1, uint32 parameter
+ * count, uint32 channels 32, classes 17, K1 80, K 288, float32 scale[4] and
+ * shift[4] (input normalisation of X, Y, B and log2 distance), float32
+ * parameters[count], then the SHA-256 of every preceding byte. */
+typedef struct cujpegxl_b200_acsnet cujpegxl_b200_acsnet;
+
+#define CUJPEGXL_B200_ACSNET_SPLIT 1u /* use the predicted transform split */
+#define CUJPEGXL_B200_ACSNET_QF 2u    /* also use the predicted quant field */
+
+/* Parameters of the network (the length of a blob's parameter array). */
+uint32_t cujpegxl_b200_acsnet_param_count(void);
+
+/* Checks a weights blob (layout, sizes and SHA-256) without a device:
+ * CUJPEGXL_OK or CUJPEGXL_INVALID_ARGUMENT. */
+cujpegxl_status cujpegxl_b200_acsnet_check_blob(const void* blob, size_t size);
+
+/* Uploads a checked blob to `device_ordinal`. */
+cujpegxl_status cujpegxl_b200_acsnet_create(const void* blob, size_t size, int32_t device_ordinal,
+                                            cujpegxl_b200_acsnet** out_net);
+void cujpegxl_b200_acsnet_destroy(cujpegxl_b200_acsnet* net);
+
+/* Attaches `net` (NULL detaches) to an encoder on the same device. `flags` is
+ * CUJPEGXL_B200_ACSNET_SPLIT, optionally with CUJPEGXL_B200_ACSNET_QF;
+ * `margin` in [0, 1]. The network must outlive its use by the encoder. */
+cujpegxl_status cujpegxl_b200_encoder_set_acsnet(cujpegxl_encoder* encoder, const cujpegxl_b200_acsnet* net,
+                                                 float margin, uint32_t flags);
+
+/* After an encode with a network attached: regions the network decided and
+ * full 32x32 regions of the frame. Waits for the encoder's stream. */
+cujpegxl_status cujpegxl_b200_encoder_acsnet_stats(cujpegxl_encoder* encoder, uint32_t* decided,
+                                                   uint32_t* regions);
+
+/* Training. All pointers in a batch are device addresses; sample i uses tile
+ * tiles[tile_index[i]] ([3][32][32] float X, Y, B planes) at log2 distance
+ * log2_distance[i], with labels label_class[i] (split class 0..16) and
+ * label_qf[i][16] (log2 quant field of the blocks in raster order). */
+typedef struct cujpegxl_b200_acsnet_batch {
+    const float* tiles;
+    const int32_t* tile_index;
+    const float* log2_distance;
+    const int8_t* label_class;
+    const float* label_qf;
+    uint32_t n;
+} cujpegxl_b200_acsnet_batch;
+
+typedef struct cujpegxl_b200_acsnet_trainer cujpegxl_b200_acsnet_trainer;
+
+/* params[param_count] and norm[8] (scale[4] then shift[4]) are host arrays.
+ * Batches passed later hold at most max_batch samples. */
+cujpegxl_status cujpegxl_b200_acsnet_trainer_create(const float* params, const float* norm, uint32_t max_batch,
+                                                    int32_t device_ordinal,
+                                                    cujpegxl_b200_acsnet_trainer** out_trainer);
+void cujpegxl_b200_acsnet_trainer_destroy(cujpegxl_b200_acsnet_trainer* trainer);
+
+/* out[n][33] (device): the 17 split logits, then the 16 log2 quant fields. */
+cujpegxl_status cujpegxl_b200_acsnet_trainer_forward(cujpegxl_b200_acsnet_trainer* trainer,
+                                                     const cujpegxl_b200_acsnet_batch* batch, float* out,
+                                                     uintptr_t stream);
+
+/* Gradient of the batch-mean loss (cross-entropy of the split plus qf_weight
+ * times the mean squared log2 quant-field error) into grad[param_count]
+ * (device), without changing the parameters. stats[n][4] (device, may be
+ * NULL): cross-entropy, quant-field squared error, 1 if the arg-max class is
+ * the label, softmax margin. */
+cujpegxl_status cujpegxl_b200_acsnet_trainer_gradient(cujpegxl_b200_acsnet_trainer* trainer,
+                                                      const cujpegxl_b200_acsnet_batch* batch, float qf_weight,
+                                                      float* grad, float* stats, uintptr_t stream);
+
+/* One Adam step (beta1 0.9, beta2 0.999, epsilon 1e-8) on the batch. */
+cujpegxl_status cujpegxl_b200_acsnet_trainer_step(cujpegxl_b200_acsnet_trainer* trainer,
+                                                  const cujpegxl_b200_acsnet_batch* batch, float qf_weight,
+                                                  float learning_rate, float* stats, uintptr_t stream);
+
+/* Copies the FP32 parameters to params[param_count] (host); synchronous. */
+cujpegxl_status cujpegxl_b200_acsnet_trainer_params(cujpegxl_b200_acsnet_trainer* trainer, float* params);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
