@@ -123,18 +123,20 @@ class Encoder:
     def set_debug(self, enable: bool) -> None:
         check("set_debug", self._L.cujpegxl_b200_encoder_set_debug(self._h, 1 if enable else 0))
 
-    def read_planes(self, debug: bool = False) -> dict:
+    def read_planes(self, debug: bool = False, keys=None) -> dict:
+        """Planes of the last encode (the stage dumps too with debug=True);
+        `keys` restricts the copy to the named planes."""
         bw, bh = self.width // 8, self.height // 8
         nb, nt = bw * bh, ((bw + 7) // 8) * ((bh + 7) // 8)
-        r = {"ac": np.zeros(3 * nb * 64, np.int16), "dc": np.zeros(3 * nb, np.int32),
-             "acs": np.zeros(nb, np.int8), "qf": np.zeros(nb, np.int32),
-             "ytox": np.zeros(nt, np.int8), "ytob": np.zeros(nt, np.int8)}
+        shapes = {"ac": (3 * nb * 64, np.int16), "dc": (3 * nb, np.int32), "acs": (nb, np.int8),
+                  "qf": (nb, np.int32), "ytox": (nt, np.int8), "ytob": (nt, np.int8)}
         if debug:
-            r["xyb"] = np.zeros(3 * self.width * self.height, np.float32)
-            r["sharp"] = np.zeros(3 * self.width * self.height, np.float32)
-            r["coeff"] = np.zeros(3 * nb * 64, np.uint16)
+            shapes.update({"xyb": (3 * self.width * self.height, np.float32),
+                           "sharp": (3 * self.width * self.height, np.float32),
+                           "coeff": (3 * nb * 64, np.uint16), "cost": (3 * nb, np.float32)})
+        r = {k: np.zeros(n, dt) for k, (n, dt) in shapes.items() if keys is None or k in keys}
         p = _capi.Planes(*[_capi.ptr(r.get(k)) for k in ("ac", "dc", "acs", "qf", "ytox", "ytob",
-                                                         "xyb", "sharp", "coeff")])
+                                                         "xyb", "sharp", "coeff", "cost")])
         check("read_planes", self._L.cujpegxl_b200_encoder_read_planes(self._h, ctypes.byref(p)))
         return r
 
@@ -143,7 +145,7 @@ class Encoder:
                 (("ac", np.int16), ("dc", np.int32), ("acs", np.int8), ("qf", np.int32),
                  ("ytox", np.int8), ("ytob", np.int8))}
         p = _capi.Planes(*[_capi.ptr(keep.get(k)) for k in ("ac", "dc", "acs", "qf", "ytox", "ytob")],
-                         None, None, None)
+                         None, None, None, None)
         out = self._output()
         check("encode_planes", self._L.cujpegxl_b200_encode_planes(self._h, ctypes.byref(p), global_scale,
                                                                    quant_dc, ctypes.byref(out)))

@@ -55,12 +55,14 @@ class Output(ctypes.Structure):
 
 
 class Planes(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_void_p) for n in ("ac", "dc", "acs", "qf", "ytox", "ytob", "xyb", "sharp", "coeff")]
+    _fields_ = [(n, ctypes.c_void_p) for n in ("ac", "dc", "acs", "qf", "ytox", "ytob", "xyb", "sharp", "coeff",
+                                                "cost")]
 
 
 class NetBatch(ctypes.Structure):
     _fields_ = [("tiles", ctypes.c_size_t), ("tile_index", ctypes.c_size_t), ("log2_distance", ctypes.c_size_t),
-                ("label_class", ctypes.c_size_t), ("label_qf", ctypes.c_size_t), ("n", ctypes.c_uint32)]
+                ("label_class", ctypes.c_size_t), ("label_qf", ctypes.c_size_t), ("n", ctypes.c_uint32),
+                ("label_soft", ctypes.c_size_t)]
 
 
 class DevicePlanes(ctypes.Structure):

@@ -8,7 +8,7 @@ quantisation produce on seeded synthetic frames, entirely on the GPU by the
 library's own BF16 kernels (forward, backward, Adam); at encode time regions
 where its softmax margin is below a threshold keep the heuristic.
 
-    python -m cujpegxl_b200.acsnet --out cujpegxl_b200/data/acsnet_v1.jxbn
+    python -m cujpegxl_b200.acsnet --out cujpegxl_b200/data/acsnet_v2.jxbn
 
 trains the shipped weights (about a minute on one B200) and writes a JSON
 report beside them.
@@ -39,11 +39,11 @@ NW = C * K1 + 3 * C * K
 OFF_B = NW
 NPARAMS = NW + 4 * C
 MAGIC = b"JXBN"
-VERSION = 1
+VERSION = 2
 SPLIT = 1
 QF = 2
 DEFAULT_MARGIN = 0.2
-DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "data" / "acsnet_v1.jxbn"
+DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "data" / "acsnet_v2.jxbn"
 
 
 def pack_blob(params: np.ndarray, norm: np.ndarray) -> bytes:
@@ -111,10 +111,34 @@ def region_qf(qf: np.ndarray, width: int, height: int) -> np.ndarray:
 
 
 def region_tiles(xyb: np.ndarray, width: int, height: int) -> np.ndarray:
-    """[H/32 * W/32][3][32][32] XYB tiles of the full regions, raster order."""
+    """[H/32 * W/32][3][34][34] XYB inputs of the full regions, raster order:
+    each region with a 1-pixel ring of its neighbours (coordinates clamped to
+    the image, as the inference kernel reads them)."""
     rw, rh = width // 32, height // 32
-    x = np.asarray(xyb, np.float32).reshape(3, height, width)[:, :32 * rh, :32 * rw]
-    return np.ascontiguousarray(x.reshape(3, rh, 32, rw, 32).transpose(1, 3, 0, 2, 4).reshape(rh * rw, 3, 32, 32))
+    x = np.pad(np.asarray(xyb, np.float32).reshape(3, height, width), ((0, 0), (1, 1), (1, 1)), mode="edge")
+    out = np.empty((rh * rw, 3, 34, 34), np.float32)
+    for ry in range(rh):
+        for rx in range(rw):
+            out[ry * rw + rx] = x[:, 32 * ry:32 * ry + 34, 32 * rx:32 * rx + 34]
+    return out
+
+
+def class_costs(cost: np.ndarray, width: int, height: int) -> np.ndarray:
+    """RD cost of each of the 17 splits of every full region, [H/32][W/32][17],
+    from the selection-cost planes ([3][B]: DCT8 per block, DCT16 at quad and
+    DCT32 at region first blocks). Their arg-min is the heuristic's choice."""
+    bw, bh = width // 8, height // 8
+    rw, rh = width // 32, height // 32
+    c = np.asarray(cost, np.float64).reshape(3, bh, bw)[:, :4 * rh, :4 * rw]
+    c = c.reshape(3, rh, 4, rw, 4).transpose(0, 1, 3, 2, 4)  # [3][rh][rw][4][4]
+    c8 = c[0].reshape(rh, rw, 2, 2, 2, 2).sum(axis=(3, 5)).reshape(rh, rw, 4)
+    c16 = c[1][:, :, 0::2, 0::2].reshape(rh, rw, 4)
+    out = np.empty((rh, rw, NCLS), np.float64)
+    out[..., 0] = c[2][:, :, 0, 0]
+    for m in range(16):
+        bits = np.array([(m >> q) & 1 for q in range(4)], bool)
+        out[..., 1 + m] = np.where(bits, c8, c16).sum(axis=-1)
+    return out
 
 
 class AcsNet:
@@ -154,16 +178,25 @@ def check_blob(blob: bytes) -> bool:
     return _capi.lib().cujpegxl_b200_acsnet_check_blob(buf, len(blob)) == _capi.OK
 
 
-def _batch(tiles, tile_index, log2d, label_class=None, label_qf=None) -> _capi.NetBatch:
+def _batch(tiles, tile_index, log2d, label_class=None, label_qf=None, label_soft=None) -> _capi.NetBatch:
     def p(t):
         return 0 if t is None else t.data_ptr()
-    return _capi.NetBatch(p(tiles), p(tile_index), p(log2d), p(label_class), p(label_qf), int(tile_index.numel()))
+    return _capi.NetBatch(p(tiles), p(tile_index), p(log2d), p(label_class), p(label_qf), int(tile_index.numel()),
+                          p(label_soft))
+
+
+def soft_targets(regret, temperature: float):
+    """Target distribution over the 17 splits from their relative RD regret
+    (cost / min cost - 1): softmax(-regret / temperature)."""
+    import torch
+    return torch.softmax(-regret / temperature, dim=1).float().contiguous()
 
 
 class Trainer:
     """FP32 master weights, Adam state and activation scratch on the device.
-    Batches are torch CUDA tensors: tiles float32 [T][3][32][32], tile_index
-    int32 [n], log2d float32 [n], label_class int8 [n], label_qf float32 [n][16]."""
+    Batches are torch CUDA tensors: tiles float32 [T][3][34][34], tile_index
+    int32 [n], log2d float32 [n], label_class int8 [n], label_qf float32 [n][16],
+    optional label_soft float32 [n][17]."""
 
     def __init__(self, params: np.ndarray, norm: np.ndarray, max_batch: int, device_ordinal: int = 0):
         import torch
@@ -188,17 +221,18 @@ class Trainer:
             self._h, ctypes.byref(b), out.data_ptr(), self._stream()))
         return out
 
-    def gradient(self, tiles, tile_index, log2d, label_class, label_qf, qf_weight: float):
+    def gradient(self, tiles, tile_index, log2d, label_class, label_qf, qf_weight: float, label_soft=None):
         t = self._torch
         grad = t.empty(NPARAMS, dtype=t.float32, device=self.device)
         stats = t.empty((tile_index.numel(), 4), dtype=t.float32, device=self.device)
-        b = _batch(tiles, tile_index, log2d, label_class, label_qf)
+        b = _batch(tiles, tile_index, log2d, label_class, label_qf, label_soft)
         check("acsnet_trainer_gradient", self._L.cujpegxl_b200_acsnet_trainer_gradient(
             self._h, ctypes.byref(b), qf_weight, grad.data_ptr(), stats.data_ptr(), self._stream()))
         return grad, stats
 
-    def step(self, tiles, tile_index, log2d, label_class, label_qf, qf_weight: float, lr: float, stats=None):
-        b = _batch(tiles, tile_index, log2d, label_class, label_qf)
+    def step(self, tiles, tile_index, log2d, label_class, label_qf, qf_weight: float, lr: float, stats=None,
+             label_soft=None):
+        b = _batch(tiles, tile_index, log2d, label_class, label_qf, label_soft)
         check("acsnet_trainer_step", self._L.cujpegxl_b200_acsnet_trainer_step(
             self._h, ctypes.byref(b), qf_weight, lr, 0 if stats is None else stats.data_ptr(), self._stream()))
 
@@ -231,33 +265,36 @@ def build_dataset(frames: list[tuple[int, int, int]], distances: list[float], de
 
     frames: (width, height, seed). Every full 32x32 region of every frame is
     one tile; each tile gets one sample per distance, labelled with the split
-    the RD heuristic chose and the adaptive quant field (log2) of its blocks."""
+    the RD heuristic chose, the relative RD regret of all 17 splits
+    (cost / min cost - 1) and the adaptive quant field (log2) of its blocks."""
     import torch
     from . import Encoder
     from .synth import make_nv12
     dev = torch.device("cuda", device_ordinal)
-    tiles, t_idx, l2d, cls, lqf = [], [], [], [], []
+    tiles, t_idx, l2d, cls, lqf, reg = [], [], [], [], [], []
     base = 0
     for (w, h, seed) in frames:
         nv12 = make_nv12(w, h, seed)
         with Encoder(w, h, distances[0], device_ordinal) as enc:
             enc.set_debug(True)
-            enc.encode_host(nv12)
-            xyb = enc.read_planes(debug=True)["xyb"]
-            enc.set_debug(False)
-            tl = region_tiles(xyb, w, h)
-            tiles.append(torch.from_numpy(tl).to(dev))
             for d in distances:
                 enc.configure(w, h, d)
                 enc.encode_host(nv12)
-                pl = enc.read_planes()
+                pl = enc.read_planes(debug=True, keys=("acs", "qf", "cost", "xyb") if d == distances[0] else
+                                     ("acs", "qf", "cost"))
+                if d == distances[0]:
+                    tl = region_tiles(pl["xyb"], w, h)
+                    tiles.append(torch.from_numpy(tl).to(dev))
                 c = split_classes(pl["acs"], w, h).reshape(-1)
                 q = region_qf(pl["qf"], w, h).reshape(-1, 16)
+                cc = class_costs(pl["cost"], w, h).reshape(-1, NCLS)
                 ok = np.nonzero(c >= 0)[0]
                 t_idx.append(base + ok.astype(np.int32))
                 l2d.append(np.full(ok.size, math.log2(d), np.float32))
                 cls.append(c[ok])
                 lqf.append(np.log2(q[ok].astype(np.float64)).astype(np.float32))
+                low = cc[ok].min(axis=1, keepdims=True)
+                reg.append((cc[ok] / np.maximum(low, 1e-9) - 1.0).astype(np.float32))
         base += tl.shape[0]
         log(f"dataset: {w}x{h} seed {seed}: {tl.shape[0]} tiles")
     return {
@@ -266,6 +303,7 @@ def build_dataset(frames: list[tuple[int, int, int]], distances: list[float], de
         "log2d": torch.from_numpy(np.concatenate(l2d)).to(dev),
         "label_class": torch.from_numpy(np.concatenate(cls)).to(dev),
         "label_qf": torch.from_numpy(np.concatenate(lqf)).to(dev),
+        "regret": torch.from_numpy(np.concatenate(reg)).to(dev),
     }
 
 
@@ -286,11 +324,13 @@ def normalisation(data: dict) -> np.ndarray:
 
 def evaluate(trainer: Trainer, data: dict, margin: float = DEFAULT_MARGIN) -> dict:
     """Split accuracy over all samples, the fraction with a softmax margin of
-    at least `margin` and the accuracy on those, and the log2 quant-field RMSE."""
+    at least `margin` and the accuracy on those, the mean relative RD regret
+    of the network's split where it is sure (and over all samples, counting
+    the heuristic's fallback as no regret), and the log2 quant-field RMSE."""
     import torch
     n = data["tile_index"].numel()
     correct = covered = covered_ok = 0
-    sq = 0.0
+    sq = regret = 0.0
     for s in range(0, n, trainer.max_batch):
         e = min(n, s + trainer.max_batch)
         out = trainer.forward(data["tiles"], data["tile_index"][s:e], data["log2d"][s:e])
@@ -304,15 +344,21 @@ def evaluate(trainer: Trainer, data: dict, margin: float = DEFAULT_MARGIN) -> di
         covered += int(conf.sum())
         covered_ok += int((ok & conf).sum())
         sq += float(((out[:, NCLS:].double() - data["label_qf"][s:e].double()) ** 2).sum())
+        r = data["regret"][s:e].double().gather(1, pred[:, None])[:, 0]
+        regret += float((r * conf).sum())
     return {"samples": n, "accuracy": correct / n, "coverage": covered / n,
-            "covered_accuracy": covered_ok / max(1, covered), "qf_rmse_log2": math.sqrt(sq / (16 * n))}
+            "covered_accuracy": covered_ok / max(1, covered), "regret_covered": regret / max(1, covered),
+            "regret_effective": regret / n, "qf_rmse_log2": math.sqrt(sq / (16 * n))}
 
 
 def train(data: dict, *, steps: int, batch: int, lr: float, qf_weight: float, seed: int,
           device_ordinal: int = 0, log=print, params: np.ndarray | None = None,
-          norm: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray, list]:
+          norm: np.ndarray | None = None, temperature: float = 0.0) -> tuple[np.ndarray, np.ndarray, list]:
     """Adam with a cosine learning-rate decay over `steps` batches drawn with
-    replacement (seeded). Returns (params, norm, loss curve)."""
+    replacement (seeded). temperature > 0 trains the split against
+    soft_targets(regret, temperature) instead of the heuristic's one-hot
+    choice, so that near-ties cost little and expensive mistakes much.
+    Returns (params, norm, loss curve)."""
     import torch
     norm = normalisation(data) if norm is None else norm
     params = init_params(seed) if params is None else params
@@ -328,8 +374,9 @@ def train(data: dict, *, steps: int, batch: int, lr: float, qf_weight: float, se
         for step in range(steps):
             idx = torch.randint(0, n, (batch,), generator=gen, device=tr.device)
             rate = lr * 0.5 * (1.0 + math.cos(math.pi * step / steps))
+            soft = soft_targets(data["regret"][idx], temperature) if temperature > 0 else None
             tr.step(data["tiles"], data["tile_index"][idx], data["log2d"][idx], data["label_class"][idx],
-                    data["label_qf"][idx], qf_weight, rate, stats)
+                    data["label_qf"][idx], qf_weight, rate, stats, soft)
             acc += stats.double().mean(dim=0)
             since += 1
             if (step + 1) % 200 == 0 or step + 1 == steps:
@@ -392,11 +439,12 @@ def main(argv=None) -> int:
     ap.add_argument("--frames-4k", type=int, default=24)
     ap.add_argument("--val-frames", type=int, default=4)
     ap.add_argument("--distances", default="0.5,1,1.5,2,3,4")
-    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--steps", type=int, default=40000)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--qf-weight", type=float, default=1.0)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--temperature", type=float, default=0.03)
     a = ap.parse_args(argv)
     dists = [float(x) for x in a.distances.split(",")]
     t0 = time.time()
@@ -405,12 +453,13 @@ def main(argv=None) -> int:
     t_data = time.time() - t0
     t1 = time.time()
     params, norm, curve = train(train_data, steps=a.steps, batch=a.batch, lr=a.lr, qf_weight=a.qf_weight,
-                                seed=a.seed)
+                                seed=a.seed, temperature=a.temperature)
     t_train = time.time() - t1
     report = {"frames_1080p": a.frames_1080p, "frames_4k": a.frames_4k, "distances": dists,
               "train_samples": int(train_data["tile_index"].numel()),
               "train_tiles": int(train_data["tiles"].shape[0]), "steps": a.steps, "batch": a.batch,
-              "lr": a.lr, "qf_weight": a.qf_weight, "seed": a.seed, "dataset_seconds": round(t_data, 1),
+              "lr": a.lr, "qf_weight": a.qf_weight, "seed": a.seed, "temperature": a.temperature,
+              "dataset_seconds": round(t_data, 1),
               "train_seconds": round(t_train, 1), "curve": curve}
     with Trainer(params, norm, a.batch) as tr:
         report["train_eval"] = evaluate(tr, train_data)

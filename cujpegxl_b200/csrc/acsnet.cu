@@ -49,7 +49,7 @@ struct NetSmem {
     bf16 w[3][kNetC * kWS];
     float bias[4][kNetC];
     bf16 zero[8];
-    bf16 x1[1024 * kNetIn];
+    bf16 x1[kNetInPix * kNetIn];
     bf16 x2[256 * kActS];
     bf16 x3[64 * kActS];
     bf16 x4[16 * kActS];
@@ -114,27 +114,26 @@ __device__ __forceinline__ void store_pair(bf16* dst, float lo, float hi) {
 }
 
 // Shared-memory address of im2col row p, reduction columns k0..k0+7, for a
-// 3x3 convolution with padding 1 over a kInW x kInW input of kCin channels
-// stored kInS apart; the zero chunk where the tap is padding.
-template <int kInW, int kStride, int kCin, int kInS>
+// 3x3 convolution with padding kPad over a kInW x kInW input of kCin channels
+// stored kInS apart, kOutW x kOutW outputs; the zero chunk where the tap is
+// padding (or a reduction column past the nine taps).
+template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS>
 __device__ __forceinline__ unsigned im2col_row(unsigned in, unsigned zero, int p, int k0) {
-    constexpr int kOutW{kInW / kStride};
     const int tap{k0 / kCin};
     const int ci{k0 - tap * kCin};
     const int oy{p / kOutW};
     const int ox{p - oy * kOutW};
-    const int iy{oy * kStride + tap / 3 - 1};
-    const int ix{ox * kStride + tap % 3 - 1};
+    const int iy{oy * kStride + tap / 3 - kPad};
+    const int ix{ox * kStride + tap % 3 - kPad};
     const bool ok{tap < 9 && iy >= 0 && iy < kInW && ix >= 0 && ix < kInW};
     return ok ? in + 2u * static_cast<unsigned>((iy * kInW + ix) * kInS + ci) : zero;
 }
 
 // Forward of a layer with at least four 16-row position tiles (L1, L2): warp w
 // takes position tiles w, w+4, ... and all four 8-channel output tiles.
-template <int kInW, int kStride, int kCin, int kInS, int kK, int kWStr>
+template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS, int kK, int kWStr>
 __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* out,
                                          int warp, int lane) {
-    constexpr int kOutW{kInW / kStride};
     constexpr int kMW{kOutW * kOutW / 64};
     float acc[kMW][4][4];
 #pragma unroll
@@ -161,8 +160,8 @@ __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w,
 #pragma unroll
         for (int i{0}; i < kMW; ++i) {
             unsigned a[4];
-            ldsm_x4(a, im2col_row<kInW, kStride, kCin, kInS>(in, zero, (warp + 4 * i) * 16 + (lane & 15),
-                                                             k0 + (lane >> 4) * 8));
+            ldsm_x4(a, im2col_row<kInW, kOutW, kStride, kPad, kCin, kInS>(in, zero, (warp + 4 * i) * 16 + (lane & 15),
+                                                                          k0 + (lane >> 4) * 8));
 #pragma unroll
             for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
         }
@@ -190,7 +189,7 @@ __device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w,
 #pragma unroll 3
     for (int k0{0}; k0 < kNetK; k0 += 16) {
         unsigned a[4];
-        ldsm_x4(a, im2col_row<kInW, kStride, kNetC, kActS>(in, zero, lane & 15, k0 + (lane >> 4) * 8));
+        ldsm_x4(a, im2col_row<kInW, 4, kStride, 1, kNetC, kActS>(in, zero, lane & 15, k0 + (lane >> 4) * 8));
         unsigned b[2];
         ldsm_x2(b, w + 2u * static_cast<unsigned>((8 * warp + (lane & 7)) * kWS + k0 + ((lane >> 3) & 1) * 8));
         mma(acc, a, b[0], b[1]);
@@ -361,9 +360,10 @@ __device__ __forceinline__ uint4 input_pixel(const NetParamsDev& p, float x, flo
 // The four layers over the region in s.x1; ends with s.out filled.
 __device__ __forceinline__ void net_forward(NetSmem& s, int warp, int lane) {
     const unsigned zero{saddr(s.zero)};
-    fwd_rows<32, 2, kNetIn, kNetIn, kNetK1, kW1S>(saddr(s.x1), zero, saddr(s.w1), s.bias[0], s.x2, warp, lane);
+    fwd_rows<kNetInW, 16, 2, 0, kNetIn, kNetIn, kNetK1, kW1S>(saddr(s.x1), zero, saddr(s.w1), s.bias[0], s.x2, warp,
+                                                            lane);
     __syncthreads();
-    fwd_rows<16, 2, kNetC, kActS, kNetK, kWS>(saddr(s.x2), zero, saddr(s.w[0]), s.bias[1], s.x3, warp, lane);
+    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS>(saddr(s.x2), zero, saddr(s.w[0]), s.bias[1], s.x3, warp, lane);
     __syncthreads();
     fwd_cols<8, 2, true>(saddr(s.x3), zero, saddr(s.w[1]), s.bias[2], s.x4, nullptr, warp, lane);
     __syncthreads();
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(kNetThreads, 2)
     const int tw{(W + 63) >> 6};
     const int ntiles{tw * ((H + 63) >> 6)};
     std::uint8_t* win_luma{reinterpret_cast<std::uint8_t*>(s.x2)};
-    std::uint8_t* win_chroma{win_luma + 1024};
+    std::uint8_t* win_chroma{win_luma + kNetInPix + 12};
     for (int t{static_cast<int>(blockIdx.x)}; t < ntiles; t += static_cast<int>(gridDim.x)) {
 #pragma unroll 1
         for (int ri{0}; ri < 4; ++ri) {
@@ -457,8 +457,11 @@ __global__ void __launch_bounds__(kNetThreads, 2)
             __syncthreads();  // the previous region is done with x2 and out
             const int cx0{(px0 >> 1) - 2};
             const int cy0{(py0 >> 1) - 2};
-            for (int i{tid}; i < 1024; i += kNetThreads) {
-                win_luma[i] = in.luma[static_cast<std::size_t>(py0 + (i >> 5)) * in.luma_pitch + px0 + (i & 31)];
+            // Luma of the region and its 1-pixel ring, at clamped coordinates.
+            for (int i{tid}; i < kNetInPix; i += kNetThreads) {
+                const int gx{min(max(px0 - 1 + i % kNetInW, 0), W - 1)};
+                const int gy{min(max(py0 - 1 + i / kNetInW, 0), H - 1)};
+                win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
             }
             for (int i{tid}; i < kRegionWin * kRegionWin; i += kNetThreads) {
                 const int jx{min(max(cx0 + i % kRegionWin, 0), (W >> 1) - 1)};
@@ -468,10 +471,11 @@ __global__ void __launch_bounds__(kNetThreads, 2)
                 win_chroma[2 * i + 1] = c[1];
             }
             __syncthreads();
-            for (int i{tid}; i < 1024; i += kNetThreads) {
+            for (int i{tid}; i < kNetInPix; i += kNetThreads) {
+                const int gx{min(max(px0 - 1 + i % kNetInW, 0), W - 1)};
+                const int gy{min(max(py0 - 1 + i / kNetInW, 0), H - 1)};
                 float x, y, b;
-                xyb_pixel<kRegionWin>(win_luma[i], win_chroma, cx0, cy0, px0 + (i & 31), py0 + (i >> 5), W, H, x,
-                                      y, b);
+                xyb_pixel<kRegionWin>(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
                 *reinterpret_cast<uint4*>(&s.x1[i * kNetIn]) = input_pixel(p, x, y, b, log2_distance);
             }
             __syncthreads();
@@ -511,11 +515,11 @@ __global__ void __launch_bounds__(kNetThreads)
     const unsigned zero{saddr(s.zero)};
     for (std::uint32_t i{blockIdx.x}; i < b.n; i += gridDim.x) {
         __syncthreads();
-        const float* tile{b.tiles + static_cast<std::size_t>(b.tile_index[i]) * 3072};
+        const float* tile{b.tiles + static_cast<std::size_t>(b.tile_index[i]) * 3 * kNetInPix};
         const float l2d{b.log2_distance[i]};
-        for (int px{tid}; px < 1024; px += kNetThreads) {
+        for (int px{tid}; px < kNetInPix; px += kNetThreads) {
             *reinterpret_cast<uint4*>(&s.x1[px * kNetIn]) =
-                input_pixel(p, tile[px], tile[1024 + px], tile[2048 + px], l2d);
+                input_pixel(p, tile[px], tile[kNetInPix + px], tile[2 * kNetInPix + px], l2d);
         }
         __syncthreads();
         net_forward(s, warp, lane);
@@ -531,8 +535,13 @@ __global__ void __launch_bounds__(kNetThreads)
             const int label{b.label_class[i]};
             const float lg{split_logit(s.out, lane)};
             const SplitHead h{split_head(lg)};
-            const float dlogit{(h.prob - (lane == label ? 1.0f : 0.0f)) * inv_batch};
-            const float ce{h.lse - __shfl_sync(0xffffffffu, lg, label)};
+            // Target: the label's one-hot vector, or a given distribution.
+            float t{lane == label ? 1.0f : 0.0f};
+            if (b.label_soft != nullptr) {
+                t = lane < kNetClasses ? b.label_soft[static_cast<std::size_t>(i) * kNetClasses + lane] : 0.0f;
+            }
+            const float dlogit{(h.prob - t) * inv_batch};
+            const float ce{h.lse - warp_sum(lane < kNetClasses ? t * lg : 0.0f)};
             float d{0.0f};
             if (lane < 16) d = s.out[lane * kNetC] - b.label_qf[static_cast<std::size_t>(i) * 16 + lane];
             const float sq{warp_sum(d * d)};
@@ -570,7 +579,7 @@ __global__ void __launch_bounds__(kNetThreads)
                     *reinterpret_cast<const uint4*>(src + px * stride + c * 8);
             }
         };
-        put(kNetActX1, s.x1, 1024, kNetIn, kNetIn);
+        put(kNetActX1, s.x1, kNetInPix, kNetIn, kNetIn);
         put(kNetActX2, s.x2, 256, kActS, kNetC);
         put(kNetActX3, s.x3, 64, kActS, kNetC);
         put(kNetActX4, s.x4, 16, kActS, kNetC);
@@ -584,12 +593,14 @@ __global__ void __launch_bounds__(kNetThreads)
 // Geometry of layer L (1..4) for the weight gradient.
 template <int L>
 struct LayerGeo {
-    static constexpr int kInW = L == 1 ? 32 : (L == 2 ? 16 : (L == 3 ? 8 : 4));
+    static constexpr int kInW = L == 1 ? kNetInW : (L == 2 ? 16 : (L == 3 ? 8 : 4));
+    static constexpr int kOutW = L == 1 ? 16 : (L == 2 ? 8 : 4);
+    static constexpr int kPad = L == 1 ? 0 : 1;
     static constexpr int kStride = L == 4 ? 1 : 2;
     static constexpr int kCin = L == 1 ? kNetIn : kNetC;
     static constexpr int kInS = L == 1 ? kNetIn : kActS;
     static constexpr int kK = L == 1 ? kNetK1 : kNetK;
-    static constexpr int kP = (kInW / kStride) * (kInW / kStride);
+    static constexpr int kP = kOutW * kOutW;
     static constexpr int kXOff = L == 1 ? kNetActX1 : (L == 2 ? kNetActX2 : (L == 3 ? kNetActX3 : kNetActX4));
     static constexpr int kGOff = L == 1 ? kNetActG1 : (L == 2 ? kNetActG2 : (L == 3 ? kNetActG3 : kNetActG4));
     static constexpr int kWOff = L == 1 ? kNetW1 : (L == 2 ? kNetW2 : (L == 3 ? kNetW3 : kNetW4));
@@ -658,7 +669,7 @@ __global__ void __launch_bounds__(kGradThreads) acsnet_wgrad_kernel(const bf16* 
                 const int pair{warp + 8 * pi};
                 if (pair < kPairs) {
                     unsigned bb[4];
-                    ldsm_x4_t(bb, im2col_row<G::kInW, G::kStride, G::kCin, G::kInS>(
+                    ldsm_x4_t(bb, im2col_row<G::kInW, G::kOutW, G::kStride, G::kPad, G::kCin, G::kInS>(
                                       xa, za, kp + (lane & 7) + ((lane >> 3) & 1) * 8, pair * 16 + (lane >> 4) * 8));
 #pragma unroll
                     for (int m{0}; m < 2; ++m) {
@@ -862,7 +873,7 @@ float rdf(const std::uint8_t* p) {
 bool blob_ok(const void* blob, std::size_t size) {
     if (blob == nullptr || size != kBlobBytes) return false;
     const auto* b{static_cast<const std::uint8_t*>(blob)};
-    if (std::memcmp(b, "JXBN", 4) != 0 || rd32(b + 4) != 1u || rd32(b + 8) != static_cast<std::uint32_t>(jxb::kNetParams) ||
+    if (std::memcmp(b, "JXBN", 4) != 0 || rd32(b + 4) != 2u || rd32(b + 8) != static_cast<std::uint32_t>(jxb::kNetParams) ||
         rd32(b + 12) != 32u || rd32(b + 16) != 17u || rd32(b + 20) != 80u || rd32(b + 24) != 288u) {
         return false;
     }
@@ -947,7 +958,7 @@ bool batch_dev(const cujpegxl_b200_acsnet_batch* b, std::uint32_t max_batch, boo
     }
     if (labels && (b->label_class == nullptr || b->label_qf == nullptr)) return false;
     *out = jxb::NetBatchDev{b->tiles, b->tile_index, b->log2_distance, labels ? b->label_class : nullptr,
-                            labels ? b->label_qf : nullptr, b->n};
+                            labels ? b->label_qf : nullptr, labels ? b->label_soft : nullptr, b->n};
     return true;
 }
 

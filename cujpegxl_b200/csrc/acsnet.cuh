@@ -1,12 +1,14 @@
 // Transform-decision network: a 4-layer convolutional network over one 32x32
-// region of XYB pixels that predicts the region's DCT32/DCT16/DCT8 split
-// (17 classes) and the log2 quant field of each of its 16 blocks.
+// region of XYB pixels (with a 1-pixel ring of its neighbours, clamped at the
+// image border) that predicts the region's DCT32/DCT16/DCT8 split (17
+// classes) and the log2 quant field of each of its 16 blocks.
 //
-// Layers (BF16 weights and activations, FP32 accumulation, zero padding 1):
-//   L1  3x3 stride 2   8 -> 32 channels   32x32 -> 16x16   ReLU
+// Layers (BF16 weights and activations, FP32 accumulation):
+//   L1  3x3 stride 2   8 -> 32 channels   34x34 -> 16x16   ReLU (no padding)
 //   L2  3x3 stride 2  32 -> 32            16x16 ->  8x8    ReLU
 //   L3  3x3 stride 2  32 -> 32             8x8  ->  4x4    ReLU
 //   L4  3x3 stride 1  32 -> 32             4x4  ->  4x4    (linear)
+// (L2..L4 zero-pad by 1.)
 // Input channels: X, Y, B and log2(distance), each normalised as
 // (v - shift) * scale, then four zero channels. Output channel 0 of L4 at
 // block position p is the block's log2 quant field; channels 1..17 averaged
@@ -22,6 +24,8 @@
 
 namespace jxb {
 
+constexpr int kNetInW = 34;      // input side: the region and a 1-pixel ring
+constexpr int kNetInPix = kNetInW * kNetInW;
 constexpr int kNetC = 32;        // output channels of every layer
 constexpr int kNetIn = 8;        // stored input channels
 constexpr int kNetClasses = 17;
@@ -50,23 +54,24 @@ struct NetParamsDev {
 
 // Per-sample activations kept by the training forward/backward kernel for the
 // weight-gradient kernel (BF16, compact [position][channel]).
-constexpr int kNetActX1 = 0;                       // [1024][8]
-constexpr int kNetActX2 = kNetActX1 + 1024 * 8;    // [256][32]
+constexpr int kNetActX1 = 0;                       // [34*34][8]
+constexpr int kNetActX2 = kNetActX1 + kNetInPix * 8;  // [256][32]
 constexpr int kNetActX3 = kNetActX2 + 256 * 32;    // [64][32]
 constexpr int kNetActX4 = kNetActX3 + 64 * 32;     // [16][32]
 constexpr int kNetActG1 = kNetActX4 + 16 * 32;     // [256][32] dL/d(L1 pre-activation)
 constexpr int kNetActG2 = kNetActG1 + 256 * 32;    // [64][32]
 constexpr int kNetActG3 = kNetActG2 + 64 * 32;     // [16][32]
 constexpr int kNetActG4 = kNetActG3 + 16 * 32;     // [16][32] dL/d(L4 output)
-constexpr int kNetActPerSample = kNetActG4 + 16 * 32;  // 30208 BF16 values
+constexpr int kNetActPerSample = kNetActG4 + 16 * 32;  // 31264 BF16 values
 
 // One training or evaluation batch in device memory.
 struct NetBatchDev {
-    const float* tiles;          // [ntiles][3][32][32] XYB
+    const float* tiles;          // [ntiles][3][34][34] XYB
     const std::int32_t* tile_index;  // [n] tile of each sample
     const float* log2_distance;  // [n]
     const std::int8_t* label_class;  // [n] or null (forward only)
     const float* label_qf;       // [n][16] log2 quant field, or null
+    const float* label_soft;     // [n][17] target distribution replacing the one-hot class, or null
     std::uint32_t n;
 };
 

@@ -42,6 +42,7 @@ struct cujpegxl_encoder {
     float* dbg_xyb{nullptr};
     float* dbg_sharp{nullptr};
     std::uint16_t* dbg_coeff{nullptr};
+    float* dbg_cost{nullptr};
     std::uint8_t* nv12_dev{nullptr};
     std::uint8_t* nv12_pinned{nullptr};
     unsigned long long* result_pinned{nullptr};
@@ -196,7 +197,7 @@ bool allocate(cujpegxl_encoder* e) {
     const std::size_t o_nqf{a.take(nb * 2)};
     std::size_t o_dbg{0};
     if (e->debug) {
-        o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2);
+        o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2 + 3 * nb * 4);
     }
     void* base{nullptr};
     if (cudaMalloc(&base, a.total) != cudaSuccess) return false;
@@ -220,6 +221,8 @@ bool allocate(cujpegxl_encoder* e) {
     fo.dbg_xyb = e->dbg_xyb;
     fo.dbg_sharp = e->dbg_sharp;
     fo.dbg_coeff = e->dbg_coeff;
+    e->dbg_cost = e->debug ? reinterpret_cast<float*>(e->dbg_coeff + 3 * nb * 64) : nullptr;
+    fo.dbg_cost = e->dbg_cost;
 
     jxb::EntropyDev& ed{e->ed};
     ed = jxb::EntropyDev{};
@@ -601,6 +604,7 @@ cujpegxl_status cujpegxl_b200_encoder_read_planes(cujpegxl_encoder* encoder, con
         {host->xyb, encoder->dbg_xyb, 3 * W * H * 4},
         {host->sharp, encoder->dbg_sharp, 3 * W * H * 4},
         {host->coeff, encoder->dbg_coeff, 3 * nb * 64 * 2},
+        {host->cost, encoder->dbg_cost, 3 * nb * 4},
     };
     for (const Copy& c : copies) {
         if (c.dst == nullptr) continue;

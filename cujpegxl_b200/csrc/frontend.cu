@@ -763,6 +763,20 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         __syncthreads();
     }
+    if (out.dbg_cost != nullptr) {
+        for (int lb{tid}; lb < 64; lb += kThreads) {
+            const int lbx{lb & 7};
+            const int lby{lb >> 3};
+            if (bx0 + lbx < bw && by0 + lby < bh) {
+                const std::size_t at{static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx};
+                out.dbg_cost[at] = sm.cost8[lb];
+                out.dbg_cost[nblocks + at] =
+                    ((lbx | lby) & 1) == 0 ? sm.cost16[(lby >> 1) * 4 + (lbx >> 1)] : 0.0f;
+                out.dbg_cost[2 * static_cast<std::size_t>(nblocks) + at] =
+                    ((lbx | lby) & 3) == 0 ? sm.cost32[(lby >> 2) * 2 + (lbx >> 2)] : 0.0f;
+            }
+        }
+    }
     // 4d. RD decision per region (src/transform_select_impl.cuh:130-201).
     if (tid < 4) {
         const int ri{tid};

@@ -39,6 +39,7 @@ struct FrontendOutputs {
     float* dbg_xyb;       // [3][H][W] XYB before sharpening
     float* dbg_sharp;     // [3][H][W] XYB after inverse gaborish
     std::uint16_t* dbg_coeff;  // [3][B*64] FP16 bit patterns, covered-block layout
+    float* dbg_cost;      // [3][B] selection costs: DCT8, DCT16 at quad and DCT32 at region first blocks
 };
 
 struct FrontendInputs {

@@ -31,6 +31,10 @@ typedef struct cujpegxl_b200_planes {
     float* xyb;       /* [3][H][W] XYB before sharpening */
     float* sharp;     /* [3][H][W] XYB after inverse gaborish */
     uint16_t* coeff;  /* [3][B*64] FP16 DCT coefficients (bit patterns) */
+    float* cost;      /* [3][B] RD costs of the transform selection: DCT8 at every
+                       * block, DCT16 at the first block of every 16x16 quad and
+                       * DCT32 at the first block of every 32x32 region (0
+                       * elsewhere); only where the RD search ran */
 } cujpegxl_b200_planes;
 
 /* Enables (non-zero) or disables the float/FP16 stage dumps of the frontend.
@@ -175,7 +179,7 @@ void cujpegxl_b200_batch_destroy(cujpegxl_b200_batch* batch);
  * decisions only steer the encoder: the stream stays conformant and its
  * entropy coding exact.
  *
- * Weights blob (little-endian): "JXBN", uint32 version 1, uint32 parameter
+ * Weights blob (little-endian): "JXBN", uint32 version 2, uint32 parameter
  * count, uint32 channels 32, classes 17, K1 80, K 288, float32 scale[4] and
  * shift[4] (input normalisation of X, Y, B and log2 distance), float32
  * parameters[count], then the SHA-256 of every preceding byte. */
@@ -208,9 +212,12 @@ cujpegxl_status cujpegxl_b200_encoder_acsnet_stats(cujpegxl_encoder* encoder, ui
                                                    uint32_t* regions);
 
 /* Training. All pointers in a batch are device addresses; sample i uses tile
- * tiles[tile_index[i]] ([3][32][32] float X, Y, B planes) at log2 distance
+ * tiles[tile_index[i]] ([3][34][34] float X, Y, B planes: the region and a
+ * 1-pixel ring, clamped at the image border) at log2 distance
  * log2_distance[i], with labels label_class[i] (split class 0..16) and
- * label_qf[i][16] (log2 quant field of the blocks in raster order). */
+ * label_qf[i][16] (log2 quant field of the blocks in raster order).
+ * label_soft (may be NULL) replaces the one-hot target of the split by a
+ * distribution [n][17]; label_class then only feeds the accuracy statistic. */
 typedef struct cujpegxl_b200_acsnet_batch {
     const float* tiles;
     const int32_t* tile_index;
@@ -218,6 +225,7 @@ typedef struct cujpegxl_b200_acsnet_batch {
     const int8_t* label_class;
     const float* label_qf;
     uint32_t n;
+    const float* label_soft;
 } cujpegxl_b200_acsnet_batch;
 
 typedef struct cujpegxl_b200_acsnet_trainer cujpegxl_b200_acsnet_trainer;
@@ -234,9 +242,10 @@ cujpegxl_status cujpegxl_b200_acsnet_trainer_forward(cujpegxl_b200_acsnet_traine
                                                      const cujpegxl_b200_acsnet_batch* batch, float* out,
                                                      uintptr_t stream);
 
-/* Gradient of the batch-mean loss (cross-entropy of the split plus qf_weight
- * times the mean squared log2 quant-field error) into grad[param_count]
- * (device), without changing the parameters. stats[n][4] (device, may be
+/* Gradient of the batch-mean loss (cross-entropy of the split against its
+ * one-hot label or label_soft, plus qf_weight times the mean squared log2
+ * quant-field error) into grad[param_count] (device), without changing the
+ * parameters. stats[n][4] (device, may be
  * NULL): cross-entropy, quant-field squared error, 1 if the arg-max class is
  * the label, softmax margin. */
 cujpegxl_status cujpegxl_b200_acsnet_trainer_gradient(cujpegxl_b200_acsnet_trainer* trainer,

@@ -57,19 +57,19 @@ def biases(params: np.ndarray, layer: int) -> np.ndarray:
     return np.asarray(params[OFF_B + layer * C:OFF_B + (layer + 1) * C], np.float32).astype(np.float64)
 
 
-def im2col(x: np.ndarray, stride: int) -> np.ndarray:
-    """[H][W][Cin] -> [P][9 Cin], column = (ky * 3 + kx) * Cin + ci, zero padding 1."""
+def im2col(x: np.ndarray, stride: int, pad: int = 1) -> np.ndarray:
+    """[H][W][Cin] -> [P][9 Cin], column = (ky * 3 + kx) * Cin + ci, zero padding `pad`."""
     h, w, cn = x.shape
-    oh, ow = h // stride, w // stride
-    xp = np.zeros((h + 2, w + 2, cn), np.float64)
-    xp[1:-1, 1:-1] = x
+    oh, ow = (h + 2 * pad - 3) // stride + 1, (w + 2 * pad - 3) // stride + 1
+    xp = np.zeros((h + 2 * pad, w + 2 * pad, cn), np.float64)
+    xp[pad:pad + h, pad:pad + w] = x
     cols = [xp[ky:ky + stride * oh:stride, kx:kx + stride * ow:stride, :] for ky in range(3) for kx in range(3)]
     return np.concatenate(cols, axis=2).reshape(oh * ow, 9 * cn)
 
 
 def col2im(dcol: np.ndarray, h: int, stride: int, cn: int) -> np.ndarray:
-    """Adjoint of im2col: [P][9 Cin] -> [H][W][Cin]."""
-    oh = h // stride
+    """Adjoint of im2col with padding 1: [P][9 Cin] -> [H][W][Cin]."""
+    oh = (h - 1) // stride + 1
     d = dcol[:, :9 * cn].reshape(oh, oh, 9, cn)
     dxp = np.zeros((h + 2, h + 2, cn), np.float64)
     for ky in range(3):
@@ -83,21 +83,26 @@ def _r(v: np.ndarray, rnd: bool) -> np.ndarray:
 
 
 def net_input(norm: np.ndarray, tile: np.ndarray, log2d: float, rnd: bool = True) -> np.ndarray:
-    """[3][32][32] XYB tile -> [32][32][8] input (X, Y, B, log2 distance, zeros)."""
+    """[3][34][34] XYB tile (a region and its 1-pixel ring) -> [34][34][8]
+    input (X, Y, B, log2 distance, zeros)."""
     scale = np.asarray(norm[:4], np.float32)
     shift = np.asarray(norm[4:8], np.float32)
-    x = np.zeros((32, 32, NIN), np.float64)
+    x = np.zeros((34, 34, NIN), np.float64)
     for c in range(3):
         v = (np.asarray(tile[c], np.float32) - shift[c]) * scale[c] if rnd else \
             (np.asarray(tile[c], np.float64) - float(shift[c])) * float(scale[c])
         x[:, :, c] = _r(v, rnd)
     v = (np.float32(log2d) - shift[3]) * scale[3] if rnd else (float(log2d) - float(shift[3])) * float(scale[3])
-    x[:, :, 3] = _r(np.full((32, 32), v), rnd)
+    x[:, :, 3] = _r(np.full((34, 34), v), rnd)
     return x
 
 
-def _layer(x: np.ndarray, params: np.ndarray, layer: int, stride: int, relu: bool, rnd: bool):
-    a = im2col(x, stride)
+PADS = (0, 1, 1, 1)
+STRIDES = (2, 2, 2, 1)
+
+
+def _layer(x: np.ndarray, params: np.ndarray, layer: int, relu: bool, rnd: bool):
+    a = im2col(x, STRIDES[layer], PADS[layer])
     if a.shape[1] < KS[layer]:
         a = np.pad(a, ((0, 0), (0, KS[layer] - a.shape[1])))
     y = a @ weights(params, layer, rnd).T + biases(params, layer)
@@ -107,12 +112,12 @@ def _layer(x: np.ndarray, params: np.ndarray, layer: int, stride: int, relu: boo
 
 
 def forward(params: np.ndarray, norm: np.ndarray, tile: np.ndarray, log2d: float, rnd: bool = True) -> dict:
-    """Activations x1 [32,32,8], x2 [16,16,32], x3 [8,8,32], x4 [4,4,32] and out [16][32]."""
+    """Activations x1 [34,34,8], x2 [16,16,32], x3 [8,8,32], x4 [4,4,32] and out [16][32]."""
     x1 = net_input(norm, tile, log2d, rnd)
-    x2 = _layer(x1, params, 0, 2, True, rnd).reshape(16, 16, C)
-    x3 = _layer(x2, params, 1, 2, True, rnd).reshape(8, 8, C)
-    x4 = _layer(x3, params, 2, 2, True, rnd).reshape(4, 4, C)
-    out = _layer(x4, params, 3, 1, False, rnd)
+    x2 = _layer(x1, params, 0, True, rnd).reshape(16, 16, C)
+    x3 = _layer(x2, params, 1, True, rnd).reshape(8, 8, C)
+    x4 = _layer(x3, params, 2, True, rnd).reshape(4, 4, C)
+    out = _layer(x4, params, 3, False, rnd)
     return {"x1": x1, "x2": x2, "x3": x3, "x4": x4, "out": out}
 
 
@@ -140,8 +145,10 @@ def decide(out: np.ndarray, margin: float) -> tuple[int, np.ndarray]:
 
 
 def loss_and_grad(params: np.ndarray, norm: np.ndarray, tiles: np.ndarray, log2d: np.ndarray,
-                  labels: np.ndarray, label_qf: np.ndarray, qf_weight: float, rnd: bool = True):
-    """Mean loss over the batch, per-sample stats [n][4] and the gradient [NPARAMS]."""
+                  labels: np.ndarray, label_qf: np.ndarray, qf_weight: float, rnd: bool = True,
+                  soft: np.ndarray | None = None):
+    """Mean loss over the batch, per-sample stats [n][4] and the gradient
+    [NPARAMS]; `soft` [n][17] replaces the one-hot split targets."""
     n = len(tiles)
     grad = np.zeros(NPARAMS, np.float64)
     stats = np.zeros((n, 4), np.float64)
@@ -152,20 +159,20 @@ def loss_and_grad(params: np.ndarray, norm: np.ndarray, tiles: np.ndarray, log2d
         logits, qf = head(f["out"])
         prob, top, mg, lse = softmax_stats(logits)
         lab = int(labels[i])
-        ce = lse - logits[lab]
+        target = np.eye(NCLS)[lab] if soft is None else np.asarray(soft[i], np.float64)
+        ce = lse - float((target * logits).sum())
         d = qf - np.asarray(label_qf[i], np.float64)
         sq = float((d * d).sum())
         stats[i] = (ce, sq / 16.0, 1.0 if top == lab else 0.0, mg)
         total += ce + qf_weight * sq / 16.0
-        dlogit = (prob - np.eye(NCLS)[lab]) / n
+        dlogit = (prob - target) / n
         g = np.zeros((16, C), np.float64)
         g[:, 0] = 2.0 * qf_weight * d / n / 16.0
         g[:, 1:1 + NCLS] = dlogit[None, :] / 16.0
         g = _r(g, rnd)
         xs = [f["x1"], f["x2"], f["x3"], f["x4"]]
-        strides = (2, 2, 2, 1)
         for layer in (3, 2, 1, 0):
-            a = im2col(xs[layer], strides[layer])
+            a = im2col(xs[layer], STRIDES[layer], PADS[layer])
             if a.shape[1] < KS[layer]:
                 a = np.pad(a, ((0, 0), (0, KS[layer] - a.shape[1])))
             grad[OFF_W[layer]:OFF_W[layer] + C * KS[layer]] += (g.T @ a).reshape(-1)
@@ -173,7 +180,7 @@ def loss_and_grad(params: np.ndarray, norm: np.ndarray, tiles: np.ndarray, log2d
             if layer == 0:
                 break
             h = xs[layer].shape[0]
-            dx = col2im(g @ w[layer], h, strides[layer], C)
+            dx = col2im(g @ w[layer], h, STRIDES[layer], C)
             g = _r(np.where(xs[layer] > 0, dx, 0.0), rnd).reshape(h * h, C)
     return total / n, stats, grad
 

@@ -17,10 +17,10 @@ NORM = np.array([30.0, 4.0, 4.0, 1.0, 0.0, 0.4, 0.4, 0.5], np.float32)
 
 def _tiles(n: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
-    out = np.empty((n, 3, 32, 32), np.float32)
-    yy, xx = np.mgrid[0:32, 0:32] / 32.0
+    out = np.empty((n, 3, 34, 34), np.float32)
+    yy, xx = np.mgrid[0:34, 0:34] / 32.0
     for i in range(n):
-        tex = rng.normal(0, rng.uniform(0.002, 0.05), (32, 32))
+        tex = rng.normal(0, rng.uniform(0.002, 0.05), (34, 34))
         out[i, 0] = rng.normal(0, 0.01) + 0.2 * tex * rng.uniform(0, 1)
         out[i, 1] = 0.4 + 0.2 * (xx * rng.uniform(-1, 1) + yy * rng.uniform(-1, 1)) + tex
         out[i, 2] = out[i, 1] + rng.normal(0, 0.02)
@@ -105,7 +105,39 @@ def test_split_classes_match_oracle(w, h):
     assert np.array_equal(rq[1, 0], qf[4:8, 0:4].reshape(16))
     xyb = rng.normal(size=(3, h, w)).astype(np.float32)
     t = acsnet.region_tiles(xyb, w, h)
-    assert np.array_equal(t[(w // 32) + 1], xyb[:, 32:64, 32:64])
+    assert t.shape == ((h // 32) * (w // 32), 3, 34, 34)
+    assert np.array_equal(t[(w // 32) + 1], xyb[:, 31:65, 31:65])
+    # The ring is clamped to the image at its border.
+    assert np.array_equal(t[0][:, 1:, 1:], xyb[:, :33, :33])
+    assert np.array_equal(t[0][:, 0, 1:], xyb[:, 0, :33]) and np.array_equal(t[0][:, 1:, 0], xyb[:, :33, 0])
+
+
+def test_class_costs_argmin_is_the_rd_rule():
+    """The cheapest of the 17 split costs is the split the RD rule picks
+    (DCT16 over four DCT8 when not dearer, then DCT32 over the split)."""
+    w, h = 256, 192
+    bw, bh = w // 8, h // 8
+    rng = np.random.default_rng(4)
+    cost = np.zeros((3, bh, bw), np.float32)
+    cost[0] = rng.uniform(10, 20, (bh, bw))
+    cost[1][0::2, 0::2] = rng.uniform(25, 95, (bh // 2, bw // 2))
+    cost[2][0::4, 0::4] = rng.uniform(100, 330, (bh // 4, bw // 4))
+    cc = acsnet.class_costs(cost.reshape(-1), w, h)
+    for ry in range(h // 32):
+        for rx in range(w // 32):
+            split, m = 0.0, 0
+            for q in range(4):
+                by, bx = 4 * ry + 2 * (q >> 1), 4 * rx + 2 * (q & 1)
+                s8 = float(cost[0][by:by + 2, bx:bx + 2].sum())
+                c16 = float(cost[1][by, bx])
+                if c16 <= s8:
+                    split += c16
+                else:
+                    split += s8
+                    m |= 1 << q
+            want = 0 if cost[2][4 * ry, 4 * rx] <= split else 1 + m
+            assert int(np.argmin(cc[ry, rx])) == want
+            assert np.isclose(cc[ry, rx].min(), min(split, cost[2][4 * ry, 4 * rx]))
 
 
 def test_oracle_gradient_matches_finite_differences():

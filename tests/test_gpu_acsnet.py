@@ -19,10 +19,10 @@ NORM = np.array([30.0, 4.0, 4.0, 1.0, 0.0, 0.4, 0.4, 0.5], np.float32)
 
 def _tiles(n: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
-    out = np.empty((n, 3, 32, 32), np.float32)
-    yy, xx = np.mgrid[0:32, 0:32] / 32.0
+    out = np.empty((n, 3, 34, 34), np.float32)
+    yy, xx = np.mgrid[0:34, 0:34] / 32.0
     for i in range(n):
-        tex = rng.normal(0, rng.uniform(0.002, 0.05), (32, 32))
+        tex = rng.normal(0, rng.uniform(0.002, 0.05), (34, 34))
         out[i, 0] = rng.normal(0, 0.01) + 0.2 * tex * rng.uniform(0, 1)
         out[i, 1] = 0.4 + 0.2 * (xx * rng.uniform(-1, 1) + yy * rng.uniform(-1, 1)) + tex
         out[i, 2] = out[i, 1] + rng.normal(0, 0.02)
@@ -94,6 +94,39 @@ def test_gradient_matches_oracle():
     # Padding connections get exactly zero gradient.
     w1 = g[:orc.C * orc.K1].reshape(orc.C, orc.K1)
     assert np.all(w1[:, 72:] == 0) and np.all(w1[:, :72].reshape(orc.C, 9, 8)[:, :, 4:] == 0)
+
+
+def test_soft_target_gradient_matches_oracle():
+    """The same with soft split targets (a distribution over the 17 splits)."""
+    import torch
+    rng = np.random.default_rng(21)
+    p = _params(7)
+    tiles = _tiles(10, 5)
+    l2d = rng.uniform(-1, 2, 10)
+    lab = rng.integers(0, 17, 10)
+    lq = rng.uniform(1, 6, (10, 16))
+    soft = rng.dirichlet(np.full(17, 0.3), 10).astype(np.float32)
+    d = _dev(tiles, l2d, lab, lq)
+    with acsnet.Trainer(p, NORM, 16) as tr:
+        g, st = tr.gradient(d["tiles"], d["tile_index"], d["log2d"], d["label_class"], d["label_qf"], 0.3,
+                            label_soft=torch.from_numpy(soft).cuda())
+        g = g.cpu().numpy()
+        st = st.cpu().numpy()
+    _, ost, og = orc.loss_and_grad(p, NORM, tiles, l2d, lab, lq, 0.3, rnd=True, soft=soft)
+    for layer in range(4):
+        sl = slice(orc.OFF_W[layer], orc.OFF_W[layer] + orc.C * orc.KS[layer])
+        assert _rel(g[sl], og[sl]) < 3e-2, f"layer {layer + 1}"
+    assert np.allclose(st[:, 0], ost[:, 0], rtol=1e-2, atol=1e-3)
+
+
+def test_selection_costs_reproduce_the_heuristic():
+    """The selection-cost planes of a debug encode give, per full region, 17
+    split costs whose cheapest is the split the encode chose (ties aside)."""
+    w, h = 1920, 1080
+    _, planes, _ = _encode(make_nv12(w, h, 13), w, h, 1.0, debug=True)
+    got = np.argmin(acsnet.class_costs(planes["cost"], w, h), axis=-1)
+    want = acsnet.split_classes(planes["acs"], w, h)
+    assert np.mean(got == want) > 0.995
 
 
 def test_adam_step():
