@@ -338,6 +338,54 @@ def run_ours(args) -> None:
     e2e_ms = max_over_ranks(max(e0.elapsed_time(dn) for dn in dones), pg, "cuda")
     e2e = whole_job_rate((e2e_n // S) * S, world, e2e_ms)
 
+    # The same step with learned transform decisions (the shipped network at
+    # its default margin, split only): device-resident throughput, the
+    # frontend stage with the network's inference in front of it, and the
+    # share of regions the network decided.
+    from cujpegxl_b200.acsnet import DEFAULT_MARGIN, DEFAULT_WEIGHTS, SPLIT, AcsNet
+
+    net = AcsNet.load(device_ordinal=local)
+    for e in encs:
+        e.set_acsnet(net, DEFAULT_MARGIN, SPLIT)
+    for _ in range(args.warmup):
+        enqueue_step()
+    for e in encs:
+        e.result()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    l0 = torch.cuda.Event(enable_timing=True)
+    l1 = torch.cuda.Event(enable_timing=True)
+    l0.record(streams[0])
+    for st in streams[1:]:
+        st.wait_event(l0)
+    for _ in range(args.steps):
+        enqueue_step()
+    for ev, st in zip(joins[1:], streams[1:]):
+        ev.record(st)
+        streams[0].wait_event(ev)
+    l1.record(streams[0])
+    for e in encs:
+        e.result()
+    torch.cuda.synchronize()
+    learned_ms = max_over_ranks(l0.elapsed_time(l1), pg, "cuda")
+    lf = []
+    for lm, ch in frames:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 1)
+        b.record(stream)
+        lf.append((a, b))
+    enc.result()
+    torch.cuda.synchronize()
+    learned_front = statistics.mean(a.elapsed_time(b) for a, b in lf)
+    decided, regions = enc.acsnet_stats()
+    learned_data = enc.encode_device(frames[0][0].data_ptr(), frames[0][1].data_ptr(), W, W) if rank == 0 else b""
+    for e in encs:
+        e.set_acsnet(None)
+    net.close()
+
     front_ms = statistics.mean(front)
     alg = frontend_algorithmic_bytes(W, H)
     achieved = alg / (front_ms / 1000.0) / 1e9
@@ -392,6 +440,20 @@ def run_ours(args) -> None:
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        report = json.loads(DEFAULT_WEIGHTS.with_suffix(".json").read_text())
+        lq = psnr_y(nv12, learned_data)
+        line["learned"] = {
+            "fps": whole_job_rate(n, world, learned_ms), "unit": "frames/s", "frontend_ms": learned_front,
+            "decided_regions": decided, "regions": regions, "margin": DEFAULT_MARGIN,
+            "bpp": 8.0 * len(learned_data) / (W * H), "psnr_y_db": lq,
+            "bpp_delta_pct": 100.0 * (len(learned_data) / len(data) - 1.0),
+            "psnr_delta_db": lq - quality["psnr_y_db"],
+            "bpp_delta_at_equal_psnr_pct": {
+                f"{r['frame']} d={r['distance']}": round(r["bpp_delta_at_equal_psnr_pct"], 3)
+                for r in report["codec_split"]},
+            "basis": "same step with the shipped network attached (split decisions, margin 0.2); the "
+                     "equal-PSNR bpp changes are from the weights' training report (held-out frames)",
+        }
         print(json.dumps(line), flush=True)
     # Torch's allocators record events on the streams their blocks were used
     # on when they are freed, so release every torch object that touched the

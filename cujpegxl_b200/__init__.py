@@ -242,6 +242,13 @@ class Batch:
         check("batch_copy", self._L.cujpegxl_b200_batch_copy(self._h, index, ctypes.byref(out)))
         return buf[:out.size].tobytes()
 
+    def set_acsnet(self, net, margin: float = 0.2, flags: int = 1) -> None:
+        """Learned transform decisions for every frame (see Encoder.set_acsnet);
+        the next encode captures and tunes the graph again."""
+        check("batch_set_acsnet", self._L.cujpegxl_b200_batch_set_acsnet(
+            self._h, None if net is None else net.handle, margin, flags))
+        self._net = net
+
     @property
     def lanes(self) -> int:
         return int(self._L.cujpegxl_b200_batch_lanes(self._h))

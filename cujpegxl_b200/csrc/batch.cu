@@ -316,6 +316,28 @@ cujpegxl_status cujpegxl_b200_batch_copy(cujpegxl_b200_batch* batch, size_t inde
     return CUJPEGXL_OK;
 }
 
+cujpegxl_status cujpegxl_b200_batch_set_acsnet(cujpegxl_b200_batch* batch, const cujpegxl_b200_acsnet* net,
+                                               float margin, uint32_t flags) {
+    if (batch == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    DeviceScope scope{batch->device};
+    if (!scope.ok() || cudaStreamSynchronize(batch->root) != cudaSuccess) return CUJPEGXL_INTERNAL_ERROR;
+    for (cujpegxl_encoder* e : batch->encs) {
+        const cujpegxl_status st{cujpegxl_b200_encoder_set_acsnet(e, net, margin, flags)};
+        if (st != CUJPEGXL_OK) {
+            for (cujpegxl_encoder* u : batch->encs) cujpegxl_b200_encoder_set_acsnet(u, nullptr, 0.0f, 0u);
+            return st;
+        }
+    }
+    // The captured launch sequence changes: the next encode captures (and
+    // tunes) the graph again.
+    if (batch->exec != nullptr) {
+        cudaGraphExecDestroy(batch->exec);
+        batch->exec = nullptr;
+    }
+    batch->launched = false;
+    return CUJPEGXL_OK;
+}
+
 cujpegxl_status cujpegxl_b200_batch_stream(const cujpegxl_b200_batch* batch, uintptr_t* stream) {
     if (batch == nullptr || stream == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
     *stream = reinterpret_cast<uintptr_t>(batch->root);

@@ -110,7 +110,10 @@ class _Stream:
 
 
 class Server:
-    def __init__(self, device: int = 0, budget_bytes: float = 40e9, depth: int = 2):
+    def __init__(self, device: int = 0, budget_bytes: float = 40e9, depth: int = 2, net=None,
+                 margin: float = 0.2, net_flags: int = 1):
+        """net: an acsnet.AcsNet for learned transform decisions (owned by the
+        caller), attached to every encoder with `margin` and `net_flags`."""
         import torch
 
         from . import Encoder  # noqa: F401  (fails loudly if the library is missing)
@@ -119,6 +122,7 @@ class Server:
         self.device = device
         self.budget = Budget(int(budget_bytes))
         self.depth = depth
+        self.net, self.margin, self.net_flags = net, margin, net_flags
         self.streams: list[_Stream] = []
         torch.cuda.set_device(device)
 
@@ -134,6 +138,8 @@ class Server:
         try:
             for _ in range(self.depth):
                 enc = Encoder(w, h, spec.distance, self.device)
+                if self.net is not None:
+                    enc.set_acsnet(self.net, self.margin, self.net_flags)
                 dev_bytes, _ = enc.memory()
                 need = dev_bytes + w * h * 3 // 2
                 if not self.budget.reserve(need):
@@ -253,8 +259,13 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--depth", type=int, default=2)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--learned", action="store_true", help="learned transform decisions (shipped weights)")
     args = ap.parse_args()
-    srv = Server(args.device, args.budget_gb * 1e9, args.depth)
+    net = None
+    if args.learned:
+        from .acsnet import AcsNet
+        net = AcsNet.load(device_ordinal=args.device)
+    srv = Server(args.device, args.budget_gb * 1e9, args.depth, net)
     rejected = []
     for i, spec in enumerate(DEFAULT_STREAMS):
         try:
@@ -265,6 +276,8 @@ def main() -> None:
     result["rejected"] = rejected
     print(json.dumps(result), flush=True)
     srv.close()
+    if net is not None:
+        net.close()
 
 
 if __name__ == "__main__":

@@ -257,6 +257,12 @@ cujpegxl_status cujpegxl_b200_acsnet_trainer_step(cujpegxl_b200_acsnet_trainer* 
                                                   const cujpegxl_b200_acsnet_batch* batch, float qf_weight,
                                                   float learning_rate, float* stats, uintptr_t stream);
 
+/* Attaches `net` (NULL detaches) to every frame of a batch, as
+ * cujpegxl_b200_encoder_set_acsnet does; waits for the batch's last launch,
+ * and the next cujpegxl_b200_batch_encode captures and tunes its graph anew. */
+cujpegxl_status cujpegxl_b200_batch_set_acsnet(cujpegxl_b200_batch* batch, const cujpegxl_b200_acsnet* net,
+                                               float margin, uint32_t flags);
+
 /* Copies the FP32 parameters to params[param_count] (host); synchronous. */
 cujpegxl_status cujpegxl_b200_acsnet_trainer_params(cujpegxl_b200_acsnet_trainer* trainer, float* params);
 

@@ -52,3 +52,35 @@ def test_batch_matches_single_encoders_across_relaunch_and_rebinding():
         assert batch.lanes in (1, 2, 4, 8)
     w, h, d = FRAMES[2]
     assert expected_a[2] == api.encode(nvs_a[2], w, h, d)
+
+
+def test_batch_with_learned_decisions_matches_single_encoders():
+    """Attaching the network to a batch recaptures its graph; every frame then
+    equals the learned-decision file of one encoder, and detaching restores
+    the plain files."""
+    from cujpegxl_b200.acsnet import AcsNet
+    keep, inputs, nvs = _inputs(300)
+    net = AcsNet.load()
+    learned = []
+    for nv, (w, h, d) in zip(nvs, FRAMES):
+        k, luma, chroma, lp, cp = device_nv12(nv, w, h)
+        with Encoder(w, h, d) as enc:
+            enc.set_acsnet(net)
+            learned.append(enc.encode_device(luma, chroma, lp, cp))
+            enc.set_acsnet(None)
+    plain = [_single(nv, w, h, d) for nv, (w, h, d) in zip(nvs, FRAMES)]
+    assert learned != plain
+    with Batch(FRAMES) as batch:
+        batch.encode(inputs)
+        batch.sync()
+        assert [batch.read(i) for i in range(len(FRAMES))] == plain
+        batch.set_acsnet(net)
+        for _ in range(2):
+            batch.encode(inputs)
+            batch.sync()
+            assert [batch.read(i) for i in range(len(FRAMES))] == learned
+        batch.set_acsnet(None)
+        batch.encode(inputs)
+        batch.sync()
+        assert [batch.read(i) for i in range(len(FRAMES))] == plain
+    net.close()

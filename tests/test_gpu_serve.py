@@ -16,9 +16,14 @@ from .gpu_util import device_nv12
 pytestmark = pytest.mark.gpu
 
 
-def test_serving_loop_encodes_every_frame():
+@pytest.mark.parametrize("learned", [False, True])
+def test_serving_loop_encodes_every_frame(learned):
+    """With learned decisions too: every frame in the mix equals the file the
+    same network gives that frame alone."""
+    from cujpegxl_b200.acsnet import AcsNet
+    net = AcsNet.load() if learned else None
     specs = [StreamSpec("a", 512, 384, 120.0), StreamSpec("b", 264, 264, 200.0, 2.0)]
-    srv = Server(0, 8e9, depth=2)
+    srv = Server(0, 8e9, depth=2, net=net)
     try:
         for i, s in enumerate(specs):
             srv.admit(s, seed=i)
@@ -28,12 +33,19 @@ def test_serving_loop_encodes_every_frame():
             nv = make_nv12(s.width, s.height, i)
             keep, luma, chroma, lp, cp = device_nv12(nv, s.width, s.height)
             with Encoder(s.width, s.height, s.distance) as enc:
+                if net is not None:
+                    enc.set_acsnet(net)
                 size = len(enc.encode_device(luma, chroma, lp, cp))
+                if net is not None:
+                    assert enc.acsnet_stats()[0] > 0
+                enc.set_acsnet(None)
             st = r["streams"][s.name]
             assert st["frames"] > 0 and st["mean_bytes"] == size
             assert st["p99_ms"] >= st["p50_ms"] > 0
     finally:
         srv.close()
+        if net is not None:
+            net.close()
 
 
 def test_admission_refuses_what_does_not_fit():
