@@ -44,11 +44,16 @@ constexpr int kActS = 40;          // pixel stride of 32-channel activations
 
 // Weights and one region's activations. Row strides of 88/296/40 BF16 put the
 // eight rows of every ldmatrix on distinct bank groups (stride-1 access).
-struct NetSmem {
+struct NetWeights {
     bf16 w1[kNetC * kW1S];
     bf16 w[3][kNetC * kWS];
     float bias[4][kNetC];
     bf16 zero[8];
+};
+
+// Training: one region at a time.
+struct NetSmem {
+    NetWeights wt;
     bf16 x1[kNetInPix * kNetIn];
     bf16 x2[256 * kActS];
     bf16 x3[64 * kActS];
@@ -64,9 +69,24 @@ struct TrainSmem {
     bf16 g4[16 * kActS];
 };
 
-static_assert(sizeof(NetSmem) % 16 == 0 && sizeof(TrainSmem) % 16 == 0, "16-byte shared-memory layout");
-// Two inference CTAs per SM.
-static_assert(2 * (sizeof(NetSmem) + 1024) <= 228 * 1024, "inference CTA too large");
+// Inference: the four regions of a 64x64 tile side by side, one warp group
+// each. x1[r] also holds the region's later activations (x3, x4 and the FP32
+// outputs) once L1 has consumed it; x2 holds the tile's NV12 window until the
+// inputs are built.
+constexpr int kInferThreads = 512;
+constexpr int kX3Off = 0;                          // BF16 offsets inside x1[r]
+constexpr int kX4Off = kX3Off + 64 * kActS;
+constexpr int kOutOff = kX4Off + 16 * kActS;       // FP32 [16][32] from here
+struct InferSmem {
+    NetWeights wt;
+    bf16 x1[4][kNetInPix * kNetIn];
+    bf16 x2[4][256 * kActS];
+};
+
+static_assert(sizeof(NetWeights) % 16 == 0 && sizeof(NetSmem) % 16 == 0 && sizeof(TrainSmem) % 16 == 0,
+              "16-byte shared-memory layout");
+static_assert(2 * (kOutOff + 2 * 16 * kNetC) <= 2 * kNetInPix * kNetIn, "later activations exceed x1");
+static_assert(sizeof(InferSmem) + 1024 <= 228 * 1024, "inference CTA too large");
 
 __device__ __forceinline__ unsigned saddr(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -113,11 +133,20 @@ __device__ __forceinline__ void store_pair(bf16* dst, float lo, float hi) {
     *reinterpret_cast<__nv_bfloat162*>(dst) = __floats2bfloat162_rn(lo, hi);
 }
 
+// Stored column of image column x in a row of width kW. With kPar the even
+// columns come first, then the odd ones: the rows a stride-2 convolution
+// gathers for consecutive outputs are then adjacent in memory, and the eight
+// rows of an ldmatrix fall on distinct banks.
+template <int kW, bool kPar>
+__device__ __forceinline__ int par_col(int x) {
+    return kPar ? (x & 1) * ((kW + 1) >> 1) + (x >> 1) : x;
+}
+
 // Shared-memory address of im2col row p, reduction columns k0..k0+7, for a
 // 3x3 convolution with padding kPad over a kInW x kInW input of kCin channels
 // stored kInS apart, kOutW x kOutW outputs; the zero chunk where the tap is
 // padding (or a reduction column past the nine taps).
-template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS>
+template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS, bool kPar = false>
 __device__ __forceinline__ unsigned im2col_row(unsigned in, unsigned zero, int p, int k0) {
     const int tap{k0 / kCin};
     const int ci{k0 - tap * kCin};
@@ -126,56 +155,65 @@ __device__ __forceinline__ unsigned im2col_row(unsigned in, unsigned zero, int p
     const int iy{oy * kStride + tap / 3 - kPad};
     const int ix{ox * kStride + tap % 3 - kPad};
     const bool ok{tap < 9 && iy >= 0 && iy < kInW && ix >= 0 && ix < kInW};
-    return ok ? in + 2u * static_cast<unsigned>((iy * kInW + ix) * kInS + ci) : zero;
+    return ok ? in + 2u * static_cast<unsigned>((iy * kInW + par_col<kInW, kPar>(ix)) * kInS + ci) : zero;
 }
 
 // Forward of a layer with at least four 16-row position tiles (L1, L2): warp w
-// takes position tiles w, w+4, ... and all four 8-channel output tiles.
-template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS, int kK, int kWStr>
+// takes position tiles w, w+4, ... (two at a time, 32 accumulators) and all
+// four 8-channel output tiles.
+template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS, int kK, int kWStr, bool kParIn = false,
+          bool kParOut = false>
 __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* out,
                                          int warp, int lane) {
     constexpr int kMW{kOutW * kOutW / 64};
-    float acc[kMW][4][4];
+    constexpr int kChunk{kMW < 2 ? kMW : 2};
+#pragma unroll 1
+    for (int i0{0}; i0 < kMW; i0 += kChunk) {
+        float acc[kChunk][4][4];
 #pragma unroll
-    for (int i{0}; i < kMW; ++i) {
+        for (int i{0}; i < kChunk; ++i) {
 #pragma unroll
-        for (int n{0}; n < 4; ++n) {
+            for (int n{0}; n < 4; ++n) {
 #pragma unroll
-            for (int j{0}; j < 4; ++j) acc[i][n][j] = 0.0f;
+                for (int j{0}; j < 4; ++j) acc[i][n][j] = 0.0f;
+            }
         }
-    }
-#pragma unroll 2
-    for (int k0{0}; k0 < kK; k0 += 16) {
-        unsigned b[4][2];
+        // Fully unrolled: every tap and channel offset is a compile-time constant.
 #pragma unroll
-        for (int h{0}; h < 2; ++h) {
-            unsigned r[4];
-            ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kWStr + k0 +
-                                                      ((lane >> 3) & 1) * 8));
-            b[2 * h][0] = r[0];
-            b[2 * h][1] = r[1];
-            b[2 * h + 1][0] = r[2];
-            b[2 * h + 1][1] = r[3];
+        for (int k0{0}; k0 < kK; k0 += 16) {
+            unsigned b[4][2];
+#pragma unroll
+            for (int h{0}; h < 2; ++h) {
+                unsigned r[4];
+                ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kWStr + k0 +
+                                                          ((lane >> 3) & 1) * 8));
+                b[2 * h][0] = r[0];
+                b[2 * h][1] = r[1];
+                b[2 * h + 1][0] = r[2];
+                b[2 * h + 1][1] = r[3];
+            }
+#pragma unroll
+            for (int i{0}; i < kChunk; ++i) {
+                unsigned a[4];
+                ldsm_x4(a, im2col_row<kInW, kOutW, kStride, kPad, kCin, kInS, kParIn>(
+                               in, zero, (warp + 4 * (i0 + i)) * 16 + (lane & 15), k0 + (lane >> 4) * 8));
+#pragma unroll
+                for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
+            }
         }
 #pragma unroll
-        for (int i{0}; i < kMW; ++i) {
-            unsigned a[4];
-            ldsm_x4(a, im2col_row<kInW, kOutW, kStride, kPad, kCin, kInS>(in, zero, (warp + 4 * i) * 16 + (lane & 15),
-                                                                          k0 + (lane >> 4) * 8));
+        for (int i{0}; i < kChunk; ++i) {
+            const int p{(warp + 4 * (i0 + i)) * 16 + (lane >> 2)};
+            const int s0{(p / kOutW) * kOutW + par_col<kOutW, kParOut>(p % kOutW)};
+            const int s1{((p + 8) / kOutW) * kOutW + par_col<kOutW, kParOut>((p + 8) % kOutW)};
 #pragma unroll
-            for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
-        }
-    }
-#pragma unroll
-    for (int i{0}; i < kMW; ++i) {
-        const int p{(warp + 4 * i) * 16 + (lane >> 2)};
-#pragma unroll
-        for (int n{0}; n < 4; ++n) {
-            const int c{n * 8 + 2 * (lane & 3)};
-            const float b0{bias[c]};
-            const float b1{bias[c + 1]};
-            store_pair(out + p * kActS + c, fmaxf(acc[i][n][0] + b0, 0.0f), fmaxf(acc[i][n][1] + b1, 0.0f));
-            store_pair(out + (p + 8) * kActS + c, fmaxf(acc[i][n][2] + b0, 0.0f), fmaxf(acc[i][n][3] + b1, 0.0f));
+            for (int n{0}; n < 4; ++n) {
+                const int c{n * 8 + 2 * (lane & 3)};
+                const float b0{bias[c]};
+                const float b1{bias[c + 1]};
+                store_pair(out + s0 * kActS + c, fmaxf(acc[i][n][0] + b0, 0.0f), fmaxf(acc[i][n][1] + b1, 0.0f));
+                store_pair(out + s1 * kActS + c, fmaxf(acc[i][n][2] + b0, 0.0f), fmaxf(acc[i][n][3] + b1, 0.0f));
+            }
         }
     }
 }
@@ -185,21 +223,23 @@ __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w,
 template <int kInW, int kStride, bool kRelu>
 __device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* outb,
                                          float* outf, int warp, int lane) {
-    float acc[4]{0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 3
+    // Two accumulators over alternate reduction steps halve the dependent
+    // chain of tensor-core operations.
+    float acc[2][4]{{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
+#pragma unroll
     for (int k0{0}; k0 < kNetK; k0 += 16) {
         unsigned a[4];
         ldsm_x4(a, im2col_row<kInW, 4, kStride, 1, kNetC, kActS>(in, zero, lane & 15, k0 + (lane >> 4) * 8));
         unsigned b[2];
         ldsm_x2(b, w + 2u * static_cast<unsigned>((8 * warp + (lane & 7)) * kWS + k0 + ((lane >> 3) & 1) * 8));
-        mma(acc, a, b[0], b[1]);
+        mma(acc[(k0 >> 4) & 1], a, b[0], b[1]);
     }
     const int p{lane >> 2};
     const int c{8 * warp + 2 * (lane & 3)};
-    const float v0{acc[0] + bias[c]};
-    const float v1{acc[1] + bias[c + 1]};
-    const float v2{acc[2] + bias[c]};
-    const float v3{acc[3] + bias[c + 1]};
+    const float v0{(acc[0][0] + acc[1][0]) + bias[c]};
+    const float v1{(acc[0][1] + acc[1][1]) + bias[c + 1]};
+    const float v2{(acc[0][2] + acc[1][2]) + bias[c]};
+    const float v3{(acc[0][3] + acc[1][3]) + bias[c + 1]};
     if (kRelu) {
         store_pair(outb + p * kActS + c, fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
         store_pair(outb + (p + 8) * kActS + c, fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
@@ -321,7 +361,7 @@ __device__ __forceinline__ void bwd_s2(unsigned gout, unsigned zero, unsigned w,
 }
 
 // Copies the weights into shared memory (rows padded to kW1S / kWS).
-__device__ void load_net(NetSmem& s, const NetParamsDev& p, int tid, int nthreads) {
+__device__ void load_net(NetWeights& s, const NetParamsDev& p, int tid, int nthreads) {
     const uint4* g{reinterpret_cast<const uint4*>(p.w)};
     for (int i{tid}; i < kNetC * (kNetK1 / 8); i += nthreads) {
         const int r{i / (kNetK1 / 8)};
@@ -358,16 +398,22 @@ __device__ __forceinline__ uint4 input_pixel(const NetParamsDev& p, float x, flo
 }
 
 // The four layers over the region in s.x1; ends with s.out filled.
-__device__ __forceinline__ void net_forward(NetSmem& s, int warp, int lane) {
-    const unsigned zero{saddr(s.zero)};
-    fwd_rows<kNetInW, 16, 2, 0, kNetIn, kNetIn, kNetK1, kW1S>(saddr(s.x1), zero, saddr(s.w1), s.bias[0], s.x2, warp,
-                                                            lane);
+// warp: the warp's index (0..3) within the group of four warps that owns the
+// region; every thread of the CTA calls this together.
+// kPar: x1 and x2 are stored with their columns parity-split (par_col).
+template <bool kPar = false>
+__device__ __forceinline__ void net_forward(const NetWeights& wt, bf16* x1, bf16* x2, bf16* x3, bf16* x4,
+                                            float* out, int warp, int lane) {
+    const unsigned zero{saddr(wt.zero)};
+    fwd_rows<kNetInW, 16, 2, 0, kNetIn, kNetIn, kNetK1, kW1S, kPar, kPar>(saddr(x1), zero, saddr(wt.w1), wt.bias[0],
+                                                                        x2, warp, lane);
     __syncthreads();
-    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS>(saddr(s.x2), zero, saddr(s.w[0]), s.bias[1], s.x3, warp, lane);
+    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS, kPar, false>(saddr(x2), zero, saddr(wt.w[0]), wt.bias[1], x3,
+                                                                 warp, lane);
     __syncthreads();
-    fwd_cols<8, 2, true>(saddr(s.x3), zero, saddr(s.w[1]), s.bias[2], s.x4, nullptr, warp, lane);
+    fwd_cols<8, 2, true>(saddr(x3), zero, saddr(wt.w[1]), wt.bias[2], x4, nullptr, warp, lane);
     __syncthreads();
-    fwd_cols<4, 1, false>(saddr(s.x4), zero, saddr(s.w[2]), s.bias[3], nullptr, s.out, warp, lane);
+    fwd_cols<4, 1, false>(saddr(x4), zero, saddr(wt.w[2]), wt.bias[3], nullptr, out, warp, lane);
     __syncthreads();
 }
 
@@ -422,17 +468,77 @@ __device__ __forceinline__ SplitHead split_head(float logit) {
 
 // ---- Inference inside an encode ----
 
-constexpr int kRegionWin = 16 + 4;  // chroma window of one 32x32 region (2-sample margins)
+// The network's input pixel: xyb_pixel's NV12 -> XYB conversion with the two
+// transfer functions taken from the hardware base-2 exponential and
+// logarithm (x^2.4 = 2^(2.4 log2 x), cbrt x = 2^(log2 x / 3)) instead of the
+// frontend's correctly rounded ones. The values differ from the frontend's
+// by about 1e-6 relative, far below the BF16 rounding of the input (4e-3),
+// and cost a fraction of the instructions.
+__device__ __forceinline__ float hw_exp2(float x) {
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
-__global__ void __launch_bounds__(kNetThreads, 2)
+__device__ __forceinline__ float hw_log2(float x) {
+    float y;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+template <int kWin>
+__device__ __forceinline__ void net_xyb_pixel(int luma, const std::uint8_t* win, int cx0, int cy0, int gx, int gy,
+                                              int width, int height, float& ox, float& oy, float& ob) {
+    const float yv{static_cast<float>(luma) * kInv255};
+    const int jx{gx >> 1};
+    const int jy{gy >> 1};
+    const int xa{(gx & 1) ? jx : max(jx - 1, 0)};
+    const int xb{(gx & 1) ? min(jx + 1, (width >> 1) - 1) : jx};
+    const int ya{(gy & 1) ? jy : max(jy - 1, 0)};
+    const int yb{(gy & 1) ? min(jy + 1, (height >> 1) - 1) : jy};
+    const int wxa{(gx & 1) ? 3 : 1};
+    const int wya{(gy & 1) ? 3 : 1};
+    const int aa{2 * ((ya - cy0) * kWin + xa - cx0)};
+    const int ab{2 * ((ya - cy0) * kWin + xb - cx0)};
+    const int ba{2 * ((yb - cy0) * kWin + xa - cx0)};
+    const int bb{2 * ((yb - cy0) * kWin + xb - cx0)};
+    const int scb{wya * (wxa * win[aa] + (4 - wxa) * win[ab]) + (4 - wya) * (wxa * win[ba] + (4 - wxa) * win[bb])};
+    const int scr{wya * (wxa * win[aa + 1] + (4 - wxa) * win[ab + 1]) +
+                  (4 - wya) * (wxa * win[ba + 1] + (4 - wxa) * win[bb + 1])};
+    const float cb{static_cast<float>(scb) * (1.0f / 4080.0f) - kChromaCenter};
+    const float cr{static_cast<float>(scr) * (1.0f / 4080.0f) - kChromaCenter};
+    auto lin = [](float e) {
+        e = clamp01(e);
+        return clamp01(e <= 0.04045f ? e * (1.0f / 12.92f) : hw_exp2(2.4f * hw_log2((e + 0.055f) * (1.0f / 1.055f))));
+    };
+    const float r{lin(kCrToR * cr + yv)};
+    const float g{lin(yv - kCbToG * cb - kCrToG * cr)};
+    const float b{lin(kCbToB * cb + yv)};
+    auto cbrt_pos = [](float v) { return v > 0.0f ? hw_exp2(hw_log2(v) * (1.0f / 3.0f)) : 0.0f; };
+    const float m0{cbrt_pos(kM00 * r + kM01 * g + kM02 * b + kOpsinBias) + kNegCbrtBias};
+    const float m1{cbrt_pos(kM10 * r + kM11 * g + kM12 * b + kOpsinBias) + kNegCbrtBias};
+    const float m2{cbrt_pos(kM20 * r + kM21 * g + kM22 * b + kOpsinBias) + kNegCbrtBias};
+    ox = 0.5f * (m0 - m1);
+    oy = 0.5f * (m0 + m1);
+    ob = m2;
+}
+
+constexpr int kTileWin = kNetInW + 32;     // luma window of a 64x64 tile and its 1-pixel ring
+constexpr int kTileChroma = 32 + 4;        // chroma window of the tile (2-sample margins)
+
+// One CTA per SM walks the frame's 64x64 tiles; its four warp groups each
+// take one of the tile's four regions through the network in lockstep (one
+// barrier per layer for all four). The weights are loaded once per CTA.
+__global__ void __launch_bounds__(kInferThreads, 1)
     acsnet_infer_kernel(FrontendInputs in, NetParamsDev p, float log2_distance, float margin,
                         NetDecisionsDev out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    NetSmem& s{*reinterpret_cast<NetSmem*>(smem_raw)};
+    InferSmem& s{*reinterpret_cast<InferSmem*>(smem_raw)};
     const int tid{static_cast<int>(threadIdx.x)};
     const int warp{tid >> 5};
     const int lane{tid & 31};
-    load_net(s, p, tid, kNetThreads);
+    const int grp{warp >> 2};
+    load_net(s.wt, p, tid, kInferThreads);
     const int W{in.width};
     const int H{in.height};
     const int bw{W >> 3};
@@ -441,56 +547,102 @@ __global__ void __launch_bounds__(kNetThreads, 2)
     const int tw{(W + 63) >> 6};
     const int ntiles{tw * ((H + 63) >> 6)};
     std::uint8_t* win_luma{reinterpret_cast<std::uint8_t*>(s.x2)};
-    std::uint8_t* win_chroma{win_luma + kNetInPix + 12};
-    for (int t{static_cast<int>(blockIdx.x)}; t < ntiles; t += static_cast<int>(gridDim.x)) {
-#pragma unroll 1
-        for (int ri{0}; ri < 4; ++ri) {
-            const int rx{2 * (t % tw) + (ri & 1)};
-            const int ry{2 * (t / tw) + (ri >> 1)};
-            if (rx >= rw || ry >= rh) continue;  // block-uniform
-            const int px0{rx * 32};
-            const int py0{ry * 32};
-            if (px0 + 32 > W || py0 + 32 > H) {
-                if (tid == 0) out.cls[ry * rw + rx] = -1;
-                continue;
+    std::uint8_t* win_chroma{win_luma + kTileWin * kTileWin + 4};
+    bf16* x1{s.x1[grp]};
+    float* o{reinterpret_cast<float*>(x1 + kOutOff)};
+    // The NV12 window of the next tile is loaded into registers while the
+    // current one runs through the network, then stored to shared memory.
+    constexpr int kLumaPer{(kTileWin * kTileWin + kInferThreads - 1) / kInferThreads};
+    constexpr int kChromaPer{(kTileChroma * kTileChroma + kInferThreads - 1) / kInferThreads};
+    unsigned pl[kLumaPer];
+    unsigned pc[kChromaPer];
+    auto fetch = [&](int t) {
+        const int px0{(t % tw) * 64};
+        const int py0{(t / tw) * 64};
+        const int cx0{(px0 >> 1) - 2};
+        const int cy0{(py0 >> 1) - 2};
+#pragma unroll
+        for (int j{0}; j < kLumaPer; ++j) {
+            const int i{tid + j * kInferThreads};
+            if (i < kTileWin * kTileWin) {
+                const int gx{min(max(px0 - 1 + i % kTileWin, 0), W - 1)};
+                const int gy{min(max(py0 - 1 + i / kTileWin, 0), H - 1)};
+                pl[j] = __ldg(in.luma + static_cast<std::size_t>(gy) * in.luma_pitch + gx);
             }
-            __syncthreads();  // the previous region is done with x2 and out
+        }
+#pragma unroll
+        for (int j{0}; j < kChromaPer; ++j) {
+            const int i{tid + j * kInferThreads};
+            if (i < kTileChroma * kTileChroma) {
+                const int jx{min(max(cx0 + i % kTileChroma, 0), (W >> 1) - 1)};
+                const int jy{min(max(cy0 + i / kTileChroma, 0), (H >> 1) - 1)};
+                const std::uint8_t* c{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
+                pc[j] = __ldg(c) | (static_cast<unsigned>(__ldg(c + 1)) << 8);
+            }
+        }
+    };
+    if (static_cast<int>(blockIdx.x) < ntiles) fetch(static_cast<int>(blockIdx.x));
+    for (int t{static_cast<int>(blockIdx.x)}; t < ntiles; t += static_cast<int>(gridDim.x)) {
+        const int px0{(t % tw) * 64};
+        const int py0{(t / tw) * 64};
+        unsigned full{0};  // regions of the tile that are a full 32x32 inside the image
+#pragma unroll
+        for (int r{0}; r < 4; ++r) {
+            full |= (px0 + 32 * (r & 1) + 32 <= W && py0 + 32 * (r >> 1) + 32 <= H ? 1u : 0u) << r;
+        }
+        __syncthreads();  // the previous tile is done with the window and the outputs
+#pragma unroll
+        for (int j{0}; j < kLumaPer; ++j) {
+            const int i{tid + j * kInferThreads};
+            if (i < kTileWin * kTileWin) win_luma[i] = static_cast<std::uint8_t>(pl[j]);
+        }
+#pragma unroll
+        for (int j{0}; j < kChromaPer; ++j) {
+            const int i{tid + j * kInferThreads};
+            if (i < kTileChroma * kTileChroma) {
+                win_chroma[2 * i] = static_cast<std::uint8_t>(pc[j]);
+                win_chroma[2 * i + 1] = static_cast<std::uint8_t>(pc[j] >> 8);
+            }
+        }
+        __syncthreads();
+        if (t + static_cast<int>(gridDim.x) < ntiles) fetch(t + static_cast<int>(gridDim.x));
+        if (full != 0) {   // block-uniform
             const int cx0{(px0 >> 1) - 2};
             const int cy0{(py0 >> 1) - 2};
-            // Luma of the region and its 1-pixel ring, at clamped coordinates.
-            for (int i{tid}; i < kNetInPix; i += kNetThreads) {
-                const int gx{min(max(px0 - 1 + i % kNetInW, 0), W - 1)};
-                const int gy{min(max(py0 - 1 + i / kNetInW, 0), H - 1)};
-                win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
-            }
-            for (int i{tid}; i < kRegionWin * kRegionWin; i += kNetThreads) {
-                const int jx{min(max(cx0 + i % kRegionWin, 0), (W >> 1) - 1)};
-                const int jy{min(max(cy0 + i / kRegionWin, 0), (H >> 1) - 1)};
-                const std::uint8_t* c{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
-                win_chroma[2 * i] = c[0];
-                win_chroma[2 * i + 1] = c[1];
-            }
-            __syncthreads();
-            for (int i{tid}; i < kNetInPix; i += kNetThreads) {
-                const int gx{min(max(px0 - 1 + i % kNetInW, 0), W - 1)};
-                const int gy{min(max(py0 - 1 + i / kNetInW, 0), H - 1)};
+            for (int i{tid}; i < 4 * kNetInPix; i += kInferThreads) {
+                const int r{i / kNetInPix};
+                if (((full >> r) & 1u) == 0) continue;
+                const int k{i - r * kNetInPix};
+                const int wy{32 * (r >> 1) + k / kNetInW};
+                const int wx{32 * (r & 1) + k % kNetInW};
+                const int gx{min(max(px0 - 1 + wx, 0), W - 1)};
+                const int gy{min(max(py0 - 1 + wy, 0), H - 1)};
                 float x, y, b;
-                xyb_pixel<kRegionWin>(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
-                *reinterpret_cast<uint4*>(&s.x1[i * kNetIn]) = input_pixel(p, x, y, b, log2_distance);
+                net_xyb_pixel<kTileChroma>(win_luma[wy * kTileWin + wx], win_chroma, cx0, cy0, gx, gy, W, H, x, y,
+                                           b);
+                const int at{(k / kNetInW) * kNetInW + par_col<kNetInW, true>(k % kNetInW)};
+                *reinterpret_cast<uint4*>(&s.x1[r][at * kNetIn]) = input_pixel(p, x, y, b, log2_distance);
             }
             __syncthreads();
-            net_forward(s, warp, lane);
-            if (warp == 0) {
-                const SplitHead h{split_head(split_logit(s.out, lane))};
-                const int cls{h.margin >= margin ? h.top : -1};
+            // Groups of regions outside the image run on stale data and
+            // their results are dropped.
+            net_forward<true>(s.wt, x1, s.x2[grp], x1 + kX3Off, x1 + kX4Off, o, warp & 3, lane);
+        }
+        if ((warp & 3) == 0) {
+            const int rx{2 * (t % tw) + (grp & 1)};
+            const int ry{2 * (t / tw) + (grp >> 1)};
+            if (rx < rw && ry < rh) {
+                int cls{-1};
+                if (((full >> grp) & 1u) != 0) {
+                    const SplitHead h{split_head(split_logit(o, lane))};
+                    cls = h.margin >= margin ? h.top : -1;
+                }
                 if (lane == 0) out.cls[ry * rw + rx] = static_cast<std::int8_t>(cls);
                 if (cls >= 0 && out.qf != nullptr && lane < 16) {
                     // fmaxf maps a NaN to 1.
-                    const float q{fminf(fmaxf(rintf(exp2f(s.out[lane * kNetC])), 1.0f),
-                                        static_cast<float>(kQuantMax))};
-                    const int qi{static_cast<int>(q)};
+                    const float q{fminf(fmaxf(rintf(exp2f(o[lane * kNetC])), 1.0f), static_cast<float>(kQuantMax))};
                     out.qf[static_cast<std::size_t>(ry * 4 + (lane >> 2)) * bw + rx * 4 + (lane & 3)] =
-                        static_cast<std::int16_t>(qi);
+                        static_cast<std::int16_t>(static_cast<int>(q));
                 }
             }
         }
@@ -511,8 +663,8 @@ __global__ void __launch_bounds__(kNetThreads)
     const int tid{static_cast<int>(threadIdx.x)};
     const int warp{tid >> 5};
     const int lane{tid & 31};
-    load_net(s, p, tid, kNetThreads);
-    const unsigned zero{saddr(s.zero)};
+    load_net(s.wt, p, tid, kNetThreads);
+    const unsigned zero{saddr(s.wt.zero)};
     for (std::uint32_t i{blockIdx.x}; i < b.n; i += gridDim.x) {
         __syncthreads();
         const float* tile{b.tiles + static_cast<std::size_t>(b.tile_index[i]) * 3 * kNetInPix};
@@ -522,7 +674,7 @@ __global__ void __launch_bounds__(kNetThreads)
                 input_pixel(p, tile[px], tile[kNetInPix + px], tile[2 * kNetInPix + px], l2d);
         }
         __syncthreads();
-        net_forward(s, warp, lane);
+        net_forward(s.wt, s.x1, s.x2, s.x3, s.x4, s.out, warp, lane);
         if (outv != nullptr && warp == 0) {
             float* o{outv + static_cast<std::size_t>(i) * kNetOut};
             const float lg{split_logit(s.out, lane)};
@@ -562,11 +714,11 @@ __global__ void __launch_bounds__(kNetThreads)
             }
         }
         __syncthreads();
-        bwd_l4(saddr(ts.g4), zero, saddr(s.w[2]), s.x4, ts.g3, warp, lane);
+        bwd_l4(saddr(ts.g4), zero, saddr(s.wt.w[2]), s.x4, ts.g3, warp, lane);
         __syncthreads();
-        bwd_s2<8>(saddr(ts.g3), zero, saddr(s.w[1]), s.x3, ts.g2, warp, lane);
+        bwd_s2<8>(saddr(ts.g3), zero, saddr(s.wt.w[1]), s.x3, ts.g2, warp, lane);
         __syncthreads();
-        bwd_s2<16>(saddr(ts.g2), zero, saddr(s.w[0]), s.x2, ts.g1, warp, lane);
+        bwd_s2<16>(saddr(ts.g2), zero, saddr(s.wt.w[0]), s.x2, ts.g1, warp, lane);
         __syncthreads();
         // Compact copies for the weight-gradient kernel (8 BF16 per uint4).
         bf16* a{act + static_cast<std::size_t>(i) * kNetActPerSample};
@@ -743,7 +895,7 @@ int sm_count() {
 
 bool acsnet_kernels_init() {
     return cudaFuncSetAttribute(acsnet_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(NetSmem))) == cudaSuccess &&
+                                static_cast<int>(sizeof(InferSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(acsnet_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(TrainSmem))) == cudaSuccess;
 }
@@ -751,8 +903,8 @@ bool acsnet_kernels_init() {
 bool acsnet_infer_launch(const FrontendInputs& in, const NetParamsDev& p, float log2_distance, float margin,
                          const NetDecisionsDev& out, void* stream) {
     const int ntiles{((in.width + 63) >> 6) * ((in.height + 63) >> 6)};
-    const int grid{ntiles < 2 * sm_count() ? ntiles : 2 * sm_count()};
-    acsnet_infer_kernel<<<grid, kNetThreads, sizeof(NetSmem), static_cast<cudaStream_t>(stream)>>>(
+    const int grid{ntiles < sm_count() ? ntiles : sm_count()};
+    acsnet_infer_kernel<<<grid, kInferThreads, sizeof(InferSmem), static_cast<cudaStream_t>(stream)>>>(
         in, p, log2_distance, margin, out);
     return cudaGetLastError() == cudaSuccess;
 }
