@@ -42,23 +42,32 @@ def query_backend(device_ordinal: int = 0) -> str:
     return L.cujpegxl_backend_string(out.value).decode()
 
 
-def max_output_size(width: int, height: int, distance: float = 1.0, device_ordinal: int = 0) -> int:
+SINGLE_GROUP = 1  # CUJPEGXL_B200_ENCODER_SINGLE_GROUP
+
+
+def max_output_size(width: int, height: int, distance: float = 1.0, device_ordinal: int = 0,
+                    flags: int = 0) -> int:
     cfg = _capi.Config(width, height, distance, device_ordinal)
     out = ctypes.c_size_t(0)
-    check("max_output_size", _capi.lib().cujpegxl_max_output_size(ctypes.byref(cfg), ctypes.byref(out)))
+    check("max_output_size", _capi.lib().cujpegxl_b200_max_output_size_ex(ctypes.byref(cfg), flags,
+                                                                          ctypes.byref(out)))
     return out.value
 
 
 class Encoder:
-    """One encoder handle (cujpegxl_encoder_create ... _destroy)."""
+    """One encoder handle (cujpegxl_encoder_create ... _destroy).
+    flags=SINGLE_GROUP also accepts frames of one 256x256 AC group
+    (cujpegxl_b200_encoder_create_ex)."""
 
-    def __init__(self, width: int, height: int, distance: float = 1.0, device_ordinal: int = 0):
+    def __init__(self, width: int, height: int, distance: float = 1.0, device_ordinal: int = 0, flags: int = 0):
         self._L = _capi.lib()
         self._h = ctypes.c_void_p(None)
         cfg = _capi.Config(width, height, distance, device_ordinal)
-        check("encoder_create", self._L.cujpegxl_encoder_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        check("encoder_create", self._L.cujpegxl_b200_encoder_create_ex(ctypes.byref(cfg), flags,
+                                                                        ctypes.byref(self._h)))
         self.width, self.height, self.distance, self.device_ordinal = width, height, distance, device_ordinal
-        self._buf = np.zeros(max_output_size(width, height, distance, device_ordinal), np.uint8)
+        self.flags = flags
+        self._buf = np.zeros(max_output_size(width, height, distance, device_ordinal, flags), np.uint8)
         self._net = None
 
     def close(self) -> None:
@@ -87,7 +96,7 @@ class Encoder:
         cfg = _capi.Config(width, height, distance, dev)
         check("encoder_configure", self._L.cujpegxl_encoder_configure(self._h, ctypes.byref(cfg)))
         self.width, self.height, self.distance, self.device_ordinal = width, height, distance, dev
-        self._buf = np.zeros(max_output_size(width, height, distance, dev), np.uint8)
+        self._buf = np.zeros(max_output_size(width, height, distance, dev, self.flags), np.uint8)
 
     def _output(self, capacity: int | None = None) -> _capi.Output:
         cap = self._buf.size if capacity is None else capacity

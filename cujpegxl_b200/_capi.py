@@ -37,6 +37,7 @@ EXPORTS = (
     "cujpegxl_b200_acsnet_trainer_create", "cujpegxl_b200_acsnet_trainer_destroy",
     "cujpegxl_b200_acsnet_trainer_forward", "cujpegxl_b200_acsnet_trainer_gradient",
     "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params", "cujpegxl_b200_batch_set_acsnet",
+    "cujpegxl_b200_encoder_create_ex", "cujpegxl_b200_max_output_size_ex",
 )
 
 
@@ -135,6 +136,8 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_acsnet_trainer_step.argtypes = [E, P(NetBatch), F, F, ctypes.c_size_t, ctypes.c_size_t]
     L.cujpegxl_b200_acsnet_trainer_params.argtypes = [E, ctypes.c_void_p]
     L.cujpegxl_b200_batch_set_acsnet.argtypes = [E, E, F, ctypes.c_uint32]
+    L.cujpegxl_b200_encoder_create_ex.argtypes = [P(Config), ctypes.c_uint32, P(E)]
+    L.cujpegxl_b200_max_output_size_ex.argtypes = [P(Config), ctypes.c_uint32, P(ctypes.c_size_t)]
     for name in ("cujpegxl_query_backend", "cujpegxl_max_output_size", "cujpegxl_encoder_create",
                  "cujpegxl_encoder_configure", "cujpegxl_encoder_encode", "cujpegxl_b200_encoder_set_debug",
                  "cujpegxl_b200_encoder_read_planes", "cujpegxl_b200_encode_planes",
@@ -146,7 +149,8 @@ def lib() -> ctypes.CDLL:
                  "cujpegxl_b200_encoder_acsnet_stats", "cujpegxl_b200_acsnet_trainer_create",
                  "cujpegxl_b200_acsnet_trainer_forward", "cujpegxl_b200_acsnet_trainer_gradient",
                  "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params",
-                 "cujpegxl_b200_batch_set_acsnet"):
+                 "cujpegxl_b200_batch_set_acsnet", "cujpegxl_b200_encoder_create_ex",
+                 "cujpegxl_b200_max_output_size_ex"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

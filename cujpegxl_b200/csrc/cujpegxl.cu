@@ -55,6 +55,7 @@ struct cujpegxl_encoder {
     std::uint32_t net_flags{0};
     std::int8_t* net_class{nullptr};
     std::int16_t* net_qf{nullptr};
+    bool allow_single{false};  // created with CUJPEGXL_B200_ENCODER_SINGLE_GROUP
 };
 
 namespace {
@@ -107,13 +108,15 @@ bool device_exists(std::int32_t ordinal, int* major, int* minor) {
 
 // src/cujpegxl.cc:36-48: distance must be positive and finite; width and
 // height positive multiples of 8 spanning more than one 256x256 AC group.
-cujpegxl_status validate_config(const cujpegxl_config& c) {
+// allow_single: frames of one AC group (at most 256x256), which the reference
+// rejects, are accepted and written with the combined-section layout.
+cujpegxl_status validate_config(const cujpegxl_config& c, bool allow_single = false) {
     if (!(c.distance > 0.0f) || !std::isfinite(c.distance)) return CUJPEGXL_INVALID_ARGUMENT;
     if (c.width == 0 || c.height == 0 || c.width % 8 != 0 || c.height % 8 != 0) {
         return CUJPEGXL_UNSUPPORTED_RESOLUTION;
     }
     const std::size_t nac{((c.width / 8 + 31) / 32) * static_cast<std::size_t>((c.height / 8 + 31) / 32)};
-    if (nac <= 1) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
+    if (nac <= 1 && !allow_single) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
     // The TOC is written in one CTA's shared memory: about 25,000 sections
     // (1.6 gigapixels) at most.
     const std::size_t ndc{((c.width / 8 + 255) / 256) * static_cast<std::size_t>((c.height / 8 + 255) / 256)};
@@ -479,17 +482,31 @@ cujpegxl_status cujpegxl_query_backend(int32_t device_ordinal, cujpegxl_backend*
 }
 
 cujpegxl_status cujpegxl_max_output_size(const cujpegxl_config* config, size_t* out_bytes) {
-    if (config == nullptr || out_bytes == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
-    const cujpegxl_status st{validate_config(*config)};
+    return cujpegxl_b200_max_output_size_ex(config, 0u, out_bytes);
+}
+
+cujpegxl_status cujpegxl_b200_max_output_size_ex(const cujpegxl_config* config, uint32_t flags, size_t* out_bytes) {
+    if (config == nullptr || out_bytes == nullptr || (flags & ~CUJPEGXL_B200_ENCODER_SINGLE_GROUP) != 0) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    const cujpegxl_status st{validate_config(*config, (flags & CUJPEGXL_B200_ENCODER_SINGLE_GROUP) != 0)};
     if (st != CUJPEGXL_OK) return st;
     *out_bytes = jxb::worst_case_output(config->width, config->height);
     return CUJPEGXL_OK;
 }
 
 cujpegxl_status cujpegxl_encoder_create(const cujpegxl_config* config, cujpegxl_encoder** out_encoder) {
-    if (config == nullptr || out_encoder == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
+    return cujpegxl_b200_encoder_create_ex(config, 0u, out_encoder);
+}
+
+cujpegxl_status cujpegxl_b200_encoder_create_ex(const cujpegxl_config* config, uint32_t flags,
+                                                cujpegxl_encoder** out_encoder) {
+    if (config == nullptr || out_encoder == nullptr || (flags & ~CUJPEGXL_B200_ENCODER_SINGLE_GROUP) != 0) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
     *out_encoder = nullptr;
-    const cujpegxl_status st{validate_config(*config)};
+    const bool allow_single{(flags & CUJPEGXL_B200_ENCODER_SINGLE_GROUP) != 0};
+    const cujpegxl_status st{validate_config(*config, allow_single)};
     if (st != CUJPEGXL_OK) return st;
     int major{0};
     int minor{0};
@@ -498,6 +515,7 @@ cujpegxl_status cujpegxl_encoder_create(const cujpegxl_config* config, cujpegxl_
     if (e == nullptr) return CUJPEGXL_INTERNAL_ERROR;
     e->config = *config;
     e->device = config->device_ordinal;
+    e->allow_single = allow_single;
     DeviceScope scope{e->device};
     jxb::FrontendTables ft{};
     if (!scope.ok() || !device_tables(e->device, &ft) ||
@@ -513,7 +531,7 @@ cujpegxl_status cujpegxl_encoder_create(const cujpegxl_config* config, cujpegxl_
 
 cujpegxl_status cujpegxl_encoder_configure(cujpegxl_encoder* encoder, const cujpegxl_config* config) {
     if (encoder == nullptr || config == nullptr) return CUJPEGXL_INVALID_ARGUMENT;
-    const cujpegxl_status st{validate_config(*config)};
+    const cujpegxl_status st{validate_config(*config, encoder->allow_single)};
     if (st != CUJPEGXL_OK) return st;
     if (config->device_ordinal != encoder->config.device_ordinal) {
         int major{0};
@@ -543,7 +561,7 @@ cujpegxl_status cujpegxl_encoder_encode(cujpegxl_encoder* encoder, const cujpegx
         input->luma == 0 || input->chroma == 0) {
         return CUJPEGXL_INVALID_ARGUMENT;
     }
-    const cujpegxl_status st{validate_config(encoder->config)};
+    const cujpegxl_status st{validate_config(encoder->config, encoder->allow_single)};
     if (st != CUJPEGXL_OK) return st;
     if (input->luma_pitch < encoder->config.width || input->chroma_pitch < encoder->config.width) {
         return CUJPEGXL_INVALID_ARGUMENT;

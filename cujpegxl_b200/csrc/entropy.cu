@@ -841,10 +841,22 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
     auto* head_words{reinterpret_cast<unsigned int*>(head)};
     const int tid{static_cast<int>(threadIdx.x)};
     for (std::uint32_t i{static_cast<std::uint32_t>(tid)}; i < head_cap / 4; i += kLayoutThreads) head_words[i] = 0;
-    for (int s{tid}; s < e.nsec; s += kLayoutThreads) {
-        const Section sec{e.sections[s]};
-        const unsigned long long bits{prefix_at(e, sec.first + sec.count) - prefix_at(e, sec.first)};
-        sec_bytes[s] = static_cast<std::uint32_t>((bits + 7) / 8);
+    // With one AC group the four sections are one combined TOC entry: their
+    // bits follow each other with no padding between them
+    // (tools/bitstream/vardct_frame.cc:414-449).
+    const bool single{e.nac == 1};
+    const int ntoc{single ? 1 : e.nsec};
+    if (single) {
+        if (tid == 0) {
+            const unsigned long long bits{prefix_at(e, e.total_items) - prefix_at(e, 0)};
+            sec_bytes[0] = static_cast<std::uint32_t>((bits + 7) / 8);
+        }
+    } else {
+        for (int s{tid}; s < e.nsec; s += kLayoutThreads) {
+            const Section sec{e.sections[s]};
+            const unsigned long long bits{prefix_at(e, sec.first + sec.count) - prefix_at(e, sec.first)};
+            sec_bytes[s] = static_cast<std::uint32_t>((bits + 7) / 8);
+        }
     }
     __syncthreads();
     if (tid == 0) {
@@ -883,10 +895,10 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
         sh_toc_start = w.pos;
     }
     __syncthreads();
-    // Each thread takes a contiguous run of sections.
-    const int per{(e.nsec + kLayoutThreads - 1) / kLayoutThreads};
-    const int lo{min(e.nsec, tid * per)};
-    const int hi{min(e.nsec, lo + per)};
+    // Each thread takes a contiguous run of TOC entries.
+    const int per{(ntoc + kLayoutThreads - 1) / kLayoutThreads};
+    const int lo{min(ntoc, tid * per)};
+    const int hi{min(ntoc, lo + per)};
     unsigned long long my_bits{0};
     unsigned long long my_bytes{0};
     for (int s{lo}; s < hi; ++s) {
@@ -942,10 +954,15 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
     }
     __syncthreads();
     if (sh_status != 0) return;
-    {
+    if (single) {
+        const unsigned long long base{prefix_at(e, 0)};
+        for (int s{tid}; s < e.nsec; s += kLayoutThreads) {
+            e.sec_pos[s] = sh_start * 8 + (prefix_at(e, e.sections[s].first) - base);
+        }
+    } else {
         unsigned long long pos{sh_start + byte_off};
         for (int s{lo}; s < hi; ++s) {
-            e.sec_pos[s] = pos;
+            e.sec_pos[s] = pos * 8;
             pos += sec_bytes[s];
         }
     }
@@ -1007,7 +1024,7 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     if (tid == 0) {
         const Section sec{e.sections[st.section]};
         const unsigned long long p0{prefix_at(e, st.item0)};
-        const unsigned long long start{e.sec_pos[st.section] * 8 + (p0 - prefix_at(e, sec.first))};
+        const unsigned long long start{e.sec_pos[st.section] + (p0 - prefix_at(e, sec.first))};
         const unsigned long long bits{prefix_at(e, st.item0 + static_cast<std::uint32_t>(nitems)) - p0};
         const unsigned long long nw{bits == 0 ? 0ull : ((start + bits + 31) >> 5) - (start >> 5)};
         sh_start = start;
@@ -1142,7 +1159,7 @@ __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
         const Section sec{e.sections[s0]};
         const std::uint32_t end{min(min(first + blockDim.x, sec.first + sec.count), e.ac_first)};
         const unsigned long long p0{prefix_at(e, first)};
-        const unsigned long long start{e.sec_pos[s0] * 8 + (p0 - prefix_at(e, sec.first))};
+        const unsigned long long start{e.sec_pos[s0] + (p0 - prefix_at(e, sec.first))};
         const unsigned long long bits{prefix_at(e, end) - p0};
         const unsigned long long nw{bits == 0 ? 0ull : ((start + bits + 31) >> 5) - (start >> 5)};
         sh_start = start;
@@ -1156,7 +1173,7 @@ __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
     if (item < e.ac_first) {
         const int s{find_section(e.sections, 0, misc_hi(e), item)};
         const Section sec{e.sections[s]};
-        const unsigned long long pos{e.sec_pos[s] * 8 + (prefix_at(e, item) - prefix_at(e, sec.first))};
+        const unsigned long long pos{e.sec_pos[s] + (prefix_at(e, item) - prefix_at(e, sec.first))};
         const bool in_window{nwords >= 0 && item < sh_end};
         EmitVisitor v{&e, in_window ? win : reinterpret_cast<unsigned int*>(e.out),
                       in_window ? pos - ((sh_start >> 5) << 5) : pos, deferred, &sh_ndeferred};

@@ -95,7 +95,7 @@ struct EntropyDev {
     std::uint32_t* item_pre;         // [total_items] exclusive prefix within its scan tile
     std::uint32_t* tile_sum;         // [num_tiles]
     unsigned long long* tile_off;    // [num_tiles + 1]
-    unsigned long long* sec_pos;     // [nsec] absolute byte offset of each section in `out`
+    unsigned long long* sec_pos;     // [nsec] absolute bit offset of each section in `out`
     unsigned long long* result;      // [4]: total bytes, body start, status, 0
     std::uint8_t* out;               // output buffer (container + codestream)
     std::size_t out_capacity;

@@ -175,7 +175,8 @@ std::vector<std::uint8_t> dc_global_bits(std::uint32_t global_scale, std::uint32
     w.put(1, 1);
     w.put(1, 1);
     w.put(1, 0);
-    w.pos = (w.pos + 7) & ~7u;
+    // Unpadded: a separate DcGlobal section is padded by the layout, and in
+    // the combined single-group section the DcGroup follows bit for bit.
     *nbits = w.pos;
     return hb.bytes();
 }

@@ -573,7 +573,6 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
     const int nac{xg * ((f.bh + kAcGroupBlocks - 1) / kAcGroupBlocks)};
     const int xdg{(f.bw + kDcGroupBlocks - 1) / kDcGroupBlocks};
     const int ndc{xdg * ((f.bh + kDcGroupBlocks - 1) / kDcGroupBlocks)};
-    if (nac <= 1) fail("single-group frames are outside the subset");
     f.tiles_x = (f.bw + 7) / 8;
     const int tiles{f.tiles_x * ((f.bh + 7) / 8)};
     f.dc.assign(static_cast<std::size_t>(3) * nb, 0);
@@ -583,11 +582,13 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
     f.ytob.assign(static_cast<std::size_t>(tiles), 0);
     f.ac.assign(static_cast<std::size_t>(3) * nb * kCoeffsPerBlock, 0);
 
-    // TOC: DcGlobal, the DC groups, AcGlobal, the AC groups.
+    // TOC: DcGlobal, the DC groups, AcGlobal, the AC groups; with one AC
+    // group a single entry for all four, read as one bit stream.
     expect(br, 1, 0, "TOC permutation");
     br.align();
     const U32Dist toc_dist[4]{{false, 0, 10}, {false, 1024, 14}, {false, 17408, 22}, {false, 4211712, 30}};
-    const int nsec{2 + ndc + nac};
+    const bool single{nac == 1};
+    const int nsec{single ? 1 : 2 + ndc + nac};
     std::vector<std::size_t> sec_size(static_cast<std::size_t>(nsec));
     for (int s{0}; s < nsec; ++s) sec_size[static_cast<std::size_t>(s)] = read_u32(br, toc_dist);
     br.align();
@@ -601,7 +602,15 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
     auto section = [&](int s) {
         return BitReader{cs.data() + sec_at[static_cast<std::size_t>(s)], sec_size[static_cast<std::size_t>(s)]};
     };
+    BitReader whole{section(0)};
+    // The reader of logical section s: its own TOC section, or the combined one.
+    auto part = [&](int s, BitReader& own) -> BitReader& {
+        if (single) return whole;
+        own = section(s);
+        return own;
+    };
     auto finish = [&](const BitReader& r, int s) {
+        if (single) return;
         if (r.byte_pos() != sec_size[static_cast<std::size_t>(s)]) {
             fail("section " + std::to_string(s) + " ends at byte " + std::to_string(r.byte_pos()) + " of " +
                  std::to_string(sec_size[static_cast<std::size_t>(s)]));
@@ -609,7 +618,8 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
     };
 
     {  // DcGlobal
-        BitReader r{section(0)};
+        BitReader own{whole};
+        BitReader& r{part(0, own)};
         expect(r, 1, 1, "LF dequantisation all_default");
         const U32Dist gs[4]{{false, 1, 11}, {false, 2049, 11}, {false, 4097, 12}, {false, 8193, 16}};
         const U32Dist qdc[4]{{true, 16, 0}, {false, 1, 5}, {false, 1, 8}, {false, 1, 16}};
@@ -621,7 +631,8 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
         finish(r, 0);
     }
     for (int g{0}; g < ndc; ++g) {
-        BitReader r{section(1 + g)};
+        BitReader own{whole};
+        BitReader& r{part(1 + g, own)};
         read_dc_group(r, f, g);
         finish(r, 1 + g);
     }
@@ -631,7 +642,8 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
     const std::vector<std::uint16_t> order{natural_orders()};
     EntropyCode ac;
     {  // AcGlobal
-        BitReader r{section(1 + ndc)};
+        BitReader own{whole};
+        BitReader& r{part(1 + ndc, own)};
         expect(r, 1, 1, "dequantisation matrices all_default");
         expect(r, ceil_log2(static_cast<std::uint32_t>(nac)), 0, "num_histograms - 1");
         const U32Dist used[4]{{true, 0x5F, 0}, {true, 0x13, 0}, {true, 0, 0}, {false, 0, 13}};
@@ -640,9 +652,14 @@ void parse_frame(const std::uint8_t* data, std::size_t size, Frame& f) {
         finish(r, 1 + ndc);
     }
     for (int g{0}; g < nac; ++g) {
-        BitReader r{section(2 + ndc + g)};
+        BitReader own{whole};
+        BitReader& r{part(2 + ndc + g, own)};
         read_ac_group(r, f, g, ac, order);
         finish(r, 2 + ndc + g);
+    }
+    if (single && whole.byte_pos() != sec_size[0]) {
+        fail("combined section ends at byte " + std::to_string(whole.byte_pos()) + " of " +
+             std::to_string(sec_size[0]));
     }
 }
 

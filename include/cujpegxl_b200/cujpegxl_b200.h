@@ -37,6 +37,22 @@ typedef struct cujpegxl_b200_planes {
                        * elsewhere); only where the RD search ran */
 } cujpegxl_b200_planes;
 
+/* cujpegxl_encoder_create with options. CUJPEGXL_B200_ENCODER_SINGLE_GROUP
+ * also accepts frames of a single 256x256 AC group (width and height at most
+ * 256 pixels), which the reference rejects with UNSUPPORTED_RESOLUTION
+ * (src/cujpegxl.cc:36-48): their DcGlobal, DcGroup, AcGlobal and AcGroup are
+ * written as one combined section with a single TOC entry, concatenated bit
+ * by bit and padded once at the end, as the reference's own codestream tool
+ * writes such frames (tools/bitstream/vardct_frame.cc:414-449). The option
+ * stays with the encoder through cujpegxl_encoder_configure. */
+#define CUJPEGXL_B200_ENCODER_SINGLE_GROUP 1u
+cujpegxl_status cujpegxl_b200_encoder_create_ex(const cujpegxl_config* config, uint32_t flags,
+                                                cujpegxl_encoder** out_encoder);
+
+/* cujpegxl_max_output_size with the same options. */
+cujpegxl_status cujpegxl_b200_max_output_size_ex(const cujpegxl_config* config, uint32_t flags,
+                                                 size_t* out_bytes);
+
 /* Enables (non-zero) or disables the float/FP16 stage dumps of the frontend.
  * Replaces no reference interface. */
 cujpegxl_status cujpegxl_b200_encoder_set_debug(cujpegxl_encoder* encoder, int32_t enable);

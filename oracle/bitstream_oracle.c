@@ -549,10 +549,14 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
     const size_t xg = (bw + 31) / 32, yg = (bh + 31) / 32, nac = xg * yg;
     const size_t xdg = (bw + 255) / 256, ydg = (bh + 255) / 256, ndc = xdg * ydg;
     const size_t cmw = (bw + 7) / 8;
-    if (nac <= 1) return 0;
+    /* One AC group: DcGlobal, the DcGroup, AcGlobal and the AcGroup are one
+     * combined section, concatenated bit by bit and padded once at its end,
+     * with a single TOC entry (tools/bitstream/vardct_frame.cc:414-449). */
+    const int single = nac == 1;
     const size_t nsec = 2 + ndc + nac;
     BW* sec = (BW*)calloc(nsec, sizeof(BW));
     for (size_t i = 0; i < nsec; ++i) bw_init(&sec[i]);
+#define SECTION_END(w) do { if (!single) bw_pad(w); } while (0)
 
     /* DcGlobal */
     bw_put(&sec[0], 1, 1);
@@ -561,7 +565,7 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
     bw_put(&sec[0], 1, 1);
     bw_put(&sec[0], 1, 1);
     bw_put(&sec[0], 1, 0);
-    bw_pad(&sec[0]);
+    SECTION_END(&sec[0]);
 
     /* DcGroups */
     for (size_t g = 0; g < ndc; ++g) {
@@ -607,7 +611,7 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
         Chan mc[4] = {{cw, chh, meta}, {cw, chh, meta + cw * chh}, {count, 2, aq}, {dgw, dgh, epf}};
         bw_put(w, ceil_log2(dgw * dgh), (uint32_t)(count - 1));
         modular_header_and_tokens(w, mc, 4, 0);
-        bw_pad(w);
+        SECTION_END(w);
         free(meta);
         free(dch);
     }
@@ -639,7 +643,7 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
     uint16_t* bits = (uint16_t*)calloc(32 * 256, 2);
     for (int c = 0; c < 32; ++c)
         if (alpha[c] > 1) build_and_store(hist + c * 256, alpha[c], depth + c * 256, bits + c * 256, acg);
-    bw_pad(acg);
+    SECTION_END(acg);
     for (size_t g = 0; g < nac; ++g) {
         BW* w = &sec[2 + ndc + g];
         for (size_t i = 0; i < gt[g].n; ++i) {
@@ -647,13 +651,20 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
             bw_put(w, depth[t->cluster * 256 + t->sym], bits[t->cluster * 256 + t->sym]);
             if (t->nb) bw_put(w, t->nb, t->bits);
         }
-        bw_pad(w);
+        SECTION_END(w);
         free(gt[g].t);
     }
     free(gt);
     free(hist);
     free(depth);
     free(bits);
+#undef SECTION_END
+    size_t nout = nsec;
+    if (single) {
+        for (size_t i = 1; i < nsec; ++i) bw_append(&sec[0], &sec[i]);
+        bw_pad(&sec[0]);
+        nout = 1;
+    }
 
     /* Codestream head. */
     BW head;
@@ -685,7 +696,7 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
     bw_put(&head, 1, 0);       /* TOC: no permutation */
     bw_pad(&head);
     size_t body = 0;
-    for (size_t i = 0; i < nsec; ++i) {
+    for (size_t i = 0; i < nout; ++i) {
         write_u32(&head, kTocDist, (uint32_t)bw_bytes(&sec[i]));
         body += bw_bytes(&sec[i]);
     }
@@ -706,7 +717,7 @@ size_t oracle_assemble(int width, int height, const int16_t* ac, const int32_t* 
     if (large) for (int i = 0; i < 8; ++i) file[at++] = (uint8_t)(box >> (8 * (7 - i)));
     memcpy(file + at, head.buf, bw_bytes(&head));
     at += bw_bytes(&head);
-    for (size_t i = 0; i < nsec; ++i) { memcpy(file + at, sec[i].buf, bw_bytes(&sec[i])); at += bw_bytes(&sec[i]); }
+    for (size_t i = 0; i < nout; ++i) { memcpy(file + at, sec[i].buf, bw_bytes(&sec[i])); at += bw_bytes(&sec[i]); }
     if (out) memcpy(out, file, total < cap ? total : cap);
     free(file);
     bw_free(&head);
