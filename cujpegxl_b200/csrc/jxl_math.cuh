@@ -123,11 +123,14 @@ JX_HD float jx_exp(float x) {
     return p * u2f(static_cast<std::uint32_t>(ni + 127) << 23);
 }
 
-// Cube root of a positive normal x.
+// Cube root of a positive normal x: Newton iterations for x^(-1/3) from a
+// bit-pattern seed within a few percent (quadratic convergence: three reach
+// float precision), then one Newton correction of x^(1/3) itself. At most
+// 0.72 ulp on the XYB domain.
 JX_HD float jx_cbrt(float x) {
     const std::uint32_t u{f2u(x)};
     float r{u2f(0x54a2fa8cu - u / 3u)};  // seed for x^(-1/3), within a few percent
-    for (int it{0}; it < 4; ++it) {
+    for (int it{0}; it < 3; ++it) {
         const float t{(r * r) * r};
         const float e{jx_fma(-x, t, 1.0f)};
         r = jx_fma(r * 0.333333343f, e, r);
@@ -139,10 +142,32 @@ JX_HD float jx_cbrt(float x) {
     return y;
 }
 
-// x^2.4 for x in (0, 1].
+// x^2.4 for positive normal x, as x^2 * x^0.4 with x = 2^k m, m in [1, 2)
+// and k = 5q + r (r in 0..4): x^0.4 = 2^(2q) * 2^(0.4 r) * m^0.4. m^0.4 is a
+// degree-8 polynomial in m - 1.5 (Chebyshev interpolation of m^0.4 at 200
+// nodes on [1, 2], converted to powers and rounded to float; relative error
+// 8e-8 in float evaluation). At most 2.6 ulp on (0.09, 1], and 1 maps to 1.
 JX_HD float jx_pow24(float x) {
-    const float e{jx_exp2(0.4f * jx_log2(x))};
-    return (x * x) * e;
+    const std::uint32_t u{f2u(x)};
+    const int k{static_cast<int>((u >> 23) & 0xffu) - 127};
+    const float m{u2f((u & 0x7fffffu) | 0x3f800000u)};
+    const int q{(k >= 0 ? k : k - 4) / 5};  // floor(k / 5)
+    const int r{k - 5 * q};
+    const float c{r == 0 ? 1.0f
+                         : (r == 1 ? 1.31950791077289425f
+                                   : (r == 2 ? 1.74110112659224828f
+                                             : (r == 3 ? 2.29739670999407037f : 3.03143313302079624f)))};
+    const float v{m - 1.5f};  // exact
+    float p{-8.58357804e-04f};
+    p = jx_fma(p, v, 1.51637842e-03f);
+    p = jx_fma(p, v, -2.33355959e-03f);
+    p = jx_fma(p, v, 4.58948039e-03f);
+    p = jx_fma(p, v, -9.66759456e-03f);
+    p = jx_fma(p, v, 2.23054436e-02f);
+    p = jx_fma(p, v, -6.27241061e-02f);
+    p = jx_fma(p, v, 3.13621006e-01f);
+    p = jx_fma(p, v, 1.17607902e+00f);
+    return ((x * x) * (p * c)) * u2f(static_cast<std::uint32_t>(2 * q + 127) << 23);
 }
 
 }  // namespace jxb

@@ -86,7 +86,7 @@ float oracle_exp(float x) {
 float oracle_cbrt(float x) {
     const uint32_t u = f2u(x);
     float r = u2f(0x54a2fa8cu - u / 3u);
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < 3; ++it) {
         const float t = (r * r) * r;
         const float e = fmaf(-x, t, 1.0f);
         r = fmaf(r * 0.333333343f, e, r);
@@ -99,8 +99,26 @@ float oracle_cbrt(float x) {
 }
 
 float oracle_pow24(float x) {
-    const float e = oracle_exp2(0.4f * oracle_log2(x));
-    return (x * x) * e;
+    const uint32_t u = f2u(x);
+    const int k = (int)((u >> 23) & 0xffu) - 127;
+    const float m = u2f((u & 0x7fffffu) | 0x3f800000u);
+    const int q = (k >= 0 ? k : k - 4) / 5;
+    const int r = k - 5 * q;
+    const float c = r == 0 ? 1.0f
+                           : (r == 1 ? 1.31950791077289425f
+                                     : (r == 2 ? 1.74110112659224828f
+                                               : (r == 3 ? 2.29739670999407037f : 3.03143313302079624f)));
+    const float v = m - 1.5f;
+    float p = -8.58357804e-04f;
+    p = fmaf(p, v, 1.51637842e-03f);
+    p = fmaf(p, v, -2.33355959e-03f);
+    p = fmaf(p, v, 4.58948039e-03f);
+    p = fmaf(p, v, -9.66759456e-03f);
+    p = fmaf(p, v, 2.23054436e-02f);
+    p = fmaf(p, v, -6.27241061e-02f);
+    p = fmaf(p, v, 3.13621006e-01f);
+    p = fmaf(p, v, 1.17607902e+00f);
+    return ((x * x) * (p * c)) * u2f((uint32_t)(2 * q + 127) << 23);
 }
 
 /* IEEE binary16 conversions (round to nearest even). */
