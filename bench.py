@@ -510,6 +510,29 @@ def run_batch(args) -> None:
     dt = start.elapsed_time(stop) / 1000.0
     n = args.steps * len(MIXED64)
     mp = sum(w * h for w, h in MIXED64) * args.steps / 1e6
+
+    # The same batch with learned transform decisions (the shipped network,
+    # split and quant field, margin 0.2): the graph is captured and tuned
+    # again, then timed the same way.
+    from cujpegxl_b200.acsnet import DEFAULT_MARGIN, QF, SPLIT, AcsNet
+
+    net = AcsNet.load(device_ordinal=local)
+    batch.set_acsnet(net, DEFAULT_MARGIN, SPLIT | QF)
+    for _ in range(args.warmup):
+        batch.encode(inputs)
+        batch.sync()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        batch.encode(inputs)
+    stop.record(stream)
+    lsizes = batch.sync()
+    torch.cuda.synchronize()
+    ldt = start.elapsed_time(stop) / 1000.0
+    learned = {"value": n / ldt, "unit": "frames/s", "mp_per_s": mp / ldt, "bytes_per_step": sum(lsizes),
+               "lanes": batch.lanes, "decisions": "split and quant field, margin 0.2"}
+    batch.set_acsnet(None)
+    net.close()
     if rank == 0:
         print(json.dumps({
             "metric": "mixed-resolution batch frames/s", "value": n / dt, "unit": "frames/s", "n_gpus": world,
@@ -521,6 +544,7 @@ def run_batch(args) -> None:
             "mp_per_s": mp / dt, "bytes_per_step": sum(sizes),
             "timing": "CUDA events on the batch's stream around K graph launches (each ends with the "
                       "device-to-host copy of every frame's size)",
+            "learned": learned,
         }), flush=True)
     torch.cuda.synchronize()
     del start, stop, stream
