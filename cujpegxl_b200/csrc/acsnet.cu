@@ -468,12 +468,7 @@ __device__ __forceinline__ SplitHead split_head(float logit) {
 
 // ---- Inference inside an encode ----
 
-// The network's input pixel: xyb_pixel's NV12 -> XYB conversion with the two
-// transfer functions taken from the hardware base-2 exponential and
-// logarithm (x^2.4 = 2^(2.4 log2 x), cbrt x = 2^(log2 x / 3)) instead of the
-// frontend's correctly rounded ones. The values differ from the frontend's
-// by about 1e-6 relative, far below the BF16 rounding of the input (4e-3),
-// and cost a fraction of the instructions.
+// Hardware base-2 exponential and logarithm (PTX ex2/lg2.approx).
 __device__ __forceinline__ float hw_exp2(float x) {
     float y;
     asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -486,38 +481,36 @@ __device__ __forceinline__ float hw_log2(float x) {
     return y;
 }
 
-template <int kWin>
-__device__ __forceinline__ void net_xyb_pixel(int luma, const std::uint8_t* win, int cx0, int cy0, int gx, int gy,
-                                              int width, int height, float& ox, float& oy, float& ob) {
+// The network's input pixel: xyb_pixel's NV12 -> XYB conversion, from the
+// pixel's luma byte and its four chroma taps ((cb, cr) pairs as 16-bit words:
+// top-left, top-right, bottom-left, bottom-right, weights wxa (left) and wya
+// (top) in {1, 3}), with the two transfer functions taken from the hardware
+// exp2/log2 (x^2.4 = 2^(2.4 log2 x), cbrt x = 2^(log2 x / 3)) instead of the
+// frontend's exact ones. The values differ from the frontend's by about 1e-6
+// relative, far below the BF16 rounding of the input (4e-3), at a fraction of
+// the instructions.
+__device__ __forceinline__ void net_xyb_taps(int luma, unsigned aa, unsigned ab, unsigned ba, unsigned bb, int wxa,
+                                             int wya, float& ox, float& oy, float& ob) {
     const float yv{static_cast<float>(luma) * kInv255};
-    const int jx{gx >> 1};
-    const int jy{gy >> 1};
-    const int xa{(gx & 1) ? jx : max(jx - 1, 0)};
-    const int xb{(gx & 1) ? min(jx + 1, (width >> 1) - 1) : jx};
-    const int ya{(gy & 1) ? jy : max(jy - 1, 0)};
-    const int yb{(gy & 1) ? min(jy + 1, (height >> 1) - 1) : jy};
-    const int wxa{(gx & 1) ? 3 : 1};
-    const int wya{(gy & 1) ? 3 : 1};
-    const int aa{2 * ((ya - cy0) * kWin + xa - cx0)};
-    const int ab{2 * ((ya - cy0) * kWin + xb - cx0)};
-    const int ba{2 * ((yb - cy0) * kWin + xa - cx0)};
-    const int bb{2 * ((yb - cy0) * kWin + xb - cx0)};
-    const int scb{wya * (wxa * win[aa] + (4 - wxa) * win[ab]) + (4 - wya) * (wxa * win[ba] + (4 - wxa) * win[bb])};
-    const int scr{wya * (wxa * win[aa + 1] + (4 - wxa) * win[ab + 1]) +
-                  (4 - wya) * (wxa * win[ba + 1] + (4 - wxa) * win[bb + 1])};
+    const int wxb{4 - wxa};
+    const int wyb{4 - wya};
+    const int scb{wya * (wxa * static_cast<int>(aa & 0xffu) + wxb * static_cast<int>(ab & 0xffu)) +
+                  wyb * (wxa * static_cast<int>(ba & 0xffu) + wxb * static_cast<int>(bb & 0xffu))};
+    const int scr{wya * (wxa * static_cast<int>(aa >> 8) + wxb * static_cast<int>(ab >> 8)) +
+                  wyb * (wxa * static_cast<int>(ba >> 8) + wxb * static_cast<int>(bb >> 8))};
     const float cb{static_cast<float>(scb) * (1.0f / 4080.0f) - kChromaCenter};
     const float cr{static_cast<float>(scr) * (1.0f / 4080.0f) - kChromaCenter};
     auto lin = [](float e) {
         e = clamp01(e);
         return clamp01(e <= 0.04045f ? e * (1.0f / 12.92f) : hw_exp2(2.4f * hw_log2((e + 0.055f) * (1.0f / 1.055f))));
     };
-    const float r{lin(kCrToR * cr + yv)};
-    const float g{lin(yv - kCbToG * cb - kCrToG * cr)};
-    const float b{lin(kCbToB * cb + yv)};
+    const float r{lin(jx_fma(kCrToR, cr, yv))};
+    const float g{lin(jx_fma(-kCrToG, cr, jx_fma(-kCbToG, cb, yv)))};
+    const float b{lin(jx_fma(kCbToB, cb, yv))};
     auto cbrt_pos = [](float v) { return v > 0.0f ? hw_exp2(hw_log2(v) * (1.0f / 3.0f)) : 0.0f; };
-    const float m0{cbrt_pos(kM00 * r + kM01 * g + kM02 * b + kOpsinBias) + kNegCbrtBias};
-    const float m1{cbrt_pos(kM10 * r + kM11 * g + kM12 * b + kOpsinBias) + kNegCbrtBias};
-    const float m2{cbrt_pos(kM20 * r + kM21 * g + kM22 * b + kOpsinBias) + kNegCbrtBias};
+    const float m0{cbrt_pos(jx_fma(kM02, b, jx_fma(kM01, g, jx_fma(kM00, r, kOpsinBias)))) + kNegCbrtBias};
+    const float m1{cbrt_pos(jx_fma(kM12, b, jx_fma(kM11, g, jx_fma(kM10, r, kOpsinBias)))) + kNegCbrtBias};
+    const float m2{cbrt_pos(jx_fma(kM22, b, jx_fma(kM21, g, jx_fma(kM20, r, kOpsinBias)))) + kNegCbrtBias};
     ox = 0.5f * (m0 - m1);
     oy = 0.5f * (m0 + m1);
     ob = m2;
@@ -609,19 +602,41 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         if (full != 0) {   // block-uniform
             const int cx0{(px0 >> 1) - 2};
             const int cy0{(py0 >> 1) - 2};
-            for (int i{tid}; i < 4 * kNetInPix; i += kInferThreads) {
-                const int r{i / kNetInPix};
-                if (((full >> r) & 1u) == 0) continue;
-                const int k{i - r * kNetInPix};
-                const int wy{32 * (r >> 1) + k / kNetInW};
-                const int wx{32 * (r & 1) + k % kNetInW};
-                const int gx{min(max(px0 - 1 + wx, 0), W - 1)};
-                const int gy{min(max(py0 - 1 + wy, 0), H - 1)};
-                float x, y, b;
-                net_xyb_pixel<kTileChroma>(win_luma[wy * kTileWin + wx], win_chroma, cx0, cy0, gx, gy, W, H, x, y,
-                                           b);
-                const int at{(k / kNetInW) * kNetInW + par_col<kNetInW, true>(k % kNetInW)};
-                *reinterpret_cast<uint4*>(&s.x1[r][at * kNetIn]) = input_pixel(p, x, y, b, log2_distance);
+            // Thread t takes stored (parity-split) column t % 34 of rows
+            // t / 34, t / 34 + 15, ... of every full region: its column's
+            // chroma taps and clamps are computed once, and a warp's stores
+            // are contiguous.
+            constexpr int kRowLanes{kInferThreads / kNetInW};  // 15
+            if (tid < kNetInW * kRowLanes) {
+                const int c{tid % kNetInW};
+                const int x{c < (kNetInW + 1) / 2 ? 2 * c : 2 * (c - (kNetInW + 1) / 2) + 1};
+                const auto* cw{reinterpret_cast<const std::uint16_t*>(win_chroma)};
+#pragma unroll 1
+                for (int rx{0}; rx < 2; ++rx) {
+                    const int wx{32 * rx + x};
+                    const int gx{min(max(px0 - 1 + wx, 0), W - 1)};
+                    const int jx{gx >> 1};
+                    const int xa{((gx & 1) ? jx : max(jx - 1, 0)) - cx0};
+                    const int xb{((gx & 1) ? min(jx + 1, (W >> 1) - 1) : jx) - cx0};
+                    const int wxa{(gx & 1) ? 3 : 1};
+#pragma unroll 1
+                    for (int ry{0}; ry < 2; ++ry) {
+                        const int r{2 * ry + rx};
+                        if (((full >> r) & 1u) == 0) continue;
+                        for (int row{tid / kNetInW}; row < kNetInW; row += kRowLanes) {
+                            const int wy{32 * ry + row};
+                            const int gy{min(max(py0 - 1 + wy, 0), H - 1)};
+                            const int jy{gy >> 1};
+                            const int ya{(((gy & 1) ? jy : max(jy - 1, 0)) - cy0) * kTileChroma};
+                            const int yb{(((gy & 1) ? min(jy + 1, (H >> 1) - 1) : jy) - cy0) * kTileChroma};
+                            float xv, yv, bv;
+                            net_xyb_taps(win_luma[wy * kTileWin + wx], cw[ya + xa], cw[ya + xb], cw[yb + xa],
+                                         cw[yb + xb], wxa, (gy & 1) ? 3 : 1, xv, yv, bv);
+                            *reinterpret_cast<uint4*>(&s.x1[r][(row * kNetInW + c) * kNetIn]) =
+                                input_pixel(p, xv, yv, bv, log2_distance);
+                        }
+                    }
+                }
             }
             __syncthreads();
             // Groups of regions outside the image run on stale data and
