@@ -158,6 +158,55 @@ __device__ __forceinline__ unsigned im2col_row(unsigned in, unsigned zero, int p
     return ok ? in + 2u * static_cast<unsigned>((iy * kInW + par_col<kInW, kPar>(ix)) * kInS + ci) : zero;
 }
 
+// im2col rows of one output position p, with everything that depends on p
+// computed once: the address of the tap (0, 0) and a 9-bit mask of the taps
+// inside the input. Tap (ky, kx) then lies a compile-time offset away: rows
+// kInW apart, and columns at c(kx) from the position's column, where c is
+// (kx - kPad) plainly and, in the parity-split layout (stride 2), the stored
+// column of 2 ox + kx - kPad relative to ox.
+template <int kInW, int kOutW, int kStride, int kPad, int kCin, int kInS, bool kPar = false>
+struct Im2colRows {
+    unsigned base;
+    unsigned valid;
+
+    __device__ __forceinline__ Im2colRows(unsigned in, int p) {
+        const int oy{p / kOutW};
+        const int ox{p - oy * kOutW};
+        const int iy0{oy * kStride - kPad};
+        const int ix0{ox * kStride - kPad};
+        valid = 0;
+#pragma unroll
+        for (int t{0}; t < 9; ++t) {
+            const int iy{iy0 + t / 3};
+            const int ix{ix0 + t % 3};
+            valid |= (iy >= 0 && iy < kInW && ix >= 0 && ix < kInW ? 1u : 0u) << t;
+        }
+        base = in + 2u * static_cast<unsigned>((iy0 * kInW + (kPar ? ox : ix0)) * kInS);
+    }
+
+    __host__ __device__ static constexpr int col(int kx) {
+        return !kPar ? kx : ((((kx - kPad) & 1) != 0) ? (kInW + 1) / 2 + ((kx - kPad) >> 1) : ((kx - kPad) >> 1));
+    }
+
+    __host__ __device__ static constexpr unsigned offset(int tap, int ci) {
+        return 2u * static_cast<unsigned>(((tap / 3) * kInW + col(tap % 3)) * kInS + ci);
+    }
+
+    __device__ __forceinline__ unsigned tap_at(unsigned zero, int tap, int ci) const {
+        return tap < 9 && ((valid >> tap) & 1u) != 0 ? base + offset(tap, ci) : zero;
+    }
+
+    // Address of reduction columns k0 + 8h .. k0 + 8h + 7 (k0 a compile-time
+    // constant once the caller's loop is unrolled, h the lane's half 0/1).
+    __device__ __forceinline__ unsigned at(unsigned zero, int k0, int h) const {
+        if (kCin >= 16) {  // both halves in one tap
+            const int tap{k0 / kCin};
+            return tap < 9 && ((valid >> tap) & 1u) != 0 ? base + offset(tap, k0 - tap * kCin) + 16u * h : zero;
+        }
+        return h ? tap_at(zero, k0 / kCin + 1, 0) : tap_at(zero, k0 / kCin, 0);
+    }
+};
+
 // Forward of a layer with at least four 16-row position tiles (L1, L2): warp w
 // takes position tiles w, w+4, ... (two at a time, 32 accumulators) and all
 // four 8-channel output tiles.
@@ -167,8 +216,12 @@ __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w,
                                          int warp, int lane) {
     constexpr int kMW{kOutW * kOutW / 64};
     constexpr int kChunk{kMW < 2 ? kMW : 2};
+    using Rows = Im2colRows<kInW, kOutW, kStride, kPad, kCin, kInS, kParIn>;
 #pragma unroll 1
     for (int i0{0}; i0 < kMW; i0 += kChunk) {
+        // kChunk is 1 or 2: the rows of position tiles i0 and i0 + kChunk - 1.
+        const Rows rows0{in, (warp + 4 * i0) * 16 + (lane & 15)};
+        const Rows rows1{in, (warp + 4 * (i0 + kChunk - 1)) * 16 + (lane & 15)};
         float acc[kChunk][4][4];
 #pragma unroll
         for (int i{0}; i < kChunk; ++i) {
@@ -195,8 +248,7 @@ __device__ __forceinline__ void fwd_rows(unsigned in, unsigned zero, unsigned w,
 #pragma unroll
             for (int i{0}; i < kChunk; ++i) {
                 unsigned a[4];
-                ldsm_x4(a, im2col_row<kInW, kOutW, kStride, kPad, kCin, kInS, kParIn>(
-                               in, zero, (warp + 4 * (i0 + i)) * 16 + (lane & 15), k0 + (lane >> 4) * 8));
+                ldsm_x4(a, (i == 0 ? rows0 : rows1).at(zero, k0, lane >> 4));
 #pragma unroll
                 for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
             }
@@ -226,10 +278,11 @@ __device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w,
     // Two accumulators over alternate reduction steps halve the dependent
     // chain of tensor-core operations.
     float acc[2][4]{{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
+    const Im2colRows<kInW, 4, kStride, 1, kNetC, kActS> rows{in, lane & 15};
 #pragma unroll
     for (int k0{0}; k0 < kNetK; k0 += 16) {
         unsigned a[4];
-        ldsm_x4(a, im2col_row<kInW, 4, kStride, 1, kNetC, kActS>(in, zero, lane & 15, k0 + (lane >> 4) * 8));
+        ldsm_x4(a, rows.at(zero, k0, lane >> 4));
         unsigned b[2];
         ldsm_x2(b, w + 2u * static_cast<unsigned>((8 * warp + (lane & 7)) * kWS + k0 + ((lane >> 3) & 1) * 8));
         mma(acc[(k0 >> 4) & 1], a, b[0], b[1]);
