@@ -21,6 +21,10 @@ NO_DEVICE = 4
 INTERNAL_ERROR = 5
 BUFFER_TOO_SMALL = 6
 
+# cujpegxl_b200_encoder_enqueue_stages stage bits.
+STAGE_FRONTEND = 1
+STAGE_ENTROPY = 2
+
 EXPORTS = (
     "cujpegxl_api_version", "cujpegxl_status_string", "cujpegxl_backend_string",
     "cujpegxl_query_backend", "cujpegxl_max_output_size", "cujpegxl_encoder_create",
