@@ -47,20 +47,26 @@ static_assert(kDrowsOffset + 64 * 72 <= kRegionAFloats, "final-DCT scratch excee
 // Selection bases: double-precision DCT-II basis narrowed to float
 // (basis[k*n + t], src/transform_select.cu:29-37). Final-DCT bases: the float
 // basis of src/frontend_transform.cu:104-106 (cosf of a float argument).
-__constant__ float c_sel8[64];
-__constant__ float c_sel16[256];
-__constant__ float c_sel32[1024];
-__constant__ float c_dct8[64];
-__constant__ float c_dct16[256];
-__constant__ float c_dct32[1024];
+// Stored as pairs of consecutive frequencies, {basis[k][t], basis[k+1][t]} at
+// (k/2)*n + t for even k, so that the DCT passes compute two coefficients per
+// packed f32x2 instruction (per component the same rounding as the scalar
+// instruction, so the results are those of the scalar chains).
+__constant__ float2 c_sel8[32];
+__constant__ float2 c_sel16[128];
+__constant__ float2 c_sel32[512];
+__constant__ float2 c_dct8[32];
+__constant__ float2 c_dct16[128];
+__constant__ float2 c_dct32[512];
 
 template <int N, bool kSel>
-__device__ __forceinline__ float basis(int i) {
+__device__ __forceinline__ float2 basis2(int i) {
     if (kSel) {
         return N == 8 ? c_sel8[i] : (N == 16 ? c_sel16[i] : c_sel32[i]);
     }
     return N == 8 ? c_dct8[i] : (N == 16 ? c_dct16[i] : c_dct32[i]);
 }
+
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
 // Rate-proxy table entries kept in shared memory: quantised magnitudes below
 // this are by far the most frequent.
@@ -200,26 +206,29 @@ __device__ __forceinline__ float warp_tree(float v) {
 
 // Row pass of an N-point separable DCT: dst[fx*(N+1)] for fx in [F0, F1) from
 // one pixel row. Selection bases accumulate without FMA (the host twin's
-// arithmetic); final-DCT bases accumulate with FMA.
+// arithmetic); final-DCT bases accumulate with FMA. Coefficients fx and fx+1
+// share each packed instruction; each is its own chain in c order.
 template <int N, int F0, int F1, bool kSel>
 __device__ __forceinline__ void row_pass(const float* src, float* dst) {
-    float p[N];
+    static_assert(F0 % 2 == 0 && F1 % 2 == 0, "pairs of frequencies");
+    float2 p[N];
 #pragma unroll
     for (int c{0}; c < N; ++c) {
-        p[c] = src[c];
+        p[c] = dup2(src[c]);
     }
 #pragma unroll
-    for (int fx{F0}; fx < F1; ++fx) {
-        float s{0.0f};
+    for (int fx{F0}; fx < F1; fx += 2) {
+        float2 s{0.0f, 0.0f};
 #pragma unroll
         for (int c{0}; c < N; ++c) {
             if (kSel) {
-                s = s + basis<N, true>(fx * N + c) * p[c];
+                s = __fadd2_rn(s, __fmul2_rn(basis2<N, true>((fx >> 1) * N + c), p[c]));
             } else {
-                s = jx_fma(basis<N, false>(fx * N + c), p[c], s);
+                s = __ffma2_rn(basis2<N, false>((fx >> 1) * N + c), p[c], s);
             }
         }
-        dst[fx * (N + 1)] = s;
+        dst[fx * (N + 1)] = s.x;
+        dst[(fx + 1) * (N + 1)] = s.y;
     }
 }
 
@@ -249,35 +258,42 @@ template <int N, int Y0, int Y1>
 __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, float* cr_fx, int fx,
                                         float qgsf, const float* wsel, const float* l2t,
                                         const float* l2s) {
-    float rr[N];
+    static_assert(Y0 % 2 == 0 && Y1 % 2 == 0, "pairs of frequencies");
+    float2 rr[N];
 #pragma unroll
     for (int r{0}; r < N; ++r) {
-        rr[r] = rows_fx[r];
+        rr[r] = dup2(rows_fx[r]);
     }
 #pragma unroll
-    for (int fy{Y0}; fy < Y1; ++fy) {
-        float coeff{0.0f};
+    for (int fy0{Y0}; fy0 < Y1; fy0 += 2) {
+        float2 c2{0.0f, 0.0f};
 #pragma unroll
         for (int r{0}; r < N; ++r) {
-            coeff = coeff + basis<N, true>(fy * N + r) * rr[r];
+            c2 = __fadd2_rn(c2, __fmul2_rn(basis2<N, true>((fy0 >> 1) * N + r), rr[r]));
         }
-        float d{0.0f};
-        float rt{0.0f};
-        if (!(fx < N / 8 && fy < N / 8)) {
-            const float w{wsel[fx * N + fy]};
-            const float scaled{coeff * qgsf};
-            if (fabsf(scaled) <= 0.5f * w) {
-                // |scaled / w| <= 1/2 rounds to a quotient of at most 1/2, so q
-                // is zero and err is -coeff exactly: the same d, no rate.
-                d = coeff * coeff;
-            } else {
-                const float2 dr{sel_cost_nonzero(coeff, scaled, w, qgsf, l2t, l2s)};
-                d = dr.x;
-                rt = dr.y;
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            const int fy{fy0 + h};
+            const float coeff{h == 0 ? c2.x : c2.y};
+            float d{0.0f};
+            float rt{0.0f};
+            if (!(fx < N / 8 && fy < N / 8)) {
+                const float w{wsel[fx * N + fy]};
+                const float scaled{coeff * qgsf};
+                if (fabsf(scaled) <= 0.5f * w) {
+                    // |scaled / w| <= 1/2 rounds to a quotient of at most 1/2,
+                    // so q is zero and err is -coeff exactly: the same d, no
+                    // rate.
+                    d = coeff * coeff;
+                } else {
+                    const float2 dr{sel_cost_nonzero(coeff, scaled, w, qgsf, l2t, l2s)};
+                    d = dr.x;
+                    rt = dr.y;
+                }
             }
+            cd_fx[fy] = d;
+            cr_fx[fy] = rt;
         }
-        cd_fx[fy] = d;
-        cr_fx[fy] = rt;
     }
 }
 
@@ -287,23 +303,26 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
 template <int N, int Y0, int Y1>
 __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int fx, int fbx,
                                         int fby) {
-    float rr[N];
+    static_assert(Y0 % 2 == 0 && Y1 % 2 == 0, "pairs of frequencies");
+    float2 rr[N];
 #pragma unroll
     for (int r{0}; r < N; ++r) {
-        rr[r] = rows_fx[r];
+        rr[r] = dup2(rows_fx[r]);
     }
     constexpr int side{N / 8};
 #pragma unroll
-    for (int fy{Y0}; fy < Y1; ++fy) {
-        float coeff{0.0f};
+    for (int fy{Y0}; fy < Y1; fy += 2) {
+        float2 c2{0.0f, 0.0f};
 #pragma unroll
         for (int r{0}; r < N; ++r) {
-            coeff = jx_fma(basis<N, false>(fy * N + r), rr[r], coeff);
+            c2 = __ffma2_rn(basis2<N, false>((fy >> 1) * N + r), rr[r], c2);
         }
+        // raw and raw + 1 share their 64-slot group (raw is even), and the
+        // pair's slot is 4-byte aligned (kCoefBlock is even).
         const int raw{fx * N + fy};
         const int q{raw >> 6};
         const int lb{(fby + q / side) * 8 + fbx + q % side};
-        coef[lb * kCoefBlock + (raw & 63)] = __float2half_rn(coeff);
+        *reinterpret_cast<__half2*>(coef + lb * kCoefBlock + (raw & 63)) = __floats2half2_rn(c2.x, c2.y);
     }
 }
 
@@ -1265,16 +1284,17 @@ FrontendScalars frontend_scalars(float distance, std::uint32_t* global_scale,
 bool frontend_tables_init(FrontendTables* tables) {
     // Bases.
     for (int n : {8, 16, 32}) {
+        // Pair layout: element 2 * ((k / 2) * n + t) + (k & 1) holds basis[k][t].
         std::vector<float> sel(static_cast<std::size_t>(n) * n);
         std::vector<float> dct(static_cast<std::size_t>(n) * n);
         for (int k{0}; k < n; ++k) {
             const double g{k == 0 ? 1.0 / n : 1.4142135623730950488 / n};
             const float gf{k == 0 ? 1.0f / n : 1.4142135623730951f / n};
             for (int t{0}; t < n; ++t) {
-                sel[k * n + t] =
-                    static_cast<float>(g * std::cos(3.14159265358979323846 * (t + 0.5) * k / n));
+                const int at{2 * ((k >> 1) * n + t) + (k & 1)};
+                sel[at] = static_cast<float>(g * std::cos(3.14159265358979323846 * (t + 0.5) * k / n));
                 const float arg{3.14159265358979323846f * (t + 0.5f) * k / n};
-                dct[k * n + t] = gf * std::cos(arg);
+                dct[at] = gf * std::cos(arg);
             }
         }
         const void* sel_sym{n == 8 ? static_cast<const void*>(&c_sel8)
