@@ -478,15 +478,22 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
     for (int ri{0}; ri < 4; ++ri) dmask |= (sm.net[ri] >= 0 ? 1u : 0u) << ri;
     const unsigned qmask{in.net_qf != nullptr ? dmask : 0u};
-    // 1b. XYB of every halo pixel from the window.
-    for (int i{tid}; i < kXplane; i += kThreads) {
-        const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
-        const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
-        float x, y, b;
-        xyb_pixel<kChromaWin>(win_luma[i], win_chroma, cx0, cy0, gx, gy, W, H, x, y, b);
-        xyb[i] = x;
-        xyb[kXplane + i] = y;
-        xyb[2 * kXplane + i] = b;
+    // 1b. XYB of every halo pixel from the window, two horizontally adjacent
+    // pixels per thread (the row length kXs is even, so a pair never spans
+    // two rows, and its float2 stores are 8-byte aligned).
+    static_assert(kXs % 2 == 0 && kXplane % 2 == 0, "XYB pairs");
+    for (int i2{tid}; i2 < kXplane / 2; i2 += kThreads) {
+        const int i{2 * i2};
+        const int row{i / kXs};
+        const int col{i - row * kXs};
+        const int gx0{min(max(px0 - kHalo + col, 0), W - 1)};
+        const int gx1{min(max(px0 - kHalo + col + 1, 0), W - 1)};
+        const int gy{min(max(py0 - kHalo + row, 0), H - 1)};
+        float2 x, y, b;
+        xyb_pixel2<kChromaWin>(win_luma[i], win_luma[i + 1], win_chroma, cx0, cy0, gx0, gx1, gy, W, H, x, y, b);
+        *reinterpret_cast<float2*>(xyb + i) = x;
+        *reinterpret_cast<float2*>(xyb + kXplane + i) = y;
+        *reinterpret_cast<float2*>(xyb + 2 * kXplane + i) = b;
     }
     __syncthreads();
 
@@ -1139,60 +1146,75 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float ytox{static_cast<float>(sm.mx) * kCflColorScale};
     const float ytob{jx_fma(static_cast<float>(sm.mb), kCflColorScale, kCflBaseB)};
     const std::size_t cplane{static_cast<std::size_t>(nblocks) * 64};
-    for (int k{tid}; k < 4096; k += kThreads) {  // 16 uniform iterations per warp
+    // Two adjacent slots (one even raw index and the next) per thread: they
+    // share the block, its quant field and weights row, and their coefficient,
+    // weight and output pairs move as single 4- or 8-byte accesses.
+    for (int k2{tid}; k2 < 2048; k2 += kThreads) {  // 8 uniform iterations per warp
+        const int k{2 * k2};
         const int lb{k >> 6};
         const int slot{k & 63};
         const int lbx{lb & 7};
         const int lby{lb >> 3};
         const bool inside{bx0 + lbx < bw && by0 + lby < bh};
         const int f{inside ? static_cast<int>(sm.owner[lb]) : -1};
-        std::int16_t ax{0};
-        std::int16_t ay{0};
-        std::int16_t ab{0};
+        std::int16_t ax[2]{0, 0};
+        std::int16_t ay[2]{0, 0};
+        std::int16_t ab[2]{0, 0};
         if (inside) {
             const int n{sm.acs[f]};
             const int side{n >> 3};
             const int lrow{side == 1 ? 3 : (side == 2 ? 4 : 5)};  // log2(n)
             const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
-            const int raw{q * 64 + slot};
-            if (!((raw >> lrow) < side && (raw & (n - 1)) < side)) {
+            const int raw{q * 64 + slot};  // even; raw + 1 is in the same row
+            const bool llf_row{(raw >> lrow) < side};
+            const int col{raw & (n - 1)};
+            const bool llf[2]{llf_row && col < side, llf_row && col + 1 < side};
+            if (!(llf[0] && llf[1])) {
                 const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
                 const float* wt{tb.dequant + si * 3072};
                 const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
                 const int ci{lb * kCoefBlock + slot};
-                const float xr{__half2float(coef[ci])};
-                const float yr{__half2float(coef[kCoefPlane + ci])};
-                const float br{__half2float(coef[2 * kCoefPlane + ci])};
-                const float wy{wt[1024 + raw]};
-                const int qy{quantize(yr, qgsf, wy)};
-                // A zero Y quantum reconstructs to a signed zero, and
-                // fma(-m, +-0, v) equals v up to the sign of a zero result,
-                // which quantises to 0 either way.
-                const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy) / qgsf};
-                const float wx{wt[raw]};
-                const int qx{quantize(jx_fma(-ytox, yq, xr), qgsf, wx)};
-                const float wb{wt[2048 + raw]};
-                const int qb{quantize(jx_fma(-ytob, yq, br), qgsf, wb)};
-                ax = static_cast<std::int16_t>(qx);
-                ay = static_cast<std::int16_t>(qy);
-                ab = static_cast<std::int16_t>(qb);
+                const float2 xr{__half22float2(*reinterpret_cast<const __half2*>(coef + ci))};
+                const float2 yr{__half22float2(*reinterpret_cast<const __half2*>(coef + kCoefPlane + ci))};
+                const float2 br{__half22float2(*reinterpret_cast<const __half2*>(coef + 2 * kCoefPlane + ci))};
+                const float2 wx{*reinterpret_cast<const float2*>(wt + raw)};
+                const float2 wy{*reinterpret_cast<const float2*>(wt + 1024 + raw)};
+                const float2 wb{*reinterpret_cast<const float2*>(wt + 2048 + raw)};
+#pragma unroll
+                for (int h{0}; h < 2; ++h) {
+                    if (llf[h]) continue;
+                    const float wyh{h == 0 ? wy.x : wy.y};
+                    const int qy{quantize(h == 0 ? yr.x : yr.y, qgsf, wyh)};
+                    // A zero Y quantum reconstructs to a signed zero, and
+                    // fma(-m, +-0, v) equals v up to the sign of a zero
+                    // result, which quantises to 0 either way.
+                    const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wyh) / qgsf};
+                    const int qx{quantize(jx_fma(-ytox, yq, h == 0 ? xr.x : xr.y), qgsf, h == 0 ? wx.x : wx.y)};
+                    const int qb{quantize(jx_fma(-ytob, yq, h == 0 ? br.x : br.y), qgsf, h == 0 ? wb.x : wb.y)};
+                    ax[h] = static_cast<std::int16_t>(qx);
+                    ay[h] = static_cast<std::int16_t>(qy);
+                    ab[h] = static_cast<std::int16_t>(qb);
+                }
             }
             const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
-            out.ac[g] = ax;
-            out.ac[cplane + g] = ay;
-            out.ac[2 * cplane + g] = ab;
+            *reinterpret_cast<short2*>(out.ac + g) = make_short2(ax[0], ax[1]);
+            *reinterpret_cast<short2*>(out.ac + cplane + g) = make_short2(ay[0], ay[1]);
+            *reinterpret_cast<short2*>(out.ac + 2 * cplane + g) = make_short2(ab[0], ab[1]);
         }
         // Non-zero counts per first block: one shared-memory add per block
         // and channel per warp (lanes of a warp mostly share a block).
         const unsigned peers{__match_any_sync(0xffffffffu, f)};
         const bool leader{(__ffs(peers) - 1) == lane};
-        const unsigned mx{__ballot_sync(0xffffffffu, ax != 0) & peers};
-        const unsigned my{__ballot_sync(0xffffffffu, ay != 0) & peers};
-        const unsigned mb{__ballot_sync(0xffffffffu, ab != 0) & peers};
+        const int cx{__popc(__ballot_sync(0xffffffffu, ax[0] != 0) & peers) +
+                     __popc(__ballot_sync(0xffffffffu, ax[1] != 0) & peers)};
+        const int cy{__popc(__ballot_sync(0xffffffffu, ay[0] != 0) & peers) +
+                     __popc(__ballot_sync(0xffffffffu, ay[1] != 0) & peers)};
+        const int cb{__popc(__ballot_sync(0xffffffffu, ab[0] != 0) & peers) +
+                     __popc(__ballot_sync(0xffffffffu, ab[1] != 0) & peers)};
         if (leader && f >= 0) {
-            if (mx) atomicAdd(&sm.nz[0][f], __popc(mx));
-            if (my) atomicAdd(&sm.nz[1][f], __popc(my));
-            if (mb) atomicAdd(&sm.nz[2][f], __popc(mb));
+            if (cx) atomicAdd(&sm.nz[0][f], cx);
+            if (cy) atomicAdd(&sm.nz[1][f], cy);
+            if (cb) atomicAdd(&sm.nz[2][f], cb);
         }
     }
     __syncthreads();
