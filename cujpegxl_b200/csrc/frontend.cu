@@ -582,26 +582,46 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 
     // ---- 3. inverse gaborish, 5x5 with image-border clamping (src/frontend_transform.cu:19-36).
-    for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
-        const int c{i >> 12};
-        const int p{i & 4095};
-        const int x{p & 63};
-        const int y{p >> 6};
-        const float* P{xyb + c * kXplane + (y + kHalo) * kXs + x + kHalo};
-        auto at = [&](int dx, int dy) { return P[dy * kXs + dx]; };
-        const float e{((at(-1, 0) + at(1, 0)) + at(0, -1)) + at(0, 1)};
-        const float r2{((at(-2, 0) + at(2, 0)) + at(0, -2)) + at(0, 2)};
-        const float dg{((at(-1, -1) + at(1, -1)) + at(-1, 1)) + at(1, 1)};
-        const float l8{((((((at(-2, -1) + at(2, -1)) + at(-2, 1)) + at(2, 1)) + at(-1, -2)) +
-                         at(1, -2)) + at(-1, 2)) + at(1, 2)};
-        const float d4{((at(-2, -2) + at(2, -2)) + at(-2, 2)) + at(2, 2)};
-        float s{kGabC * at(0, 0)};
-        s = jx_fma(kGabEdge, e, s);
-        s = jx_fma(kGabEdge2, r2, s);
-        s = jx_fma(kGabDiag, dg, s);
-        s = jx_fma(kGabKnight, l8, s);
-        s = jx_fma(kGabDiag2, d4, s);
-        shp[c * kSplane + y * kSs + x] = s;
+    // Two horizontally adjacent outputs (x even) per thread on packed f32x2
+    // arithmetic: each source row's six samples x-2..x+3 come in as three
+    // aligned float2 loads (the row stride kXs and x + kHalo - 2 are even),
+    // and operand pair (dx, dy) is {row[x+dx], row[x+1+dx]}.
+    static_assert(kXs % 2 == 0 && kHalo % 2 == 0, "gaborish pairs");
+    for (int i2{tid}; i2 < 3 * kTile * kTile / 2; i2 += kThreads) {
+        const int c{i2 >> 11};
+        const int p2{i2 & 2047};
+        const int x{2 * (p2 & 31)};
+        const int y{p2 >> 5};
+        const float* P{xyb + c * kXplane + y * kXs + x};  // sample (x - 2, y - 2)
+        float2 row[5][5];  // row[dy + 2][dx + 2]
+#pragma unroll
+        for (int r{0}; r < 5; ++r) {
+            const float2 a{*reinterpret_cast<const float2*>(P + r * kXs)};
+            const float2 b{*reinterpret_cast<const float2*>(P + r * kXs + 2)};
+            const float2 d{*reinterpret_cast<const float2*>(P + r * kXs + 4)};
+            row[r][0] = a;
+            row[r][1] = make_float2(a.y, b.x);
+            row[r][2] = b;
+            row[r][3] = make_float2(b.y, d.x);
+            row[r][4] = d;
+        }
+        auto at = [&](int dx, int dy) { return row[dy + 2][dx + 2]; };
+        auto add = [](float2 u, float2 v) { return __fadd2_rn(u, v); };
+        const float2 e{add(add(add(at(-1, 0), at(1, 0)), at(0, -1)), at(0, 1))};
+        const float2 r2{add(add(add(at(-2, 0), at(2, 0)), at(0, -2)), at(0, 2))};
+        const float2 dg{add(add(add(at(-1, -1), at(1, -1)), at(-1, 1)), at(1, 1))};
+        const float2 l8{add(add(add(add(add(add(add(at(-2, -1), at(2, -1)), at(-2, 1)), at(2, 1)), at(-1, -2)),
+                                    at(1, -2)), at(-1, 2)), at(1, 2))};
+        const float2 d4{add(add(add(at(-2, -2), at(2, -2)), at(-2, 2)), at(2, 2))};
+        float2 s{__fmul2_rn(f2dup(kGabC), at(0, 0))};
+        s = __ffma2_rn(f2dup(kGabEdge), e, s);
+        s = __ffma2_rn(f2dup(kGabEdge2), r2, s);
+        s = __ffma2_rn(f2dup(kGabDiag), dg, s);
+        s = __ffma2_rn(f2dup(kGabKnight), l8, s);
+        s = __ffma2_rn(f2dup(kGabDiag2), d4, s);
+        float* o{shp + c * kSplane + y * kSs + x};  // odd rows are not 8-byte aligned (kSs is odd)
+        o[0] = s.x;
+        o[1] = s.y;
     }
     __syncthreads();
 
