@@ -513,36 +513,79 @@ __global__ void __launch_bounds__(kThreads, 2)
     // ---- 2. adaptive quantisation (src/frontend_fused.cu:233-342).
     const float* Y{xyb + kXplane};
     {
+        // Pixels (dx, dx + 1) of each cell row in pairs on packed f32x2
+        // arithmetic (the division and square root stay scalar); the sum
+        // still accumulates in raster order.
         const int ccx{tid & 15};
         const int ccy{tid >> 4};
+        const int ix0{ccx * 4 + kHalo};  // even: the float2 loads below are aligned
         float sum{0.0f};
+#pragma unroll
         for (int dy{0}; dy < 4; ++dy) {
-            for (int dx{0}; dx < 4; ++dx) {
-                const int ix{ccx * 4 + dx + kHalo};
-                const int iy{ccy * 4 + dy + kHalo};
-                const float yv{Y[iy * kXs + ix]};
-                const float base{0.25f * (((Y[(iy + 1) * kXs + ix] + Y[(iy - 1) * kXs + ix]) +
-                                          Y[iy * kXs + ix - 1]) +
-                                         Y[iy * kXs + ix + 1])};
-                float d{ratio_gamma<false>(yv + kMatchGammaOffset) * (yv - base)};
-                d = d * d;
-                d = fminf(d, kDiffLimit);
-                sum = sum + masking_sqrt(d, sc.mask_sqrt_mul);
+            const int iy{ccy * 4 + dy + kHalo};
+            const float* C{Y + iy * kXs + ix0};
+            const float* U{C - kXs};
+            const float* D{C + kXs};
+            const float2 c0{*reinterpret_cast<const float2*>(C - 2)};  // ix0-2, ix0-1
+            const float2 c1{*reinterpret_cast<const float2*>(C)};      // ix0, ix0+1
+            const float2 c2{*reinterpret_cast<const float2*>(C + 2)};  // ix0+2, ix0+3
+            const float2 c3{*reinterpret_cast<const float2*>(C + 4)};  // ix0+4, ix0+5
+            const float2 up[2]{*reinterpret_cast<const float2*>(U), *reinterpret_cast<const float2*>(U + 2)};
+            const float2 dn[2]{*reinterpret_cast<const float2*>(D), *reinterpret_cast<const float2*>(D + 2)};
+            const float2 ctr[2]{c1, c2};
+            const float2 lft[2]{make_float2(c0.y, c1.x), make_float2(c1.y, c2.x)};
+            const float2 rgt[2]{make_float2(c1.y, c2.x), make_float2(c2.y, c3.x)};
+#pragma unroll
+            for (int h{0}; h < 2; ++h) {
+                const float2 yv{ctr[h]};
+                const float2 base{__fmul2_rn(
+                    f2dup(0.25f), __fadd2_rn(__fadd2_rn(__fadd2_rn(dn[h], up[h]), lft[h]), rgt[h]))};
+                // ratio_gamma<false>(yv + kMatchGammaOffset)
+                float2 v{__fadd2_rn(yv, f2dup(kMatchGammaOffset))};
+                v = make_float2(v.x < 0.0f ? 0.0f : v.x, v.y < 0.0f ? 0.0f : v.y);
+                const float2 v2{__fmul2_rn(v, v)};
+                const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
+                const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
+                const float2 ratio{den.x / num.x, den.y / num.y};
+                float2 d{__fmul2_rn(ratio, __fadd2_rn(yv, f2neg(base)))};
+                d = __fmul2_rn(d, d);
+                d = make_float2(fminf(d.x, kDiffLimit), fminf(d.y, kDiffLimit));
+                // masking_sqrt(d, mask_sqrt_mul)
+                const float2 t{__ffma2_rn(d, f2dup(sc.mask_sqrt_mul), f2dup(kMaskLogOffset))};
+                const float2 m{__fmul2_rn(f2dup(0.25f), make_float2(sqrtf(t.x), sqrtf(t.y)))};
+                sum = sum + m.x;
+                sum = sum + m.y;
             }
         }
         sm.pre[tid] = 0.25f * sum;
     }
     __syncthreads();
+    // The four eroded cells of each of this warp's 8 blocks (block warp + 8j),
+    // one per lane: lane 4j + k holds cell k = (k & 1, k >> 1) of block j's
+    // 2x2 cells. Their sum (e0 + e2) + (e1 + e3) is the order in which a
+    // 32-lane tree with the cells in lanes 0-3 and zeros elsewhere adds them.
+    float ero_sum;
+    {
+        const int lb{warp + 8 * (lane >> 2)};
+        const int k{lane & 3};
+        const int lbx{lb & 7};
+        const int lby{lb >> 3};
+        const float e{erosion_cell(sm.pre, (lbx >> 2) * 8, (lby >> 2) * 8, 2 * (lbx & 3) + (k & 1),
+                                   2 * (lby & 3) + (k >> 1), sc.km0, sc.km1, sc.km2, sc.km3)};
+        const float s{e + __shfl_down_sync(0xffffffffu, e, 2)};
+        ero_sum = s + __shfl_down_sync(0xffffffffu, s, 1);
+    }
     for (int lb{warp}; lb < 64; lb += kThreads / 32) {
         const int lbx{lb & 7};
         const int lby{lb >> 3};
         const int gbx{bx0 + lbx};
         const int gby{by0 + lby};
+        const float eroded{__shfl_sync(0xffffffffu, ero_sum, 4 * (lb >> 3))};
         if (gbx >= bw || gby >= bh || ((qmask >> region_of_block(lb)) & 1u) != 0) {
             continue;  // warp-uniform
         }
         const int fx{lane & 7};
-        float red[2][4];
+        float red[2][3];
         for (int half{0}; half < 2; ++half) {
             const int fy{(lane >> 3) + 4 * half};
             const int ix{lbx * 8 + fx + kHalo};
@@ -561,23 +604,19 @@ __global__ void __launch_bounds__(kThreads, 2)
             const float gp{ratio_gamma<true>(iny - xv) + ratio_gamma<true>(iny + xv)};
             const float pye{(yv + kBlueOffset) + fabsf(xv)};
             const float bp{bv > pye ? fminf(bv - pye, kBlueLimit) : 0.0f};
-            float er{0.0f};
-            if (half == 0 && lane < 4) {
-                er = erosion_cell(sm.pre, (lbx >> 2) * 8, (lby >> 2) * 8, 2 * (lbx & 3) + (lane & 1),
-                                  2 * (lby & 3) + (lane >> 1), sc.km0, sc.km1, sc.km2, sc.km3);
-            }
             red[half][0] = warp_tree(hf);
             red[half][1] = warp_tree(gp);
             red[half][2] = warp_tree(bp);
-            red[half][3] = warp_tree(er);
         }
         if (lane == 0) {
             // The block's quant field is finished from these sums by its own
-            // thread in step 4e, where most warps are otherwise idle.
+            // thread in step 4e, where most warps are otherwise idle. The
+            // eroded sum gets the second half's tree of zeros added, as the
+            // per-half reduction did.
             sm.aq_sums[0][lb] = red[0][0] + red[1][0];
             sm.aq_sums[1][lb] = red[0][1] + red[1][1];
             sm.aq_sums[2][lb] = red[0][2] + red[1][2];
-            sm.aq_sums[3][lb] = red[0][3] + red[1][3];
+            sm.aq_sums[3][lb] = eroded + 0.0f;
         }
     }
 

@@ -85,7 +85,11 @@ __device__ __forceinline__ void xyb_pixel(int luma, const std::uint8_t* win, int
 __device__ __forceinline__ float2 f2dup(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 f2neg(float2 v) { return make_float2(-v.x, -v.y); }
 
-// jx_pow24 on both components.
+// jx_pow24 on both components, for x in [2^-5, 2): the exponent k is then in
+// [-5, 0], so floor(k / 5) is -1 for k < 0 and 0 for k = 0, and the factors
+// c = 2^(0.4 r) and 2^(2 floor(k / 5)) are those jx_pow24 computes. The sRGB
+// transfer only calls it on (e + 0.055) / 1.055 with e in [0, 1], which lies
+// in [0.052, 1.0000002].
 __device__ __forceinline__ float2 jx_pow24_2(float2 x) {
     float2 m, c, scale;
     {
@@ -95,13 +99,12 @@ __device__ __forceinline__ float2 jx_pow24_2(float2 x) {
         for (int h{0}; h < 2; ++h) {
             const int k{static_cast<int>((u[h] >> 23) & 0xffu) - 127};
             mm[h] = u2f((u[h] & 0x7fffffu) | 0x3f800000u);
-            const int q{(k >= 0 ? k : k - 4) / 5};
-            const int r{k - 5 * q};
+            const int r{k < 0 ? k + 5 : k};
             cc[h] = r == 0 ? 1.0f
                            : (r == 1 ? 1.31950791077289425f
                                      : (r == 2 ? 1.74110112659224828f
                                                : (r == 3 ? 2.29739670999407037f : 3.03143313302079624f)));
-            ss[h] = u2f(static_cast<std::uint32_t>(2 * q + 127) << 23);
+            ss[h] = k < 0 ? 0.25f : 1.0f;
         }
         m = make_float2(mm[0], mm[1]);
         c = make_float2(cc[0], cc[1]);
