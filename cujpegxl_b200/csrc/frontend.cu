@@ -33,7 +33,9 @@ constexpr int kTile = 64;
 constexpr int kHalo = 2;
 constexpr int kXs = kTile + 2 * kHalo;  // 68: stride of the unsharpened XYB tile
 constexpr int kXplane = kXs * kXs;
-constexpr int kSs = kTile + 1;          // 65: stride of the sharpened tile
+// 68: stride of the sharpened tile, a multiple of 4 floats so that every
+// block row starts 16-byte aligned for the DCT passes' vector loads.
+constexpr int kSs = kTile + 4;
 constexpr int kSplane = kTile * kSs;
 constexpr int kRegionAFloats = 3 * kXplane;  // 13872
 // FP16 coefficients of the tile in region A: 64 covered-block slots per block,
@@ -43,6 +45,13 @@ constexpr int kCoefBlock = 66;
 constexpr int kCoefPlane = 64 * kCoefBlock;
 constexpr int kDrowsOffset = 3 * kCoefPlane / 2;  // floats
 static_assert(kDrowsOffset + 64 * 72 <= kRegionAFloats, "final-DCT scratch exceeds region A");
+// Row stride of one first block's row-pass output in the final-DCT scratch:
+// 36 for DCT32 (16-byte aligned rows for the column pass's vector loads; one
+// block per warp, so lanes stay on distinct banks), N + 1 for DCT16 and DCT8,
+// whose warps span several blocks. Each 32x32 region then needs at most
+// 32 * 36 = 16 * 8 * 9 floats, so the scratch bound above still holds.
+template <int N>
+constexpr int kDrowsStride = N == 32 ? 36 : N + 1;
 
 // Selection bases: double-precision DCT-II basis narrowed to float
 // (basis[k*n + t], src/transform_select.cu:29-37). Final-DCT bases: the float
@@ -208,13 +217,21 @@ __device__ __forceinline__ float warp_tree(float v) {
 // one pixel row. Selection bases accumulate without FMA (the host twin's
 // arithmetic); final-DCT bases accumulate with FMA. Coefficients fx and fx+1
 // share each packed instruction; each is its own chain in c order.
+// src is 16-byte aligned (block rows of the sharpened planes are). The
+// outputs of frequency fx go to dst[fx * stride]: stride N + 1 for the
+// selection scratch, kDrowsStride<N> for the final DCT.
 template <int N, int F0, int F1, bool kSel>
 __device__ __forceinline__ void row_pass(const float* src, float* dst) {
     static_assert(F0 % 2 == 0 && F1 % 2 == 0, "pairs of frequencies");
+    constexpr int kStride{kSel ? N + 1 : kDrowsStride<N>};
     float2 p[N];
 #pragma unroll
-    for (int c{0}; c < N; ++c) {
-        p[c] = dup2(src[c]);
+    for (int c{0}; c < N; c += 4) {
+        const float4 v{*reinterpret_cast<const float4*>(src + c)};
+        p[c] = dup2(v.x);
+        p[c + 1] = dup2(v.y);
+        p[c + 2] = dup2(v.z);
+        p[c + 3] = dup2(v.w);
     }
 #pragma unroll
     for (int fx{F0}; fx < F1; fx += 2) {
@@ -227,8 +244,8 @@ __device__ __forceinline__ void row_pass(const float* src, float* dst) {
                 s = __ffma2_rn(basis2<N, false>((fx >> 1) * N + c), p[c], s);
             }
         }
-        dst[fx * (N + 1)] = s.x;
-        dst[(fx + 1) * (N + 1)] = s.y;
+        dst[fx * kStride] = s.x;
+        dst[(fx + 1) * kStride] = s.y;
     }
 }
 
@@ -305,9 +322,21 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
                                         int fby) {
     static_assert(Y0 % 2 == 0 && Y1 % 2 == 0, "pairs of frequencies");
     float2 rr[N];
+    if constexpr (kDrowsStride<N> % 4 == 0) {
+        // 16-byte aligned rows: four samples per load.
 #pragma unroll
-    for (int r{0}; r < N; ++r) {
-        rr[r] = dup2(rows_fx[r]);
+        for (int r{0}; r < N; r += 4) {
+            const float4 v{*reinterpret_cast<const float4*>(rows_fx + r)};
+            rr[r] = dup2(v.x);
+            rr[r + 1] = dup2(v.y);
+            rr[r + 2] = dup2(v.z);
+            rr[r + 3] = dup2(v.w);
+        }
+    } else {
+#pragma unroll
+        for (int r{0}; r < N; ++r) {
+            rr[r] = dup2(rows_fx[r]);
+        }
     }
     constexpr int side{N / 8};
 #pragma unroll
@@ -423,13 +452,17 @@ __global__ void __launch_bounds__(kThreads, 2)
     {
         const int cw{W >> 1};
         const int ch{H >> 1};
-        for (int i{tid}; i < kLog2Cached; i += kThreads) sm.log2_small[i] = tb.log2_1p[i];
+        // The rate-table entry and the learned class are loaded here and
+        // stored after the window, so that their latency overlaps the
+        // window's.
+        static_assert(kLog2Cached == kThreads, "one cached rate-table entry per thread");
+        const float log2_entry{tb.log2_1p[tid]};
+        signed char net_entry{-1};
         if (tid < 4) {
             const int rw{(bw + 3) >> 2};
             const int rx{2 * tx + (tid & 1)};
             const int ry{2 * ty + (tid >> 1)};
-            sm.net[tid] = in.net_class != nullptr && rx < rw && ry < ((bh + 3) >> 2) ? in.net_class[ry * rw + rx]
-                                                                                    : static_cast<signed char>(-1);
+            if (in.net_class != nullptr && rx < rw && ry < ((bh + 3) >> 2)) net_entry = in.net_class[ry * rw + rx];
         }
         // Interior tiles whose window needs no clamping, with 4-byte aligned
         // rows, load whole 32-bit words: luma bytes px0-4 .. px0+67 of each
@@ -437,39 +470,92 @@ __global__ void __launch_bounds__(kThreads, 2)
         // (bytes px0-4 .. px0+67, word aligned).
         const bool aligned{((reinterpret_cast<std::uintptr_t>(in.luma) | in.luma_pitch |
                              reinterpret_cast<std::uintptr_t>(in.chroma) | in.chroma_pitch) & 3u) == 0};
+        // Each thread issues all of its loads before its first shared-memory
+        // store, so that it waits for one memory latency rather than one per
+        // loop iteration.
         if (aligned && px0 >= 4 && py0 >= 4 && px0 + 68 <= W && py0 + 68 <= H) {
             constexpr int kLumaWords{kXs / 4};        // 17 output words per luma row
             constexpr int kChromaWords{kChromaWin / 2};  // 18 words per chroma row
-            auto* lw{reinterpret_cast<std::uint32_t*>(win_luma)};
-            for (int i{tid}; i < kXs * kLumaWords; i += kThreads) {
-                const int row{i / kLumaWords};
-                const int w{i - row * kLumaWords};
-                const auto* src{reinterpret_cast<const std::uint32_t*>(
-                    in.luma + static_cast<std::size_t>(py0 - kHalo + row) * in.luma_pitch + px0 - 4)};
-                lw[row * kLumaWords + w] = __funnelshift_r(__ldg(&src[w]), __ldg(&src[w + 1]), 16);
+            constexpr int kLumaItems{kXs * kLumaWords};
+            constexpr int kChromaItems{kChromaWin * kChromaWords};
+            constexpr int kLumaPer{(kLumaItems + kThreads - 1) / kThreads};
+            constexpr int kChromaPer{(kChromaItems + kThreads - 1) / kThreads};
+            std::uint32_t lo[kLumaPer], hi[kLumaPer], cv[kChromaPer];
+#pragma unroll
+            for (int j{0}; j < kLumaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kLumaItems) {
+                    const int row{i / kLumaWords};
+                    const int w{i - row * kLumaWords};
+                    const auto* src{reinterpret_cast<const std::uint32_t*>(
+                        in.luma + static_cast<std::size_t>(py0 - kHalo + row) * in.luma_pitch + px0 - 4)};
+                    lo[j] = __ldg(&src[w]);
+                    hi[j] = __ldg(&src[w + 1]);
+                }
+            }
+#pragma unroll
+            for (int j{0}; j < kChromaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kChromaItems) {
+                    const int row{i / kChromaWords};
+                    const int w{i - row * kChromaWords};
+                    const auto* src{reinterpret_cast<const std::uint32_t*>(
+                        in.chroma + static_cast<std::size_t>(cy0 + row) * in.chroma_pitch + 2 * cx0)};
+                    cv[j] = __ldg(&src[w]);
+                }
+            }
+            auto* lw{reinterpret_cast<std::uint32_t*>(win_luma)};  // word i = row * kLumaWords + w
+#pragma unroll
+            for (int j{0}; j < kLumaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kLumaItems) lw[i] = __funnelshift_r(lo[j], hi[j], 16);
             }
             auto* cwd{reinterpret_cast<std::uint32_t*>(win_chroma)};
-            for (int i{tid}; i < kChromaWin * kChromaWords; i += kThreads) {
-                const int row{i / kChromaWords};
-                const int w{i - row * kChromaWords};
-                const auto* src{reinterpret_cast<const std::uint32_t*>(
-                    in.chroma + static_cast<std::size_t>(cy0 + row) * in.chroma_pitch + 2 * cx0)};
-                cwd[row * kChromaWords + w] = __ldg(&src[w]);
+#pragma unroll
+            for (int j{0}; j < kChromaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kChromaItems) cwd[i] = cv[j];
             }
         } else {
-            for (int i{tid}; i < kXplane; i += kThreads) {
-                const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
-                const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
-                win_luma[i] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
+            constexpr int kLumaPer{(kXplane + kThreads - 1) / kThreads};
+            constexpr int kChromaPer{(kChromaWin * kChromaWin + kThreads - 1) / kThreads};
+            std::uint8_t lv[kLumaPer], cb[kChromaPer], cr[kChromaPer];
+#pragma unroll
+            for (int j{0}; j < kLumaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kXplane) {
+                    const int gx{min(max(px0 - kHalo + i % kXs, 0), W - 1)};
+                    const int gy{min(max(py0 - kHalo + i / kXs, 0), H - 1)};
+                    lv[j] = in.luma[static_cast<std::size_t>(gy) * in.luma_pitch + gx];
+                }
             }
-            for (int i{tid}; i < kChromaWin * kChromaWin; i += kThreads) {
-                const int jx{min(max(cx0 + i % kChromaWin, 0), cw - 1)};
-                const int jy{min(max(cy0 + i / kChromaWin, 0), ch - 1)};
-                const std::uint8_t* p{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
-                win_chroma[2 * i] = p[0];
-                win_chroma[2 * i + 1] = p[1];
+#pragma unroll
+            for (int j{0}; j < kChromaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kChromaWin * kChromaWin) {
+                    const int jx{min(max(cx0 + i % kChromaWin, 0), cw - 1)};
+                    const int jy{min(max(cy0 + i / kChromaWin, 0), ch - 1)};
+                    const std::uint8_t* p{in.chroma + static_cast<std::size_t>(jy) * in.chroma_pitch + 2 * jx};
+                    cb[j] = p[0];
+                    cr[j] = p[1];
+                }
+            }
+#pragma unroll
+            for (int j{0}; j < kLumaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kXplane) win_luma[i] = lv[j];
+            }
+#pragma unroll
+            for (int j{0}; j < kChromaPer; ++j) {
+                const int i{tid + j * kThreads};
+                if (i < kChromaWin * kChromaWin) {
+                    win_chroma[2 * i] = cb[j];
+                    win_chroma[2 * i + 1] = cr[j];
+                }
             }
         }
+        sm.log2_small[tid] = log2_entry;
+        if (tid < 4) sm.net[tid] = net_entry;
     }
     __syncthreads();
     // Regions whose transform split (and, with net_qf, quant field) the
@@ -658,9 +744,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         s = __ffma2_rn(f2dup(kGabDiag), dg, s);
         s = __ffma2_rn(f2dup(kGabKnight), l8, s);
         s = __ffma2_rn(f2dup(kGabDiag2), d4, s);
-        float* o{shp + c * kSplane + y * kSs + x};  // odd rows are not 8-byte aligned (kSs is odd)
-        o[0] = s.x;
-        o[1] = s.y;
+        *reinterpret_cast<float2*>(shp + c * kSplane + y * kSs + x) = s;
     }
     __syncthreads();
 
@@ -983,7 +1067,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
         for (int g{0}; g < 3; ++g) {
             const int s{32 >> g};
-            const int step{s * (s + 1)};
+            const int step{s * (s + (s == 32 ? 4 : 1))};  // row strides 36, 17, 9 (kDrowsStride)
             const unsigned m0{__ballot_sync(0xffffffffu, side[0] == s)};
             const unsigned m1{__ballot_sync(0xffffffffu, side[1] == s)};
             const int c0{__popc(m0)};
@@ -1083,7 +1167,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const int f{k >> 6};
                 const int lb{sm.fb_list[f]};
                 const int fx{k & 31};
-                const float* src{drows + sm.fb_off[f] + fx * 33};
+                const float* src{drows + sm.fb_off[f] + fx * kDrowsStride<32>};
                 if (k & 32) {
                     dct_col<32, 16, 32>(src, cc, fx, lb & 7, lb >> 3);
                 } else {
