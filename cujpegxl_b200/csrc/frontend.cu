@@ -355,9 +355,25 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
     }
 }
 
+// Mixed-precision forms (sm_100): the FP16 operands are widened exactly inside
+// the instruction, so fma_f16(a, b, c) is fmaf(float(a), float(b), c) and
+// add_f16(a, c) is float(a) + c, each rounded once, without separate
+// conversions.
+__device__ __forceinline__ float fma_f16(unsigned short a, unsigned short b, float c) {
+    float d;
+    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(a), "h"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float add_f16(unsigned short a, float c) {
+    float d;
+    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(a), "f"(c));
+    return d;
+}
+
 // One CfL sum of a side-N first block lb over its non-LLF coefficients in raw
 // order, as the reference accumulates it (src/frontend_quantize.cu:63-74):
-// kWhich 0 sums x*y, 1 sums y*y and 2 sums (b - y)*y, each an FMA chain. The
+// kWhich 0 sums x*y, 1 sums y*y and 2 sums (b - y)*y, each an FMA chain of
+// float(a) * float(y) + acc (kinds 0 and 1 on the FP16 operands directly). The
 // chain is sequential; its loads are issued ahead in groups of 16 slots. An
 // LLF slot contributes fma(0, y, acc) instead of being skipped: that adds an
 // exact zero, which can change only the sign of a zero sum, and the quantised
@@ -372,34 +388,34 @@ __device__ __forceinline__ float cfl_sum(const __half* coef, int lb) {
 #pragma unroll 1
     for (int q{0}; q < kSide * kSide; ++q) {
         const int l{lb + (q / kSide) * 8 + q % kSide};
-        const __half2* py{reinterpret_cast<const __half2*>(coef + kCoefPlane + l * kCoefBlock)};
-        const __half2* po{reinterpret_cast<const __half2*>(coef + (kWhich == 2 ? 2 * kCoefPlane : 0) +
-                                                           l * kCoefBlock)};
+        const std::uint32_t* py{reinterpret_cast<const std::uint32_t*>(coef + kCoefPlane + l * kCoefBlock)};
+        const std::uint32_t* po{reinterpret_cast<const std::uint32_t*>(coef + (kWhich == 2 ? 2 * kCoefPlane : 0) +
+                                                                       l * kCoefBlock)};
         const std::uint64_t skip{q < kQLlf ? kLlf : 0ull};
 #pragma unroll
         for (int c{0}; c < 4; ++c) {
-            float2 y[8];
-            float2 o[8];
+            std::uint32_t y[8];
+            std::uint32_t o[8];
 #pragma unroll
             for (int j{0}; j < 8; ++j) {
-                y[j] = __half22float2(py[c * 8 + j]);
-                if (kWhich != 1) o[j] = __half22float2(po[c * 8 + j]);
+                y[j] = py[c * 8 + j];
+                if (kWhich != 1) o[j] = po[c * 8 + j];
             }
 #pragma unroll
             for (int j{0}; j < 16; ++j) {
-                const float yr{(j & 1) ? y[j >> 1].y : y[j >> 1].x};
-                float a;
-                if (kWhich == 0) {
-                    a = (j & 1) ? o[j >> 1].y : o[j >> 1].x;
-                } else if (kWhich == 1) {
-                    a = yr;
+                const int sh{(j & 1) * 16};
+                const auto yh{static_cast<unsigned short>(y[j >> 1] >> sh)};
+                const bool llf{((kLlf >> (16 * c + j)) & 1ull) != 0 && ((skip >> (16 * c + j)) & 1ull) != 0};
+                if (kWhich == 2) {
+                    const float yr{__half2float(__ushort_as_half(yh))};
+                    float a{add_f16(static_cast<unsigned short>(o[j >> 1] >> sh), -yr)};
+                    if (((kLlf >> (16 * c + j)) & 1ull) != 0) a = llf ? 0.0f : a;
+                    acc = jx_fma(a, yr, acc);
                 } else {
-                    a = ((j & 1) ? o[j >> 1].y : o[j >> 1].x) - yr;
+                    auto ah{kWhich == 0 ? static_cast<unsigned short>(o[j >> 1] >> sh) : yh};
+                    if (((kLlf >> (16 * c + j)) & 1ull) != 0) ah = llf ? static_cast<unsigned short>(0) : ah;
+                    acc = fma_f16(ah, yh, acc);
                 }
-                if (((kLlf >> (16 * c + j)) & 1ull) != 0) {
-                    a = ((skip >> (16 * c + j)) & 1ull) != 0 ? 0.0f : a;
-                }
-                acc = jx_fma(a, yr, acc);
             }
         }
     }
