@@ -422,6 +422,51 @@ __device__ __forceinline__ float cfl_sum(const __half* coef, int lb) {
     return acc;
 }
 
+// DC of the 8x8 position (ox, oy) of a first block f of side 8M from its
+// MxM low-frequency corner, per channel, in double as the host twin computes
+// it (src/vardct_layout.h:88-111): the sum over fx, then fy, of
+// (((ob[fx][ox] * ob[fy][oy]) * c) * s[fx]) * s[fy], times M. The basis
+// product does not depend on the channel, so it is formed once for all three
+// (the same rounded value each channel would form).
+template <int M>
+__device__ __forceinline__ void llf_to_dc(const __half* coef, int f, int ox, int oy, const double* ob,
+                                          float dcv[3]) {
+    constexpr int kN{8 * M};
+    constexpr double kS16[2]{1.0, 0.901764195028874394};
+    constexpr double kS32[4]{1.0, 0.974886821136879522, 0.901764195028874394, 0.787054918159101335};
+    double bx[M];
+    double by[M];
+#pragma unroll
+    for (int i{0}; i < M; ++i) {
+        bx[i] = ob[i * 4 + ox];
+        by[i] = ob[i * 4 + oy];
+    }
+    double ab[M][M];
+#pragma unroll
+    for (int fx{0}; fx < M; ++fx) {
+#pragma unroll
+        for (int fy{0}; fy < M; ++fy) ab[fx][fy] = bx[fx] * by[fy];
+    }
+#pragma unroll
+    for (int c{0}; c < 3; ++c) {
+        double sum{0.0};
+#pragma unroll
+        for (int fx{0}; fx < M; ++fx) {
+#pragma unroll
+            for (int fy{0}; fy < M; ++fy) {
+                const int raw{fx * kN + fy};
+                const int q{raw >> 6};
+                const int blk{f + (q >> (M >> 1)) * 8 + (q & (M - 1))};
+                const double cv{__half2float(coef[c * kCoefPlane + blk * kCoefBlock + (raw & 63)])};
+                const double sx{M == 2 ? kS16[fx] : kS32[fx]};
+                const double sy{M == 2 ? kS16[fy] : kS32[fy]};
+                sum = sum + ((ab[fx][fy] * cv) * sx) * sy;
+            }
+        }
+        dcv[c] = static_cast<float>(static_cast<double>(M) * sum);
+    }
+}
+
 // The three sums of every first block of side N, sum kind `which` per warp
 // and one first block per lane (list entries first..first+count-1).
 template <int N>
@@ -1246,25 +1291,10 @@ __global__ void __launch_bounds__(kThreads, 2)
                 for (int c{0}; c < 3; ++c) {
                     dcv[c] = __half2float(coef[c * kCoefPlane + f * kCoefBlock]);
                 }
+            } else if (m == 2) {
+                llf_to_dc<2>(coef, f, ox, oy, tb.llf_basis, dcv);
             } else {
-                const double* ob{tb.llf_basis + (m == 2 ? 0 : 16)};
-                const double s16[2]{1.0, 0.901764195028874394};
-                const double s32[4]{1.0, 0.974886821136879522, 0.901764195028874394,
-                                    0.787054918159101335};
-                const double* scl{m == 2 ? s16 : s32};
-                for (int c{0}; c < 3; ++c) {
-                    double sum{0.0};
-                    for (int fx{0}; fx < m; ++fx) {
-                        for (int fy{0}; fy < m; ++fy) {
-                            const int raw{fx * n + fy};
-                            const int q{raw >> 6};
-                            const double cv{__half2float(
-                                coef[c * kCoefPlane + (f + (q >> (m >> 1)) * 8 + (q & (m - 1))) * kCoefBlock + (raw & 63)])};
-                            sum = sum + ob[fx * 4 + ox] * ob[fy * 4 + oy] * cv * scl[fx] * scl[fy];
-                        }
-                    }
-                    dcv[c] = static_cast<float>(static_cast<double>(m) * sum);
-                }
+                llf_to_dc<4>(coef, f, ox, oy, tb.llf_basis + 16, dcv);
             }
             const float dcq_x{4096.0f * sc.dc_scale};
             const float dcq_y{512.0f * sc.dc_scale};
