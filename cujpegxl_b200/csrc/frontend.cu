@@ -98,6 +98,7 @@ struct Small {
     int n32, n16, n8;
     int mx, mb;
     signed char net[4];   // learned split class of each 32x32 region, -1 = RD heuristic
+    float2 pow_lut[6];    // factor table of jx_pow24_2, for the packed sRGB transfer
 };
 
 // Region (0..3, raster) of the tile that holds tile block lb.
@@ -617,6 +618,10 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         sm.log2_small[tid] = log2_entry;
         if (tid < 4) sm.net[tid] = net_entry;
+#pragma unroll
+        for (int k{0}; k < 6; ++k) {
+            if (tid == k) sm.pow_lut[k] = make_float2(pow24_factor_c(k), pow24_factor_scale(k));
+        }
     }
     __syncthreads();
     // Regions whose transform split (and, with net_qf, quant field) the
@@ -637,7 +642,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int gx1{min(max(px0 - kHalo + col + 1, 0), W - 1)};
         const int gy{min(max(py0 - kHalo + row, 0), H - 1)};
         float2 x, y, b;
-        xyb_pixel2<kChromaWin>(win_luma[i], win_luma[i + 1], win_chroma, cx0, cy0, gx0, gx1, gy, W, H, x, y, b);
+        xyb_pixel2<kChromaWin>(win_luma[i], win_luma[i + 1], win_chroma, cx0, cy0, gx0, gx1, gy, W, H, sm.pow_lut,
+                               x, y, b);
         *reinterpret_cast<float2*>(xyb + i) = x;
         *reinterpret_cast<float2*>(xyb + kXplane + i) = y;
         *reinterpret_cast<float2*>(xyb + 2 * kXplane + i) = b;

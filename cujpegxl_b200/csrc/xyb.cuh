@@ -85,26 +85,31 @@ __device__ __forceinline__ void xyb_pixel(int luma, const std::uint8_t* win, int
 __device__ __forceinline__ float2 f2dup(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 f2neg(float2 v) { return make_float2(-v.x, -v.y); }
 
-// jx_pow24 on both components, for x in [2^-5, 2): the exponent k is then in
-// [-5, 0], so floor(k / 5) is -1 for k < 0 and 0 for k = 0, and the factors
-// c = 2^(0.4 r) and 2^(2 floor(k / 5)) are those jx_pow24 computes. The sRGB
-// transfer only calls it on (e + 0.055) / 1.055 with e in [0, 1], which lies
-// in [0.052, 1.0000002].
-__device__ __forceinline__ float2 jx_pow24_2(float2 x) {
+// The factors jx_pow24 derives from the exponent, for x in [2^-5, 2), by
+// exponent byte e - 122 (e in 122..127, k = e - 127 in [-5, 0]):
+// {c = 2^(0.4 r), 2^(2 floor(k / 5))} with r = k - 5 floor(k / 5).
+__host__ __device__ constexpr float pow24_factor_c(int i) {
+    return i == 1 ? 1.31950791077289425f
+                  : (i == 2 ? 1.74110112659224828f
+                            : (i == 3 ? 2.29739670999407037f : (i == 4 ? 3.03143313302079624f : 1.0f)));
+}
+__host__ __device__ constexpr float pow24_factor_scale(int i) { return i == 5 ? 1.0f : 0.25f; }
+
+// jx_pow24 on both components, for x in [2^-5, 2); lut[i] = {pow24_factor_c(i), pow24_factor_scale(i)}
+// (a shared-memory copy: one 8-byte load per component replaces the
+// exponent arithmetic). The sRGB transfer only calls it on (e + 0.055) / 1.055
+// with e in [0, 1], which lies in [0.052, 1.0000002].
+__device__ __forceinline__ float2 jx_pow24_2(float2 x, const float2* lut) {
     float2 m, c, scale;
     {
         const std::uint32_t u[2]{f2u(x.x), f2u(x.y)};
         float mm[2], cc[2], ss[2];
 #pragma unroll
         for (int h{0}; h < 2; ++h) {
-            const int k{static_cast<int>((u[h] >> 23) & 0xffu) - 127};
             mm[h] = u2f((u[h] & 0x7fffffu) | 0x3f800000u);
-            const int r{k < 0 ? k + 5 : k};
-            cc[h] = r == 0 ? 1.0f
-                           : (r == 1 ? 1.31950791077289425f
-                                     : (r == 2 ? 1.74110112659224828f
-                                               : (r == 3 ? 2.29739670999407037f : 3.03143313302079624f)));
-            ss[h] = k < 0 ? 0.25f : 1.0f;
+            const float2 f{lut[static_cast<int>(u[h] >> 23) - 122]};
+            cc[h] = f.x;
+            ss[h] = f.y;
         }
         m = make_float2(mm[0], mm[1]);
         c = make_float2(cc[0], cc[1]);
@@ -142,10 +147,11 @@ __device__ __forceinline__ float2 jx_cbrt2(float2 x) {
 
 __device__ __forceinline__ float2 clamp01_2(float2 v) { return make_float2(clamp01(v.x), clamp01(v.y)); }
 
-// srgb_to_linear on both components (both branches evaluated, one kept).
-__device__ __forceinline__ float2 srgb_to_linear2(float2 e) {
+// srgb_to_linear on both components (both branches evaluated, one kept),
+// for e in [0, 1].
+__device__ __forceinline__ float2 srgb_to_linear2(float2 e, const float2* lut) {
     const float2 lin{__fmul2_rn(e, f2dup(1.0f / 12.92f))};
-    const float2 pw{jx_pow24_2(__fmul2_rn(__fadd2_rn(e, f2dup(0.055f)), f2dup(1.0f / 1.055f)))};
+    const float2 pw{jx_pow24_2(__fmul2_rn(__fadd2_rn(e, f2dup(0.055f)), f2dup(1.0f / 1.055f)), lut)};
     return make_float2(e.x <= 0.04045f ? lin.x : pw.x, e.y <= 0.04045f ? lin.y : pw.y);
 }
 
@@ -178,11 +184,13 @@ __device__ __forceinline__ float2 div4080_2(int s0, int s1) {
 }
 
 // xyb_pixel for pixels (gx0, gy) and (gx1, gy) of one row: component 0 of
-// each output is the first pixel, component 1 the second.
+// each output is the first pixel, component 1 the second. lut: the factor
+// table of jx_pow24_2. The window's (cb, cr) pairs start at even
+// byte offsets.
 template <int kWin>
 __device__ __forceinline__ void xyb_pixel2(int luma0, int luma1, const std::uint8_t* win, int cx0, int cy0, int gx0,
-                                           int gx1, int gy, int width, int height, float2& ox, float2& oy,
-                                           float2& ob) {
+                                           int gx1, int gy, int width, int height, const float2* lut, float2& ox,
+                                           float2& oy, float2& ob) {
     const float2 yv{__fmul2_rn(make_float2(static_cast<float>(luma0), static_cast<float>(luma1)), f2dup(kInv255))};
     const int cw{width >> 1};
     const int ch{height >> 1};
@@ -194,15 +202,34 @@ __device__ __forceinline__ void xyb_pixel2(int luma0, int luma1, const std::uint
         ya = max(jy - 1, 0); yb = jy; wya = 1; wyb = 3;
     }
     int scb0, scr0, scb1, scr1;
-    chroma_taps<kWin>(win, cx0, cy0, gx0, cw, ya, yb, wya, wyb, scb0, scr0);
-    chroma_taps<kWin>(win, cx0, cy0, gx1, cw, ya, yb, wya, wyb, scb1, scr1);
+    if ((gx0 & 1) == 0 && gx1 == gx0 + 1) {
+        // An even pixel and its right neighbour share chroma column jx: the
+        // even one takes columns (jx - 1, jx) with weights (1, 3), the odd
+        // one (jx, jx + 1) with (3, 1), clamped as in chroma_taps. Three
+        // 16-bit (cb, cr) loads per chroma row.
+        const int jx{gx0 >> 1};
+        const int k0{max(jx - 1, 0) - cx0};
+        const int k1{jx - cx0};
+        const int k2{min(jx + 1, cw - 1) - cx0};
+        const auto* ra{reinterpret_cast<const std::uint16_t*>(win) + (ya - cy0) * kWin};
+        const auto* rb{reinterpret_cast<const std::uint16_t*>(win) + (yb - cy0) * kWin};
+        const int a0{ra[k0]}, a1{ra[k1]}, a2{ra[k2]};
+        const int b0{rb[k0]}, b1{rb[k1]}, b2{rb[k2]};
+        scb0 = wya * ((a0 & 0xff) + 3 * (a1 & 0xff)) + wyb * ((b0 & 0xff) + 3 * (b1 & 0xff));
+        scr0 = wya * ((a0 >> 8) + 3 * (a1 >> 8)) + wyb * ((b0 >> 8) + 3 * (b1 >> 8));
+        scb1 = wya * (3 * (a1 & 0xff) + (a2 & 0xff)) + wyb * (3 * (b1 & 0xff) + (b2 & 0xff));
+        scr1 = wya * (3 * (a1 >> 8) + (a2 >> 8)) + wyb * (3 * (b1 >> 8) + (b2 >> 8));
+    } else {
+        chroma_taps<kWin>(win, cx0, cy0, gx0, cw, ya, yb, wya, wyb, scb0, scr0);
+        chroma_taps<kWin>(win, cx0, cy0, gx1, cw, ya, yb, wya, wyb, scb1, scr1);
+    }
     const float2 cb{__fadd2_rn(div4080_2(scb0, scb1), f2dup(-kChromaCenter))};
     const float2 cr{__fadd2_rn(div4080_2(scr0, scr1), f2dup(-kChromaCenter))};
 
-    const float2 r{clamp01_2(srgb_to_linear2(clamp01_2(__ffma2_rn(f2dup(kCrToR), cr, yv))))};
+    const float2 r{clamp01_2(srgb_to_linear2(clamp01_2(__ffma2_rn(f2dup(kCrToR), cr, yv)), lut))};
     const float2 g{clamp01_2(srgb_to_linear2(
-        clamp01_2(__ffma2_rn(f2dup(-kCrToG), cr, __ffma2_rn(f2dup(-kCbToG), cb, yv)))))};
-    const float2 b{clamp01_2(srgb_to_linear2(clamp01_2(__ffma2_rn(f2dup(kCbToB), cb, yv))))};
+        clamp01_2(__ffma2_rn(f2dup(-kCrToG), cr, __ffma2_rn(f2dup(-kCbToG), cb, yv))), lut))};
+    const float2 b{clamp01_2(srgb_to_linear2(clamp01_2(__ffma2_rn(f2dup(kCbToB), cb, yv)), lut))};
 
     const float2 bias{f2dup(kOpsinBias)};
     float2 m0{__fadd2_rn(__ffma2_rn(f2dup(kM02), b, __ffma2_rn(f2dup(kM01), g, __fmul2_rn(f2dup(kM00), r))), bias)};
