@@ -204,6 +204,25 @@ __device__ float erosion_cell(const float* pre, int sx0, int sy0, int cx, int cy
     return r;
 }
 
+// warp_tree on both components at once (two shuffles, one packed add per
+// step); each component's sum is warp_tree's.
+__device__ __forceinline__ float2 warp_tree2(float2 v) {
+#pragma unroll
+    for (int off{16}; off > 0; off >>= 1) {
+        v = __fadd2_rn(v, make_float2(__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)));
+    }
+    return v;
+}
+
+// ratio_gamma<true> on both components.
+__device__ __forceinline__ float2 ratio_gamma_inv2(float2 v) {
+    v = make_float2(v.x < 0.0f ? 0.0f : v.x, v.y < 0.0f ? 0.0f : v.y);
+    const float2 v2{__fmul2_rn(v, v)};
+    const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
+    const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
+    return make_float2(num.x / den.x, num.y / den.y);
+}
+
 // Sum over the 32 lanes with the shfl_down pairing (offsets 16..1); the total
 // lands in lane 0.
 __device__ __forceinline__ float warp_tree(float v) {
@@ -289,6 +308,12 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
         for (int r{0}; r < N; ++r) {
             c2 = __fadd2_rn(c2, __fmul2_rn(basis2<N, true>((fy0 >> 1) * N + r), rr[r]));
         }
+        // Weights, scaled values, half-weights and squares of the pair at once
+        // (fx * N + fy0 is even: one 8-byte weight load).
+        const float2 w2{*reinterpret_cast<const float2*>(wsel + fx * N + fy0)};
+        const float2 sc2{__fmul2_rn(c2, f2dup(qgsf))};
+        const float2 hw2{__fmul2_rn(f2dup(0.5f), w2)};
+        const float2 sq2{__fmul2_rn(c2, c2)};
 #pragma unroll
         for (int h{0}; h < 2; ++h) {
             const int fy{fy0 + h};
@@ -296,13 +321,13 @@ __device__ __forceinline__ void sel_col(const float* rows_fx, float* cd_fx, floa
             float d{0.0f};
             float rt{0.0f};
             if (!(fx < N / 8 && fy < N / 8)) {
-                const float w{wsel[fx * N + fy]};
-                const float scaled{coeff * qgsf};
-                if (fabsf(scaled) <= 0.5f * w) {
+                const float w{h == 0 ? w2.x : w2.y};
+                const float scaled{h == 0 ? sc2.x : sc2.y};
+                if (fabsf(scaled) <= (h == 0 ? hw2.x : hw2.y)) {
                     // |scaled / w| <= 1/2 rounds to a quotient of at most 1/2,
                     // so q is zero and err is -coeff exactly: the same d, no
                     // rate.
-                    d = coeff * coeff;
+                    d = h == 0 ? sq2.x : sq2.y;
                 } else {
                     const float2 dr{sel_cost_nonzero(coeff, scaled, w, qgsf, l2t, l2s)};
                     d = dr.x;
@@ -738,37 +763,44 @@ __global__ void __launch_bounds__(kThreads, 2)
             continue;  // warp-uniform
         }
         const int fx{lane & 7};
-        float red[2][3];
-        for (int half{0}; half < 2; ++half) {
-            const int fy{(lane >> 3) + 4 * half};
-            const int ix{lbx * 8 + fx + kHalo};
-            const int iy{lby * 8 + fy + kHalo};
-            const float yv{Y[iy * kXs + ix]};
-            const float xv{xyb[iy * kXs + ix]};
-            const float bv{xyb[2 * kXplane + iy * kXs + ix]};
-            float hf{0.0f};
-            if (fx < 7) {
-                hf = hf + fminf(kHfValMin, fabsf(yv - Y[iy * kXs + ix + 1]));
-            }
-            if (fy < 7) {
-                hf = hf + fminf(kHfValMin, fabsf(yv - Y[(iy + 1) * kXs + ix]));
-            }
-            const float iny{yv + kGammaBias};
-            const float gp{ratio_gamma<true>(iny - xv) + ratio_gamma<true>(iny + xv)};
-            const float pye{(yv + kBlueOffset) + fabsf(xv)};
-            const float bp{bv > pye ? fminf(bv - pye, kBlueLimit) : 0.0f};
-            red[half][0] = warp_tree(hf);
-            red[half][1] = warp_tree(gp);
-            red[half][2] = warp_tree(bp);
+        // Rows fy and fy + 4 of the block as the two components of packed
+        // pairs; each half's tree is the reference's, run on both at once.
+        const int fy{lane >> 3};
+        const int ix{lbx * 8 + fx + kHalo};
+        const int iy{lby * 8 + fy + kHalo};
+        const int i0{iy * kXs + ix};
+        const int i1{i0 + 4 * kXs};
+        const float2 yv{Y[i0], Y[i1]};
+        const float2 xv{xyb[i0], xyb[i1]};
+        const float2 bv{xyb[2 * kXplane + i0], xyb[2 * kXplane + i1]};
+        float2 hf{0.0f, 0.0f};
+        if (fx < 7) {
+            const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + 1], Y[i1 + 1])))};
+            hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)), fminf(kHfValMin, fabsf(d.y))));
         }
+        {
+            // Row fy + 4 has no lower neighbour in the block when it is 7; its
+            // term is then +0, which leaves the non-negative sum unchanged.
+            const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + kXs], Y[i1 + kXs])))};
+            hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)),
+                                            fy + 4 < 7 ? fminf(kHfValMin, fabsf(d.y)) : 0.0f));
+        }
+        const float2 iny{__fadd2_rn(yv, f2dup(kGammaBias))};
+        const float2 gp{__fadd2_rn(ratio_gamma_inv2(__fadd2_rn(iny, f2neg(xv))), ratio_gamma_inv2(__fadd2_rn(iny, xv)))};
+        const float2 pye{__fadd2_rn(__fadd2_rn(yv, f2dup(kBlueOffset)), make_float2(fabsf(xv.x), fabsf(xv.y)))};
+        const float2 bd{__fadd2_rn(bv, f2neg(pye))};
+        const float2 bp{bv.x > pye.x ? fminf(bd.x, kBlueLimit) : 0.0f, bv.y > pye.y ? fminf(bd.y, kBlueLimit) : 0.0f};
+        const float2 red0{warp_tree2(hf)};
+        const float2 red1{warp_tree2(gp)};
+        const float2 red2{warp_tree2(bp)};
         if (lane == 0) {
             // The block's quant field is finished from these sums by its own
             // thread in step 4e, where most warps are otherwise idle. The
             // eroded sum gets the second half's tree of zeros added, as the
             // per-half reduction did.
-            sm.aq_sums[0][lb] = red[0][0] + red[1][0];
-            sm.aq_sums[1][lb] = red[0][1] + red[1][1];
-            sm.aq_sums[2][lb] = red[0][2] + red[1][2];
+            sm.aq_sums[0][lb] = red0.x + red0.y;
+            sm.aq_sums[1][lb] = red1.x + red1.y;
+            sm.aq_sums[2][lb] = red2.x + red2.y;
             sm.aq_sums[3][lb] = eroded + 0.0f;
         }
     }
@@ -1344,6 +1376,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     // Two adjacent slots (one even raw index and the next) per thread: they
     // share the block, its quant field and weights row, and their coefficient,
     // weight and output pairs move as single 4- or 8-byte accesses.
+    static_assert(kThreads % 32 == 0 && 2048 % kThreads == 0, "one tile block per warp iteration");
     for (int k2{tid}; k2 < 2048; k2 += kThreads) {  // 8 uniform iterations per warp
         const int k{2 * k2};
         const int lb{k >> 6};
@@ -1396,17 +1429,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             *reinterpret_cast<short2*>(out.ac + cplane + g) = make_short2(ay[0], ay[1]);
             *reinterpret_cast<short2*>(out.ac + 2 * cplane + g) = make_short2(ab[0], ab[1]);
         }
-        // Non-zero counts per first block: one shared-memory add per block
-        // and channel per warp (lanes of a warp mostly share a block).
-        const unsigned peers{__match_any_sync(0xffffffffu, f)};
-        const bool leader{(__ffs(peers) - 1) == lane};
-        const int cx{__popc(__ballot_sync(0xffffffffu, ax[0] != 0) & peers) +
-                     __popc(__ballot_sync(0xffffffffu, ax[1] != 0) & peers)};
-        const int cy{__popc(__ballot_sync(0xffffffffu, ay[0] != 0) & peers) +
-                     __popc(__ballot_sync(0xffffffffu, ay[1] != 0) & peers)};
-        const int cb{__popc(__ballot_sync(0xffffffffu, ab[0] != 0) & peers) +
-                     __popc(__ballot_sync(0xffffffffu, ab[1] != 0) & peers)};
-        if (leader && f >= 0) {
+        // Non-zero counts per first block: the 32 pairs of a warp's iteration
+        // are the 64 slots of tile block warp + 8j, so the whole warp shares
+        // f, and lane 0 adds the warp's counts.
+        const int cx{__popc(__ballot_sync(0xffffffffu, ax[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ax[1] != 0))};
+        const int cy{__popc(__ballot_sync(0xffffffffu, ay[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ay[1] != 0))};
+        const int cb{__popc(__ballot_sync(0xffffffffu, ab[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ab[1] != 0))};
+        if (lane == 0 && f >= 0) {
             if (cx) atomicAdd(&sm.nz[0][f], cx);
             if (cy) atomicAdd(&sm.nz[1][f], cy);
             if (cb) atomicAdd(&sm.nz[2][f], cb);
