@@ -895,15 +895,17 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
         __syncthreads();
+        // Distortion and rate ride one packed pair through each step.
+#pragma unroll 2
         for (int lb{warp}; lb < 64; lb += kThreads / 32) {
             if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh &&
                 ((dmask >> region_of_block(lb)) & 1u) == 0) {
                 const int i0{lb * 72 + (lane >> 3) * 9 + (lane & 7)};
                 const int i1{lb * 72 + ((lane + 32) >> 3) * 9 + (lane & 7)};
-                const float D{warp_tree(cdist[i0] + cdist[i1])};
-                const float R{warp_tree(crate[i0] + crate[i1])};
+                const float2 DR{warp_tree2(
+                    __fadd2_rn(make_float2(cdist[i0], crate[i0]), make_float2(cdist[i1], crate[i1])))};
                 if (lane == 0) {
-                    sm.cost8[lb] = 64.0f * D + kSelectLambda * R;
+                    sm.cost8[lb] = 64.0f * DR.x + kSelectLambda * DR.y;
                 }
             }
         }
@@ -934,27 +936,22 @@ __global__ void __launch_bounds__(kThreads, 2)
         for (int qd{warp}; qd < 16; qd += kThreads / 32) {
             if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh &&
                 ((dmask >> (((qd >> 3) << 1) | ((qd & 3) >> 1))) & 1u) == 0) {
-                float pd[8];
-                float pr[8];
+                // Distortion (x) and rate (y) as packed pairs, each in the
+                // host twin's order.
+                float2 p[8];
 #pragma unroll
                 for (int j{0}; j < 8; ++j) {
                     const int t{lane + 32 * j};
-                    pd[j] = cdist[qd * 272 + (t >> 4) * 17 + (t & 15)];
-                    pr[j] = crate[qd * 272 + (t >> 4) * 17 + (t & 15)];
+                    const int at{qd * 272 + (t >> 4) * 17 + (t & 15)};
+                    p[j] = make_float2(cdist[at], crate[at]);
                 }
 #pragma unroll
-                for (int j{0}; j < 4; ++j) {
-                    pd[j] = pd[j] + pd[j + 4];
-                    pr[j] = pr[j] + pr[j + 4];
-                }
-                pd[0] = pd[0] + pd[2];
-                pd[1] = pd[1] + pd[3];
-                pr[0] = pr[0] + pr[2];
-                pr[1] = pr[1] + pr[3];
-                const float D{warp_tree(pd[0] + pd[1])};
-                const float R{warp_tree(pr[0] + pr[1])};
+                for (int j{0}; j < 4; ++j) p[j] = __fadd2_rn(p[j], p[j + 4]);
+                p[0] = __fadd2_rn(p[0], p[2]);
+                p[1] = __fadd2_rn(p[1], p[3]);
+                const float2 DR{warp_tree2(__fadd2_rn(p[0], p[1]))};
                 if (lane == 0) {
-                    sm.cost16[qd] = 256.0f * D + kSelectLambda * R;
+                    sm.cost16[qd] = 256.0f * DR.x + kSelectLambda * DR.y;
                 }
             }
         }
@@ -998,34 +995,27 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int ri{warp};
             if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh &&
                 ((dmask >> ri) & 1u) == 0) {
-                float pd[8];
-                float pr[8];
+                // Distortion (x) and rate (y) as packed pairs, each in the
+                // host twin's order.
+                float2 p[8];
 #pragma unroll
                 for (int j{0}; j < 8; ++j) {
-                    float d{0.0f};
-                    float r{0.0f};
+                    float2 dr{0.0f, 0.0f};
 #pragma unroll
                     for (int m{0}; m < 4; ++m) {
                         const int e{lane + 32 * j + 256 * m};
-                        d = d + cdist[ri * 1056 + (e >> 5) * 33 + (e & 31)];
-                        r = r + crate[ri * 1056 + (e >> 5) * 33 + (e & 31)];
+                        const int at{ri * 1056 + (e >> 5) * 33 + (e & 31)};
+                        dr = __fadd2_rn(dr, make_float2(cdist[at], crate[at]));
                     }
-                    pd[j] = d;
-                    pr[j] = r;
+                    p[j] = dr;
                 }
 #pragma unroll
-                for (int j{0}; j < 4; ++j) {
-                    pd[j] = pd[j] + pd[j + 4];
-                    pr[j] = pr[j] + pr[j + 4];
-                }
-                pd[0] = pd[0] + pd[2];
-                pd[1] = pd[1] + pd[3];
-                pr[0] = pr[0] + pr[2];
-                pr[1] = pr[1] + pr[3];
-                const float D{warp_tree(pd[0] + pd[1])};
-                const float R{warp_tree(pr[0] + pr[1])};
+                for (int j{0}; j < 4; ++j) p[j] = __fadd2_rn(p[j], p[j + 4]);
+                p[0] = __fadd2_rn(p[0], p[2]);
+                p[1] = __fadd2_rn(p[1], p[3]);
+                const float2 DR{warp_tree2(__fadd2_rn(p[0], p[1]))};
                 if (lane == 0) {
-                    sm.cost32[ri] = 1024.0f * D + kSelectLambda * R;
+                    sm.cost32[ri] = 1024.0f * DR.x + kSelectLambda * DR.y;
                 }
             }
         }
