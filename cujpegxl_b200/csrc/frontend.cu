@@ -38,13 +38,18 @@ constexpr int kXplane = kXs * kXs;
 constexpr int kSs = kTile + 4;
 constexpr int kSplane = kTile * kSs;
 constexpr int kRegionAFloats = 3 * kXplane;  // 13872
-// FP16 coefficients of the tile in region A: 64 covered-block slots per block,
-// padded to 66 so that lanes walking different blocks at the same slot hit
-// different shared-memory banks; the final-DCT row scratch follows them.
+// FP16 coefficients of the tile: 64 covered-block slots per block, padded to
+// 66 so that lanes walking different blocks at the same slot hit different
+// shared-memory banks. Channel c's plane lies over sharpened plane c (region
+// B), kCoefStride halves apart.
 constexpr int kCoefBlock = 66;
 constexpr int kCoefPlane = 64 * kCoefBlock;
-constexpr int kDrowsOffset = 3 * kCoefPlane / 2;  // floats
-static_assert(kDrowsOffset + 64 * 72 <= kRegionAFloats, "final-DCT scratch exceeds region A");
+constexpr int kCoefStride = 2 * kSplane;
+static_assert(kCoefPlane <= kCoefStride, "a coefficient plane exceeds its sharpened plane");
+// Final-DCT row scratch of one channel (floats); the three channels' lie
+// side by side in region A.
+constexpr int kDrowsChannel = 64 * 72;
+static_assert(3 * kDrowsChannel <= kRegionAFloats, "final-DCT scratch exceeds region A");
 // Row stride of one first block's row-pass output in the final-DCT scratch:
 // 36 for DCT32 (16-byte aligned rows for the column pass's vector loads; one
 // block per warp, so lanes stay on distinct banks), N + 1 for DCT16 and DCT8,
@@ -414,8 +419,8 @@ __device__ __forceinline__ float cfl_sum(const __half* coef, int lb) {
 #pragma unroll 1
     for (int q{0}; q < kSide * kSide; ++q) {
         const int l{lb + (q / kSide) * 8 + q % kSide};
-        const std::uint32_t* py{reinterpret_cast<const std::uint32_t*>(coef + kCoefPlane + l * kCoefBlock)};
-        const std::uint32_t* po{reinterpret_cast<const std::uint32_t*>(coef + (kWhich == 2 ? 2 * kCoefPlane : 0) +
+        const std::uint32_t* py{reinterpret_cast<const std::uint32_t*>(coef + kCoefStride + l * kCoefBlock)};
+        const std::uint32_t* po{reinterpret_cast<const std::uint32_t*>(coef + (kWhich == 2 ? 2 * kCoefStride : 0) +
                                                                        l * kCoefBlock)};
         const std::uint64_t skip{q < kQLlf ? kLlf : 0ull};
 #pragma unroll
@@ -483,7 +488,7 @@ __device__ __forceinline__ void llf_to_dc(const __half* coef, int f, int ox, int
                 const int raw{fx * kN + fy};
                 const int q{raw >> 6};
                 const int blk{f + (q >> (M >> 1)) * 8 + (q & (M - 1))};
-                const double cv{__half2float(coef[c * kCoefPlane + blk * kCoefBlock + (raw & 63)])};
+                const double cv{__half2float(coef[c * kCoefStride + blk * kCoefBlock + (raw & 63)])};
                 const double sx{M == 2 ? kS16[fx] : kS32[fx]};
                 const double sy{M == 2 ? kS16[fy] : kS32[fy]};
                 sum = sum + ((ab[fx][fy] * cv) * sx) * sy;
@@ -1213,69 +1218,74 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
 
     // ---- 5. variable DCT of X, Y, B -> FP16 coefficients (src/frontend_transform.cu:190-266).
-    __half* coef{reinterpret_cast<__half*>(smem)};  // [3][64 blocks][kCoefBlock]
-    float* drows{smem + kDrowsOffset};
+    // The three channels' row passes run in one phase (each channel has its
+    // own row scratch in region A), then their column passes in another; the
+    // FP16 coefficients of channel c go over sharpened plane c, which its row
+    // pass has finished reading.
+    __half* coef{reinterpret_cast<__half*>(shp)};  // [3][64 blocks][kCoefBlock], channel stride kCoefStride
     const int n32{sm.n32};
     const int n16{sm.n16};
     const int n8{sm.n8};
     const int t32{64 * n32};
     const int t16{t32 + 16 * n16};
     const int tall{t16 + 8 * n8};
-    for (int c{0}; c < 3; ++c) {
+    for (int k3{tid}; k3 < 3 * tall; k3 += kThreads) {
+        const int c{k3 >= 2 * tall ? 2 : (k3 >= tall ? 1 : 0)};
+        const int k{k3 - c * tall};
         const float* P{shp + c * kSplane};
-        for (int k{tid}; k < tall; k += kThreads) {
-            if (k < t32) {
-                const int f{k >> 6};
-                const int lb{sm.fb_list[f]};
-                const int r{k & 31};
-                const float* src{P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8};
-                float* dst{drows + sm.fb_off[f] + r};
-                if (k & 32) {
-                    row_pass<32, 16, 32, false>(src, dst);
-                } else {
-                    row_pass<32, 0, 16, false>(src, dst);
-                }
-            } else if (k < t16) {
-                const int f{n32 + ((k - t32) >> 4)};
-                const int lb{sm.fb_list[f]};
-                const int r{(k - t32) & 15};
-                row_pass<16, 0, 16, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8,
-                                           drows + sm.fb_off[f] + r);
+        float* drows{smem + c * kDrowsChannel};
+        if (k < t32) {
+            const int f{k >> 6};
+            const int lb{sm.fb_list[f]};
+            const int r{k & 31};
+            const float* src{P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8};
+            float* dst{drows + sm.fb_off[f] + r};
+            if (k & 32) {
+                row_pass<32, 16, 32, false>(src, dst);
             } else {
-                const int f{n32 + n16 + ((k - t16) >> 3)};
-                const int lb{sm.fb_list[f]};
-                const int r{(k - t16) & 7};
-                row_pass<8, 0, 8, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8,
-                                         drows + sm.fb_off[f] + r);
+                row_pass<32, 0, 16, false>(src, dst);
             }
+        } else if (k < t16) {
+            const int f{n32 + ((k - t32) >> 4)};
+            const int lb{sm.fb_list[f]};
+            const int r{(k - t32) & 15};
+            row_pass<16, 0, 16, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8, drows + sm.fb_off[f] + r);
+        } else {
+            const int f{n32 + n16 + ((k - t16) >> 3)};
+            const int lb{sm.fb_list[f]};
+            const int r{(k - t16) & 7};
+            row_pass<8, 0, 8, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8, drows + sm.fb_off[f] + r);
         }
-        __syncthreads();
-        __half* cc{coef + c * kCoefPlane};
-        for (int k{tid}; k < tall; k += kThreads) {
-            if (k < t32) {
-                const int f{k >> 6};
-                const int lb{sm.fb_list[f]};
-                const int fx{k & 31};
-                const float* src{drows + sm.fb_off[f] + fx * kDrowsStride<32>};
-                if (k & 32) {
-                    dct_col<32, 16, 32>(src, cc, fx, lb & 7, lb >> 3);
-                } else {
-                    dct_col<32, 0, 16>(src, cc, fx, lb & 7, lb >> 3);
-                }
-            } else if (k < t16) {
-                const int f{n32 + ((k - t32) >> 4)};
-                const int lb{sm.fb_list[f]};
-                const int fx{(k - t32) & 15};
-                dct_col<16, 0, 16>(drows + sm.fb_off[f] + fx * 17, cc, fx, lb & 7, lb >> 3);
-            } else {
-                const int f{n32 + n16 + ((k - t16) >> 3)};
-                const int lb{sm.fb_list[f]};
-                const int fx{(k - t16) & 7};
-                dct_col<8, 0, 8>(drows + sm.fb_off[f] + fx * 9, cc, fx, lb & 7, lb >> 3);
-            }
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    for (int k3{tid}; k3 < 3 * tall; k3 += kThreads) {
+        const int c{k3 >= 2 * tall ? 2 : (k3 >= tall ? 1 : 0)};
+        const int k{k3 - c * tall};
+        const float* drows{smem + c * kDrowsChannel};
+        __half* cc{coef + c * kCoefStride};
+        if (k < t32) {
+            const int f{k >> 6};
+            const int lb{sm.fb_list[f]};
+            const int fx{k & 31};
+            const float* src{drows + sm.fb_off[f] + fx * kDrowsStride<32>};
+            if (k & 32) {
+                dct_col<32, 16, 32>(src, cc, fx, lb & 7, lb >> 3);
+            } else {
+                dct_col<32, 0, 16>(src, cc, fx, lb & 7, lb >> 3);
+            }
+        } else if (k < t16) {
+            const int f{n32 + ((k - t32) >> 4)};
+            const int lb{sm.fb_list[f]};
+            const int fx{(k - t32) & 15};
+            dct_col<16, 0, 16>(drows + sm.fb_off[f] + fx * 17, cc, fx, lb & 7, lb >> 3);
+        } else {
+            const int f{n32 + n16 + ((k - t16) >> 3)};
+            const int lb{sm.fb_list[f]};
+            const int fx{(k - t16) & 7};
+            dct_col<8, 0, 8>(drows + sm.fb_off[f] + fx * 9, cc, fx, lb & 7, lb >> 3);
+        }
+    }
+    __syncthreads();
 
     if (out.dbg_coeff != nullptr) {
         for (int i{tid}; i < 3 * 4096; i += kThreads) {
@@ -1286,7 +1296,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (gbx < bw && gby < bh) {
                 out.dbg_coeff[static_cast<std::size_t>(c) * nblocks * 64 +
                               (static_cast<std::size_t>(gby) * bw + gbx) * 64 + (i & 63)] =
-                    __half_as_ushort(coef[c * kCoefPlane + lb * kCoefBlock + (i & 63)]);
+                    __half_as_ushort(coef[c * kCoefStride + lb * kCoefBlock + (i & 63)]);
             }
         }
     }
@@ -1317,7 +1327,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             float dcv[3];
             if (m == 1) {
                 for (int c{0}; c < 3; ++c) {
-                    dcv[c] = __half2float(coef[c * kCoefPlane + f * kCoefBlock]);
+                    dcv[c] = __half2float(coef[c * kCoefStride + f * kCoefBlock]);
                 }
             } else if (m == 2) {
                 llf_to_dc<2>(coef, f, ox, oy, tb.llf_basis, dcv);
@@ -1393,8 +1403,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
                 const int ci{lb * kCoefBlock + slot};
                 const float2 xr{__half22float2(*reinterpret_cast<const __half2*>(coef + ci))};
-                const float2 yr{__half22float2(*reinterpret_cast<const __half2*>(coef + kCoefPlane + ci))};
-                const float2 br{__half22float2(*reinterpret_cast<const __half2*>(coef + 2 * kCoefPlane + ci))};
+                const float2 yr{__half22float2(*reinterpret_cast<const __half2*>(coef + kCoefStride + ci))};
+                const float2 br{__half22float2(*reinterpret_cast<const __half2*>(coef + 2 * kCoefStride + ci))};
                 const float2 wx{*reinterpret_cast<const float2*>(wt + raw)};
                 const float2 wy{*reinterpret_cast<const float2*>(wt + 1024 + raw)};
                 const float2 wb{*reinterpret_cast<const float2*>(wt + 2048 + raw)};
