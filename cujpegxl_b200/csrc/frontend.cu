@@ -914,8 +914,9 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
         }
-        __syncthreads();
         // 4b. DCT16 candidates: the 16 quads of the tile that fit in the image.
+        // Their row pass writes only the row scratch, which the DCT8
+        // reduction above does not read, so it shares that phase.
         for (int k{tid}; k < 256; k += kThreads) {
             const int qd{k >> 4};
             const int r{k & 15};
@@ -960,8 +961,9 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
         }
-        __syncthreads();
         // 4c. DCT32 candidates: the 4 regions of the tile that fit in the image.
+        // Their row pass shares the DCT16 reduction's phase (disjoint
+        // scratch).
         for (int k{tid}; k < 256; k += kThreads) {
             const int ri{k >> 6};
             const int r{k & 31};
