@@ -1026,25 +1026,12 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
         }
-        __syncthreads();
     }
-    if (out.dbg_cost != nullptr) {
-        for (int lb{tid}; lb < 64; lb += kThreads) {
-            const int lbx{lb & 7};
-            const int lby{lb >> 3};
-            if (bx0 + lbx < bw && by0 + lby < bh) {
-                const std::size_t at{static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx};
-                out.dbg_cost[at] = sm.cost8[lb];
-                out.dbg_cost[nblocks + at] =
-                    ((lbx | lby) & 1) == 0 ? sm.cost16[(lby >> 1) * 4 + (lbx >> 1)] : 0.0f;
-                out.dbg_cost[2 * static_cast<std::size_t>(nblocks) + at] =
-                    ((lbx | lby) & 3) == 0 ? sm.cost32[(lby >> 2) * 2 + (lbx >> 2)] : 0.0f;
-            }
-        }
-    }
-    // 4d. RD decision per region (src/transform_select_impl.cuh:130-201).
-    if (tid < 4) {
-        const int ri{tid};
+    // 4d. RD decision per region (src/transform_select_impl.cuh:130-201), by
+    // lane 0 of warp ri, which wrote cost32[ri] itself (the DCT8 and DCT16
+    // costs are older than the last barrier).
+    if (warp < 4 && lane == 0) {
+        const int ri{warp};
         const int rlx{(ri & 1) * 4};
         const int rly{(ri >> 1) * 4};
         const int rbx{bx0 + rlx};
@@ -1131,7 +1118,55 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
         }
     }
+    // Warps 4-7 meanwhile clear the non-zero counters and CfL sums and finish
+    // each block's quant field from its AQ sums.
+    if (tid >= 128) {
+        for (int i{tid - 128}; i < 192; i += 128) {
+            sm.nz[i >> 6][i & 63] = 0;
+            sm.cfl[i >> 6][i & 63] = 0.0f;  // blocks that are not first blocks add zero
+        }
+    }
+    if (tid >= 128 && tid < 192) {
+        // Quant field of block lb from its AQ sums (src/frontend_fused.cu:177-201).
+        const int lb{tid - 128};
+        if (((qmask >> region_of_block(lb)) & 1u) != 0) {
+            sm.qf[lb] = in.net_qf[static_cast<std::size_t>(by0 + (lb >> 3)) * bw + bx0 + (lb & 7)];
+        } else if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
+            const float hf_sum{sm.aq_sums[0][lb]};
+            const float gamma_overall{sm.aq_sums[1][lb] * (0.5f / 64.0f)};
+            float blue_sum{sm.aq_sums[2][lb]};
+            const float aq{sm.aq_sums[3][lb]};
+            if (blue_sum >= 32.0f * kBlueLimit) {
+                blue_sum = 64.0f * kBlueLimit - blue_sum;
+            }
+            if (blue_sum >= kBlueMaxLimit * kBlueLimit) {
+                blue_sum = kBlueMaxLimit * kBlueLimit;
+            }
+            float ov{compute_mask(aq)};
+            ov = ov + jx_fma(hf_sum, kHfMul, kHfAdd);
+            ov = jx_fma(kGammaLogMul, jx_log2(gamma_overall), ov);
+            ov = jx_fma(blue_sum, kBlueMul, ov);
+            const float qval{jx_fma(jx_exp(ov), sc.mul_pb, sc.add_pb)};
+            int qi{static_cast<int>(jx_fma(qval, sc.inv_global_scale, 0.5f))};
+            qi = qi < 1 ? 1 : (qi > kQuantMax ? kQuantMax : qi);
+            sm.qf[lb] = qi;
+        }
+    }
     __syncthreads();
+    if (out.dbg_cost != nullptr) {
+        for (int lb{tid}; lb < 64; lb += kThreads) {
+            const int lbx{lb & 7};
+            const int lby{lb >> 3};
+            if (bx0 + lbx < bw && by0 + lby < bh) {
+                const std::size_t at{static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx};
+                out.dbg_cost[at] = sm.cost8[lb];
+                out.dbg_cost[nblocks + at] =
+                    ((lbx | lby) & 1) == 0 ? sm.cost16[(lby >> 1) * 4 + (lbx >> 1)] : 0.0f;
+                out.dbg_cost[2 * static_cast<std::size_t>(nblocks) + at] =
+                    ((lbx | lby) & 3) == 0 ? sm.cost32[(lby >> 2) * 2 + (lbx >> 2)] : 0.0f;
+            }
+        }
+    }
     // 4e. first-block list (DCT32 first, then DCT16, then DCT8, each in raster
     // order) with each entry's row-pass scratch offset, and the covering owner
     // of every block; warp 0, two blocks per lane.
@@ -1185,36 +1220,6 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             at += cnt;
             off += cnt * step;
-        }
-    }
-    if (tid >= 64 && tid < 256) {
-        sm.nz[(tid - 64) >> 6][tid & 63] = 0;
-        sm.cfl[(tid - 64) >> 6][tid & 63] = 0.0f;  // blocks that are not first blocks add zero
-    }
-    if (tid >= 64 && tid < 128) {
-        // Quant field of block lb from its AQ sums (src/frontend_fused.cu:177-201).
-        const int lb{tid - 64};
-        if (((qmask >> region_of_block(lb)) & 1u) != 0) {
-            sm.qf[lb] = in.net_qf[static_cast<std::size_t>(by0 + (lb >> 3)) * bw + bx0 + (lb & 7)];
-        } else if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh) {
-            const float hf_sum{sm.aq_sums[0][lb]};
-            const float gamma_overall{sm.aq_sums[1][lb] * (0.5f / 64.0f)};
-            float blue_sum{sm.aq_sums[2][lb]};
-            const float aq{sm.aq_sums[3][lb]};
-            if (blue_sum >= 32.0f * kBlueLimit) {
-                blue_sum = 64.0f * kBlueLimit - blue_sum;
-            }
-            if (blue_sum >= kBlueMaxLimit * kBlueLimit) {
-                blue_sum = kBlueMaxLimit * kBlueLimit;
-            }
-            float ov{compute_mask(aq)};
-            ov = ov + jx_fma(hf_sum, kHfMul, kHfAdd);
-            ov = jx_fma(kGammaLogMul, jx_log2(gamma_overall), ov);
-            ov = jx_fma(blue_sum, kBlueMul, ov);
-            const float qval{jx_fma(jx_exp(ov), sc.mul_pb, sc.add_pb)};
-            int qi{static_cast<int>(jx_fma(qval, sc.inv_global_scale, 0.5f))};
-            qi = qi < 1 ? 1 : (qi > kQuantMax ? kQuantMax : qi);
-            sm.qf[lb] = qi;
         }
     }
     __syncthreads();
