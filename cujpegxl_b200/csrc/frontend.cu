@@ -21,6 +21,7 @@
 #include "frontend.cuh"
 #include "jxl_constants.cuh"
 #include "jxl_math.cuh"
+#include "ratio_div.cuh"
 #include "xyb.cuh"
 
 namespace jxb {
@@ -225,7 +226,7 @@ __device__ __forceinline__ float2 ratio_gamma_inv2(float2 v) {
     const float2 v2{__fmul2_rn(v, v)};
     const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
     const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
-    return make_float2(num.x / den.x, num.y / den.y);
+    return div2_ratio(num, den);
 }
 
 // Sum over the 32 lanes with the shfl_down pairing (offsets 16..1); the total
@@ -729,7 +730,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const float2 v2{__fmul2_rn(v, v)};
                 const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
                 const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
-                const float2 ratio{den.x / num.x, den.y / num.y};
+                const float2 ratio{div2_ratio(den, num)};
                 float2 d{__fmul2_rn(ratio, __fadd2_rn(yv, f2neg(base)))};
                 d = __fmul2_rn(d, d);
                 d = make_float2(fminf(d.x, kDiffLimit), fminf(d.y, kDiffLimit));
