@@ -514,8 +514,11 @@ __device__ __forceinline__ void cfl_class(const __half* coef, const unsigned cha
 __global__ void __launch_bounds__(kThreads, 2)
     frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
     extern __shared__ __align__(16) float smem[];
+    // Region A: the XYB planes, later the selection and final-DCT row
+    // scratch. Region B: the sharpened planes, later the FP16 coefficients
+    // and the NV12 window before both.
     float* xyb{smem};                                // [3][68*68]
-    float* shp{smem + kRegionAFloats};               // [3][64*65]
+    float* shp{smem + kRegionAFloats};               // [3][64*kSs]
     Small& sm{*reinterpret_cast<Small*>(smem + kRegionAFloats + 3 * kSplane)};
 
     const int tid{static_cast<int>(threadIdx.x)};
