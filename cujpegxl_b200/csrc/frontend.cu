@@ -815,20 +815,21 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 
     // ---- 3. inverse gaborish, 5x5 with image-border clamping (src/frontend_transform.cu:19-36).
-    // Two horizontally adjacent outputs (x even) per thread on packed f32x2
-    // arithmetic: each source row's six samples x-2..x+3 come in as three
-    // aligned float2 loads (the row stride kXs and x + kHalo - 2 are even),
-    // and operand pair (dx, dy) is {row[x+dx], row[x+1+dx]}.
+    // Two horizontally adjacent outputs (x even) of two adjacent rows per
+    // thread on packed f32x2 arithmetic: each of the six source rows' six
+    // samples x-2..x+3 come in as three aligned float2 loads (the row stride
+    // kXs and x + kHalo - 2 are even), shared by both output rows, and
+    // operand pair (dx, dy) is {row[x+dx], row[x+1+dx]}.
     static_assert(kXs % 2 == 0 && kHalo % 2 == 0, "gaborish pairs");
-    for (int i2{tid}; i2 < 3 * kTile * kTile / 2; i2 += kThreads) {
-        const int c{i2 >> 11};
-        const int p2{i2 & 2047};
-        const int x{2 * (p2 & 31)};
-        const int y{p2 >> 5};
-        const float* P{xyb + c * kXplane + y * kXs + x};  // sample (x - 2, y - 2)
-        float2 row[5][5];  // row[dy + 2][dx + 2]
+    for (int i4{tid}; i4 < 3 * kTile * kTile / 4; i4 += kThreads) {
+        const int c{i4 >> 10};
+        const int p4{i4 & 1023};
+        const int x{2 * (p4 & 31)};
+        const int y0{2 * (p4 >> 5)};
+        const float* P{xyb + c * kXplane + y0 * kXs + x};  // sample (x - 2, y0 - 2)
+        float2 row[6][5];  // row[r][dx + 2] of source row y0 - 2 + r
 #pragma unroll
-        for (int r{0}; r < 5; ++r) {
+        for (int r{0}; r < 6; ++r) {
             const float2 a{*reinterpret_cast<const float2*>(P + r * kXs)};
             const float2 b{*reinterpret_cast<const float2*>(P + r * kXs + 2)};
             const float2 d{*reinterpret_cast<const float2*>(P + r * kXs + 4)};
@@ -838,21 +839,24 @@ __global__ void __launch_bounds__(kThreads, 2)
             row[r][3] = make_float2(b.y, d.x);
             row[r][4] = d;
         }
-        auto at = [&](int dx, int dy) { return row[dy + 2][dx + 2]; };
-        auto add = [](float2 u, float2 v) { return __fadd2_rn(u, v); };
-        const float2 e{add(add(add(at(-1, 0), at(1, 0)), at(0, -1)), at(0, 1))};
-        const float2 r2{add(add(add(at(-2, 0), at(2, 0)), at(0, -2)), at(0, 2))};
-        const float2 dg{add(add(add(at(-1, -1), at(1, -1)), at(-1, 1)), at(1, 1))};
-        const float2 l8{add(add(add(add(add(add(add(at(-2, -1), at(2, -1)), at(-2, 1)), at(2, 1)), at(-1, -2)),
-                                    at(1, -2)), at(-1, 2)), at(1, 2))};
-        const float2 d4{add(add(add(at(-2, -2), at(2, -2)), at(-2, 2)), at(2, 2))};
-        float2 s{__fmul2_rn(f2dup(kGabC), at(0, 0))};
-        s = __ffma2_rn(f2dup(kGabEdge), e, s);
-        s = __ffma2_rn(f2dup(kGabEdge2), r2, s);
-        s = __ffma2_rn(f2dup(kGabDiag), dg, s);
-        s = __ffma2_rn(f2dup(kGabKnight), l8, s);
-        s = __ffma2_rn(f2dup(kGabDiag2), d4, s);
-        *reinterpret_cast<float2*>(shp + c * kSplane + y * kSs + x) = s;
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            auto at = [&](int dx, int dy) { return row[h + dy + 2][dx + 2]; };
+            auto add = [](float2 u, float2 v) { return __fadd2_rn(u, v); };
+            const float2 e{add(add(add(at(-1, 0), at(1, 0)), at(0, -1)), at(0, 1))};
+            const float2 r2{add(add(add(at(-2, 0), at(2, 0)), at(0, -2)), at(0, 2))};
+            const float2 dg{add(add(add(at(-1, -1), at(1, -1)), at(-1, 1)), at(1, 1))};
+            const float2 l8{add(add(add(add(add(add(add(at(-2, -1), at(2, -1)), at(-2, 1)), at(2, 1)), at(-1, -2)),
+                                        at(1, -2)), at(-1, 2)), at(1, 2))};
+            const float2 d4{add(add(add(at(-2, -2), at(2, -2)), at(-2, 2)), at(2, 2))};
+            float2 sv{__fmul2_rn(f2dup(kGabC), at(0, 0))};
+            sv = __ffma2_rn(f2dup(kGabEdge), e, sv);
+            sv = __ffma2_rn(f2dup(kGabEdge2), r2, sv);
+            sv = __ffma2_rn(f2dup(kGabDiag), dg, sv);
+            sv = __ffma2_rn(f2dup(kGabKnight), l8, sv);
+            sv = __ffma2_rn(f2dup(kGabDiag2), d4, sv);
+            *reinterpret_cast<float2*>(shp + c * kSplane + (y0 + h) * kSs + x) = sv;
+        }
     }
     __syncthreads();
 
