@@ -1388,72 +1388,94 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float ytox{static_cast<float>(sm.mx) * kCflColorScale};
     const float ytob{jx_fma(static_cast<float>(sm.mb), kCflColorScale, kCflBaseB)};
     const std::size_t cplane{static_cast<std::size_t>(nblocks) * 64};
-    // Two adjacent slots (one even raw index and the next) per thread: they
-    // share the block, its quant field and weights row, and their coefficient,
-    // weight and output pairs move as single 4- or 8-byte accesses.
-    static_assert(kThreads % 32 == 0 && 2048 % kThreads == 0, "one tile block per warp iteration");
-    for (int k2{tid}; k2 < 2048; k2 += kThreads) {  // 8 uniform iterations per warp
-        const int k{2 * k2};
+    // Four adjacent slots (raw indices 4m .. 4m + 3, which lie in one row of
+    // their block: every row is 8, 16 or 32 long) per thread: lanes 0-15 of a
+    // warp's iteration take the 64 slots of one tile block, lanes 16-31 those
+    // of the next, so the block's setup serves four slots per lane, weights
+    // move as 16-byte loads and outputs as 8-byte stores.
+    static_assert(kThreads % 32 == 0 && 1024 % kThreads == 0, "two tile blocks per warp iteration");
+    for (int k4{tid}; k4 < 1024; k4 += kThreads) {  // 4 uniform iterations per warp
+        const int k{4 * k4};
         const int lb{k >> 6};
         const int slot{k & 63};
         const int lbx{lb & 7};
         const int lby{lb >> 3};
         const bool inside{bx0 + lbx < bw && by0 + lby < bh};
         const int f{inside ? static_cast<int>(sm.owner[lb]) : -1};
-        std::int16_t ax[2]{0, 0};
-        std::int16_t ay[2]{0, 0};
-        std::int16_t ab[2]{0, 0};
+        std::int16_t ax[4]{0, 0, 0, 0};
+        std::int16_t ay[4]{0, 0, 0, 0};
+        std::int16_t ab[4]{0, 0, 0, 0};
         if (inside) {
             const int n{sm.acs[f]};
             const int side{n >> 3};
             const int lrow{side == 1 ? 3 : (side == 2 ? 4 : 5)};  // log2(n)
             const int q{(lby - (f >> 3)) * side + lbx - (f & 7)};
-            const int raw{q * 64 + slot};  // even; raw + 1 is in the same row
+            const int raw{q * 64 + slot};  // a multiple of 4
             const bool llf_row{(raw >> lrow) < side};
             const int col{raw & (n - 1)};
-            const bool llf[2]{llf_row && col < side, llf_row && col + 1 < side};
-            if (!(llf[0] && llf[1])) {
+            if (!(llf_row && col + 3 < side)) {
                 const int si{n == 8 ? 0 : (n == 16 ? 1 : 2)};
                 const float* wt{tb.dequant + si * 3072};
                 const float qgsf{static_cast<float>(sm.qf[f]) * sc.gsf};
                 const int ci{lb * kCoefBlock + slot};
-                const float2 xr{__half22float2(*reinterpret_cast<const __half2*>(coef + ci))};
-                const float2 yr{__half22float2(*reinterpret_cast<const __half2*>(coef + kCoefStride + ci))};
-                const float2 br{__half22float2(*reinterpret_cast<const __half2*>(coef + 2 * kCoefStride + ci))};
-                const float2 wx{*reinterpret_cast<const float2*>(wt + raw)};
-                const float2 wy{*reinterpret_cast<const float2*>(wt + 1024 + raw)};
-                const float2 wb{*reinterpret_cast<const float2*>(wt + 2048 + raw)};
+                auto load4 = [&](const __half* plane, float (&v)[4]) {
+                    const float2 lo{__half22float2(*reinterpret_cast<const __half2*>(plane + ci))};
+                    const float2 hi{__half22float2(*reinterpret_cast<const __half2*>(plane + ci + 2))};
+                    v[0] = lo.x;
+                    v[1] = lo.y;
+                    v[2] = hi.x;
+                    v[3] = hi.y;
+                };
+                float xr[4], yr[4], br[4];
+                load4(coef, xr);
+                load4(coef + kCoefStride, yr);
+                load4(coef + 2 * kCoefStride, br);
+                const float4 wx4{*reinterpret_cast<const float4*>(wt + raw)};
+                const float4 wy4{*reinterpret_cast<const float4*>(wt + 1024 + raw)};
+                const float4 wb4{*reinterpret_cast<const float4*>(wt + 2048 + raw)};
+                const float wx[4]{wx4.x, wx4.y, wx4.z, wx4.w};
+                const float wy[4]{wy4.x, wy4.y, wy4.z, wy4.w};
+                const float wb[4]{wb4.x, wb4.y, wb4.z, wb4.w};
 #pragma unroll
-                for (int h{0}; h < 2; ++h) {
-                    if (llf[h]) continue;
-                    const float wyh{h == 0 ? wy.x : wy.y};
-                    const int qy{quantize(h == 0 ? yr.x : yr.y, qgsf, wyh)};
+                for (int h{0}; h < 4; ++h) {
+                    if (llf_row && col + h < side) continue;  // an LLF slot
+                    const int qy{quantize(yr[h], qgsf, wy[h])};
                     // A zero Y quantum reconstructs to a signed zero, and
                     // fma(-m, +-0, v) equals v up to the sign of a zero
                     // result, which quantises to 0 either way.
-                    const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wyh) / qgsf};
-                    const int qx{quantize(jx_fma(-ytox, yq, h == 0 ? xr.x : xr.y), qgsf, h == 0 ? wx.x : wx.y)};
-                    const int qb{quantize(jx_fma(-ytob, yq, h == 0 ? br.x : br.y), qgsf, h == 0 ? wb.x : wb.y)};
-                    ax[h] = static_cast<std::int16_t>(qx);
+                    const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy[h]) / qgsf};
+                    ax[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytox, yq, xr[h]), qgsf, wx[h]));
                     ay[h] = static_cast<std::int16_t>(qy);
-                    ab[h] = static_cast<std::int16_t>(qb);
+                    ab[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytob, yq, br[h]), qgsf, wb[h]));
                 }
             }
             const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
-            *reinterpret_cast<short2*>(out.ac + g) = make_short2(ax[0], ax[1]);
-            *reinterpret_cast<short2*>(out.ac + cplane + g) = make_short2(ay[0], ay[1]);
-            *reinterpret_cast<short2*>(out.ac + 2 * cplane + g) = make_short2(ab[0], ab[1]);
+            *reinterpret_cast<short4*>(out.ac + g) = make_short4(ax[0], ax[1], ax[2], ax[3]);
+            *reinterpret_cast<short4*>(out.ac + cplane + g) = make_short4(ay[0], ay[1], ay[2], ay[3]);
+            *reinterpret_cast<short4*>(out.ac + 2 * cplane + g) = make_short4(ab[0], ab[1], ab[2], ab[3]);
         }
-        // Non-zero counts per first block: the 32 pairs of a warp's iteration
-        // are the 64 slots of tile block warp + 8j, so the whole warp shares
-        // f, and lane 0 adds the warp's counts.
-        const int cx{__popc(__ballot_sync(0xffffffffu, ax[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ax[1] != 0))};
-        const int cy{__popc(__ballot_sync(0xffffffffu, ay[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ay[1] != 0))};
-        const int cb{__popc(__ballot_sync(0xffffffffu, ab[0] != 0)) + __popc(__ballot_sync(0xffffffffu, ab[1] != 0))};
-        if (lane == 0 && f >= 0) {
-            if (cx) atomicAdd(&sm.nz[0][f], cx);
-            if (cy) atomicAdd(&sm.nz[1][f], cy);
-            if (cb) atomicAdd(&sm.nz[2][f], cb);
+        // Non-zero counts per first block: each half-warp's 64 slots are one
+        // tile block, so lanes 0 and 16 add their half's counts.
+        auto nonzero = [](const std::int16_t (&v)[4]) {
+            return static_cast<unsigned>((v[0] != 0) + (v[1] != 0) + (v[2] != 0) + (v[3] != 0));
+        };
+        const unsigned lo_half{lane < 16 ? 1u : 0u};
+        const unsigned nx{nonzero(ax)};
+        const unsigned ny{nonzero(ay)};
+        const unsigned nbz{nonzero(ab)};
+        const unsigned cx_lo{__reduce_add_sync(0xffffffffu, lo_half * nx)};
+        const unsigned cx_hi{__reduce_add_sync(0xffffffffu, (1u - lo_half) * nx)};
+        const unsigned cy_lo{__reduce_add_sync(0xffffffffu, lo_half * ny)};
+        const unsigned cy_hi{__reduce_add_sync(0xffffffffu, (1u - lo_half) * ny)};
+        const unsigned cb_lo{__reduce_add_sync(0xffffffffu, lo_half * nbz)};
+        const unsigned cb_hi{__reduce_add_sync(0xffffffffu, (1u - lo_half) * nbz)};
+        if ((lane & 15) == 0 && f >= 0) {
+            const unsigned cx{lo_half ? cx_lo : cx_hi};
+            const unsigned cy{lo_half ? cy_lo : cy_hi};
+            const unsigned cb{lo_half ? cb_lo : cb_hi};
+            if (cx) atomicAdd(&sm.nz[0][f], static_cast<int>(cx));
+            if (cy) atomicAdd(&sm.nz[1][f], static_cast<int>(cy));
+            if (cb) atomicAdd(&sm.nz[2][f], static_cast<int>(cb));
         }
     }
     __syncthreads();
