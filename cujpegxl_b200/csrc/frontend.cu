@@ -1362,15 +1362,19 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __syncthreads();
     if (warp == 0) {
-        const float sxy{warp_tree(sm.cfl[0][lane] + sm.cfl[0][lane + 32])};
-        const float syy{warp_tree(sm.cfl[1][lane] + sm.cfl[1][lane + 32])};
+        const float2 sxy_yy{warp_tree2(__fadd2_rn(make_float2(sm.cfl[0][lane], sm.cfl[1][lane]),
+                                                  make_float2(sm.cfl[0][lane + 32], sm.cfl[1][lane + 32])))};
+        const float sxy{sxy_yy.x};
+        const float syy{sxy_yy.y};
         const float sby{warp_tree(sm.cfl[2][lane] + sm.cfl[2][lane + 32])};
         if (lane == 0) {
-            const double dxy{sxy};
-            const double dyy{syy};
-            const double dby{sby};
-            const float fx{dyy > 0.0 ? static_cast<float>(dxy / dyy) : 0.0f};
-            const float fb{dyy > 0.0 ? static_cast<float>(dby / dyy) : 0.0f};
+            // The reference divides the float sums in double and rounds the
+            // quotient to float; with 53 >= 2 * 24 + 2 significand bits that
+            // double rounding equals float division's single rounding
+            // (Figueroa, "When is double rounding innocuous?", SIGNUM 1995),
+            // so the float quotient is the same value.
+            const float fx{syy > 0.0f ? sxy / syy : 0.0f};
+            const float fb{syy > 0.0f ? sby / syy : 0.0f};
             int mx{static_cast<int>(lrintf(fx * static_cast<float>(kCflColorFactor)))};
             int mb{static_cast<int>(lrintf(fb * static_cast<float>(kCflColorFactor)))};
             mx = mx < -128 ? -128 : (mx > 127 ? 127 : mx);
