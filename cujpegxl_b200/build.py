@@ -25,7 +25,7 @@ LIB = OUT_DIR / "libcujpegxl.so.1"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["frontend.cu", "entropy.cu", "entropy_host.cu", "cujpegxl.cu", "noalloc.cu", "batch.cu", "acsnet.cu"]
-HEADERS = ["frontend.cuh", "entropy.cuh", "acsnet.cuh", "xyb.cuh", "ratio_div.cuh", "jxl_constants.cuh", "jxl_math.cuh", "prefix_code.cuh", "encoder_internal.h",
+HEADERS = ["frontend.cuh", "entropy.cuh", "acsnet.cuh", "xyb.cuh", "ratio_div.cuh", "f16_mixed.cuh", "jxl_constants.cuh", "jxl_math.cuh", "prefix_code.cuh", "encoder_internal.h",
            "jxl_dequant_tables.inc", "cujpegxl.map"]
 
 

@@ -21,6 +21,7 @@
 #include "frontend.cuh"
 #include "jxl_constants.cuh"
 #include "jxl_math.cuh"
+#include "f16_mixed.cuh"
 #include "ratio_div.cuh"
 #include "xyb.cuh"
 
@@ -137,11 +138,6 @@ __device__ __forceinline__ float ratio_gamma(float v) {
     const float num{jx_fma(kRatioNumMul, v2, kRatioEps)};
     const float den{jx_fma(kRatioDenMul * v, v2, kRatioVOffset)};
     return kInvert ? num / den : den / num;
-}
-
-// src/adaptive_quant_impl.cuh:57-61.
-__device__ __forceinline__ float masking_sqrt(float v, float sqrt_mul) {
-    return 0.25f * sqrtf(jx_fma(v, sqrt_mul, kMaskLogOffset));
 }
 
 // src/adaptive_quant_impl.cuh:63-76.
@@ -385,21 +381,6 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
         const int lb{(fby + q / side) * 8 + fbx + q % side};
         *reinterpret_cast<__half2*>(coef + lb * kCoefBlock + (raw & 63)) = __floats2half2_rn(c2.x, c2.y);
     }
-}
-
-// Mixed-precision forms (sm_100): the FP16 operands are widened exactly inside
-// the instruction, so fma_f16(a, b, c) is fmaf(float(a), float(b), c) and
-// add_f16(a, c) is float(a) + c, each rounded once, without separate
-// conversions.
-__device__ __forceinline__ float fma_f16(unsigned short a, unsigned short b, float c) {
-    float d;
-    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(a), "h"(b), "f"(c));
-    return d;
-}
-__device__ __forceinline__ float add_f16(unsigned short a, float c) {
-    float d;
-    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(a), "f"(c));
-    return d;
 }
 
 // One CfL sum of a side-N first block lb over its non-LLF coefficients in raw
@@ -737,7 +718,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 float2 d{__fmul2_rn(ratio, __fadd2_rn(yv, f2neg(base)))};
                 d = __fmul2_rn(d, d);
                 d = make_float2(fminf(d.x, kDiffLimit), fminf(d.y, kDiffLimit));
-                // masking_sqrt(d, mask_sqrt_mul)
+                // Masking square root 0.25 * sqrt(d * mul + offset) (src/adaptive_quant_impl.cuh:57-61).
                 const float2 t{__ffma2_rn(d, f2dup(sc.mask_sqrt_mul), f2dup(kMaskLogOffset))};
                 const float2 m{__fmul2_rn(f2dup(0.25f), make_float2(sqrtf(t.x), sqrtf(t.y)))};
                 sum = sum + m.x;
