@@ -215,6 +215,19 @@ struct StripeStage {
     int nactive;
 };
 
+// Asynchronous global -> shared copies (cp.async, sm_80 and later): a thread
+// issues all of its copies before waiting once for them (cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned dst{static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))};
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+    const unsigned dst{static_cast<unsigned>(__cvta_generic_to_shared(smem_dst))};
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The caller's barrier after this publishes the stage to the whole CTA.
 __device__ void stage_stripe(const EntropyDev& e, const Stripe& st, const GroupGeom& gg, StripeStage& s) {
     const int tid{static_cast<int>(threadIdx.x)};
     const int vpr{gg.gw * (kCoeffsPerBlock * 2 / 16)};  // 16-byte vectors per block row
@@ -224,11 +237,11 @@ __device__ void stage_stripe(const EntropyDev& e, const Stripe& st, const GroupG
             const std::size_t blk0{static_cast<std::size_t>(gg.by0 + st.r0 + r) * e.bw + gg.bx0};
             const uint4* src{reinterpret_cast<const uint4*>(plane + blk0 * kCoeffsPerBlock)};
             uint4* dst{reinterpret_cast<uint4*>(&s.coef[c][r][0])};
-            for (int v{tid}; v < vpr; v += kAcThreads) dst[v] = __ldg(&src[v]);
+            for (int v{tid}; v < vpr; v += kAcThreads) cp_async16(&dst[v], &src[v]);
         }
     }
     for (int i{tid}; i < (64 + 256 + 1024) / 2; i += kAcThreads) {
-        reinterpret_cast<std::uint32_t*>(s.order)[i] = __ldg(&reinterpret_cast<const std::uint32_t*>(e.order)[i]);
+        cp_async4(&reinterpret_cast<std::uint32_t*>(s.order)[i], &reinterpret_cast<const std::uint32_t*>(e.order)[i]);
     }
     const int cells{st.rows * gg.gw};
     for (int i{tid}; i < cells; i += kAcThreads) {
@@ -244,6 +257,7 @@ __device__ void stage_stripe(const EntropyDev& e, const Stripe& st, const GroupG
         }
     }
     if (tid == 0) s.nactive = 0;
+    cp_async_wait_all();
 }
 
 // Stripe-local item j: block (bx, by) of the stripe, plane c.
