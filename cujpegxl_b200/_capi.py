@@ -42,6 +42,7 @@ EXPORTS = (
     "cujpegxl_b200_acsnet_trainer_forward", "cujpegxl_b200_acsnet_trainer_gradient",
     "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params", "cujpegxl_b200_batch_set_acsnet",
     "cujpegxl_b200_encoder_create_ex", "cujpegxl_b200_max_output_size_ex",
+    "cujpegxl_b200_debug_fail_allocation", "cujpegxl_b200_debug_live_allocations",
 )
 
 
@@ -107,6 +108,9 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_encoder_result.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encoder_stream.argtypes = [E, P(ctypes.c_size_t)]
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
+    L.cujpegxl_b200_debug_fail_allocation.argtypes = [ctypes.c_uint32]
+    L.cujpegxl_b200_debug_fail_allocation.restype = None
+    L.cujpegxl_b200_debug_live_allocations.restype = ctypes.c_uint64
     L.cujpegxl_b200_encoder_memory.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encode_planes_noalloc.argtypes = [P(DevicePlanes), ctypes.c_uint32, ctypes.c_uint32,
                                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -67,6 +68,60 @@ struct DeviceTables {
 
 std::mutex g_mutex;
 DeviceTables g_tables[64];
+
+// Encoder resources (device arenas, pinned host buffers, streams) go through
+// these wrappers: they count what is live, and a test hook can make the n-th
+// acquisition fail as a real out-of-memory would, to exercise the error paths
+// of create and configure (cujpegxl_b200_debug_fail_allocation).
+std::atomic<std::uint32_t> g_fail_countdown{0};
+std::atomic<std::uint64_t> g_live{0};
+
+bool injected_failure() {
+    std::uint32_t n{g_fail_countdown.load()};
+    while (n != 0) {
+        if (g_fail_countdown.compare_exchange_weak(n, n - 1)) return n == 1;
+    }
+    return false;
+}
+
+bool acquire_device(void** p, std::size_t bytes) {
+    if (injected_failure() || cudaMalloc(p, bytes) != cudaSuccess) {
+        *p = nullptr;
+        return false;
+    }
+    ++g_live;
+    return true;
+}
+
+bool acquire_pinned(void** p, std::size_t bytes) {
+    if (injected_failure() || cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        *p = nullptr;
+        return false;
+    }
+    ++g_live;
+    return true;
+}
+
+bool acquire_stream(cudaStream_t* s) {
+    if (injected_failure() || cudaStreamCreateWithFlags(s, cudaStreamNonBlocking) != cudaSuccess) {
+        *s = nullptr;
+        return false;
+    }
+    ++g_live;
+    return true;
+}
+
+void release_device(void* p) {
+    if (p != nullptr && cudaFree(p) == cudaSuccess) --g_live;
+}
+
+void release_pinned(void* p) {
+    if (p != nullptr && cudaFreeHost(p) == cudaSuccess) --g_live;
+}
+
+void release_stream(cudaStream_t s) {
+    if (s != nullptr && cudaStreamDestroy(s) == cudaSuccess) --g_live;
+}
 
 // Restores the caller's current device on scope exit.
 class DeviceScope {
@@ -137,8 +192,8 @@ struct ArenaPlan {
 };
 
 void release(cujpegxl_encoder* e) {
-    if (e->arena) cudaFree(e->arena);
-    if (e->nv12_pinned) cudaFreeHost(e->nv12_pinned);
+    release_device(e->arena);
+    release_pinned(e->nv12_pinned);
     e->arena = nullptr;
     e->nv12_pinned = nullptr;
     e->geo_w = e->geo_h = 0;
@@ -203,7 +258,7 @@ bool allocate(cujpegxl_encoder* e) {
         o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2 + 3 * nb * 4);
     }
     void* base{nullptr};
-    if (cudaMalloc(&base, a.total) != cudaSuccess) return false;
+    if (!acquire_device(&base, a.total)) return false;
     e->arena = base;
     e->arena_bytes = a.total;
     auto* b{static_cast<std::uint8_t*>(base)};
@@ -300,8 +355,7 @@ bool allocate(cujpegxl_encoder* e) {
                 cudaSuccess &&
             cudaMemcpy(b + o_acp, plan.ac_prefix.data(), plan.ac_prefix.size(), cudaMemcpyHostToDevice) ==
                 cudaSuccess};
-    ok = ok && cudaHostAlloc(reinterpret_cast<void**>(&e->nv12_pinned),
-                             static_cast<std::size_t>(W) * H * 3 / 2 + 64, cudaHostAllocDefault) == cudaSuccess;
+    ok = ok && acquire_pinned(reinterpret_cast<void**>(&e->nv12_pinned), static_cast<std::size_t>(W) * H * 3 / 2 + 64);
     if (!ok) {
         release(e);
         return false;
@@ -519,8 +573,8 @@ cujpegxl_status cujpegxl_b200_encoder_create_ex(const cujpegxl_config* config, u
     DeviceScope scope{e->device};
     jxb::FrontendTables ft{};
     if (!scope.ok() || !device_tables(e->device, &ft) ||
-        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess || !prepare(e)) {
-        if (e->stream) cudaStreamDestroy(e->stream);
+        !acquire_stream(&e->stream) || !prepare(e)) {
+        release_stream(e->stream);
         release(e);
         delete e;
         return CUJPEGXL_INTERNAL_ERROR;
@@ -539,15 +593,13 @@ cujpegxl_status cujpegxl_encoder_configure(cujpegxl_encoder* encoder, const cujp
         if (!device_exists(config->device_ordinal, &major, &minor)) return CUJPEGXL_NO_DEVICE;
         DeviceScope old{encoder->device};
         cudaStreamSynchronize(encoder->stream);
-        cudaStreamDestroy(encoder->stream);
+        release_stream(encoder->stream);
         encoder->stream = nullptr;
         release(encoder);
         encoder->device = config->device_ordinal;
         encoder->net = nullptr;  // a network lives on one device
         DeviceScope scope{encoder->device};
-        if (cudaStreamCreateWithFlags(&encoder->stream, cudaStreamNonBlocking) != cudaSuccess) {
-            return CUJPEGXL_INTERNAL_ERROR;
-        }
+        if (!acquire_stream(&encoder->stream)) return CUJPEGXL_INTERNAL_ERROR;
     }
     encoder->config = *config;
     DeviceScope scope{encoder->device};
@@ -581,7 +633,7 @@ void cujpegxl_encoder_destroy(cujpegxl_encoder* encoder) {
         DeviceScope scope{encoder->device};
         if (encoder->stream) {
             cudaStreamSynchronize(encoder->stream);
-            cudaStreamDestroy(encoder->stream);
+            release_stream(encoder->stream);
         }
         release(encoder);
     }
@@ -756,6 +808,10 @@ cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* 
 }
 
 uint32_t cujpegxl_b200_kernels_per_encode(void) { return 12u; }
+
+void cujpegxl_b200_debug_fail_allocation(uint32_t nth) { g_fail_countdown.store(nth); }
+
+uint64_t cujpegxl_b200_debug_live_allocations(void) { return g_live.load(); }
 
 cujpegxl_status cujpegxl_b200_encoder_set_acsnet(cujpegxl_encoder* encoder, const cujpegxl_b200_acsnet* net,
                                                  float margin, uint32_t flags) {

@@ -1,14 +1,14 @@
 // Entropy coding and assembly from device planes without any allocation.
 //
-// Some callers cannot allocate device memory while they encode: code running
-// inside a CUDA graph capture or a real-time serving loop where cudaMalloc
-// would synchronise the device or is forbidden, and embedders whose device
-// memory is fully reserved by their own pool. For them,
-// cujpegxl_b200_encode_planes_noalloc takes the quantised planes and the output
-// buffer from the caller and keeps every intermediate (non-zero counts,
-// section table, histograms, prefix codes, per-item bit lengths and their
-// scan) in one file-scope __device__ array of kScratchBytes. Every GPU that
-// loads the library holds that array until the process exits.
+// Some callers cannot allocate device memory while they encode: a real-time
+// loop where cudaMalloc would synchronise the whole device and stall other
+// streams, or an embedder whose device memory is entirely reserved by its own
+// pool allocator. For them, cujpegxl_b200_encode_planes_noalloc takes the
+// quantised planes and the output buffer from the caller and keeps every
+// intermediate (non-zero counts, section table, histograms, prefix codes,
+// per-item bit lengths and their scan) in one file-scope __device__ array of
+// kScratchBytes. Every GPU that loads the library holds that array until the
+// process exits. The call synchronises its stream before it returns.
 
 #include <cuda_runtime.h>
 
@@ -87,7 +87,8 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
                                                     size_t* out_size, uintptr_t stream) {
     if (planes == nullptr || out_device == nullptr || out_size == nullptr || planes->ac == 0 ||
         planes->dc == 0 || planes->acs == 0 || planes->qf == 0 || planes->ytox == 0 || planes->ytob == 0 ||
-        (reinterpret_cast<std::uintptr_t>(out_device) & 15u) != 0 || (planes->ac & 15u) != 0) {
+        (reinterpret_cast<std::uintptr_t>(out_device) & 15u) != 0 || (planes->ac & 15u) != 0 ||
+        (planes->dc & 3u) != 0 || (planes->qf & 3u) != 0) {
         return CUJPEGXL_INVALID_ARGUMENT;
     }
     if (width == 0 || height == 0 || width % 8 != 0 || height % 8 != 0 ||

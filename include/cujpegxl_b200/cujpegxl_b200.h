@@ -113,13 +113,15 @@ typedef struct cujpegxl_b200_device_planes {
 /* No counterpart in the reference. Entropy coding and assembly of one frame
  * from quantised planes already in device memory, producing the same file as
  * cujpegxl_b200_encode_planes, for callers that cannot allocate device memory
- * while they encode (inside a stream capture, in a real-time loop where
- * cudaMalloc would synchronise the device, or with all device memory held by
- * their own pool). It allocates nothing: the caller passes the planes (the AC
- * plane 16-byte aligned, as every cudaMalloc'd buffer is) and a device output
- * buffer (16-byte aligned, `out_capacity` bytes), and every
- * intermediate lives in one fixed 7 MiB array that each GPU loading the
- * library holds until the process exits.
+ * while they encode: a real-time loop where cudaMalloc would synchronise the
+ * whole device and stall other streams, or an embedder whose device memory is
+ * entirely reserved by its own pool allocator. It allocates nothing: the
+ * caller passes the planes and a device output buffer (`out_capacity` bytes),
+ * and every intermediate lives in one fixed 7 MiB array that each GPU loading
+ * the library holds until the process exits.
+ *  - Alignment: the AC plane and the output buffer 16-byte aligned, the DC
+ *    and quant-field planes 4-byte aligned (every cudaMalloc'd buffer is);
+ *    other addresses give CUJPEGXL_INVALID_ARGUMENT.
  *  - Frames above 4,194,304 pixels (width*height) are rejected with
  *    CUJPEGXL_UNSUPPORTED_RESOLUTION; other geometry rules are those of
  *    cujpegxl_encoder_create.
@@ -128,8 +130,9 @@ typedef struct cujpegxl_b200_device_planes {
  *  - Calls share the array: calls that overlap on the GPU (different streams
  *    or threads without ordering) race and corrupt each other's output.
  *  - Work is enqueued on `stream` (a cudaStream_t as an integer, 0 for the
- *    default stream); the call waits for it and sets *out_size to the file
- *    length, or to the required length with CUJPEGXL_BUFFER_TOO_SMALL. */
+ *    default stream); the call then synchronises `stream`, reads the result
+ *    words back and sets *out_size to the file length, or to the required
+ *    length with CUJPEGXL_BUFFER_TOO_SMALL. */
 cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_planes* planes,
                                                     uint32_t width, uint32_t height,
                                                     uint32_t global_scale, uint32_t quant_dc,
@@ -138,6 +141,17 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
 
 /* Number of kernels one encode launches. */
 uint32_t cujpegxl_b200_kernels_per_encode(void);
+
+/* Test hooks for the error paths of encoder creation (the reference has no
+ * counterpart; its tests cover only argument errors). After
+ * cujpegxl_b200_debug_fail_allocation(n) with n > 0, the n-th device arena,
+ * pinned host buffer or CUDA stream that an encoder acquires from then on fails
+ * as an out-of-memory would; n = 0 turns the injection off. The count of such
+ * resources that encoders currently hold is
+ * cujpegxl_b200_debug_live_allocations(): a failed cujpegxl_encoder_create
+ * must leave it where it was. */
+void cujpegxl_b200_debug_fail_allocation(uint32_t nth);
+uint64_t cujpegxl_b200_debug_live_allocations(void);
 
 /* Device memory the encoder holds for its current geometry (one arena, all of
  * it allocated at create/configure) and its pinned host staging buffer

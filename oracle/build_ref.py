@@ -19,8 +19,10 @@ import subprocess
 import sys
 from pathlib import Path
 
-REFERENCE = Path(os.environ.get("CUJPEGXL_REFERENCE", "/root/reference"))
 HERE = Path(__file__).resolve().parent
+# The reference checkout: CUJPEGXL_REFERENCE, else a "reference" directory
+# beside this repository's root.
+REFERENCE = Path(os.environ.get("CUJPEGXL_REFERENCE", HERE.parent.parent / "reference"))
 OUT_DIR = HERE / "_ref"
 OUT = OUT_DIR / "libjxlref.so"
 

@@ -1,7 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout where the reference tree is present (default
-/root/reference, override with CUJPEGXL_REFERENCE):
+Run where the reference tree is present (CUJPEGXL_REFERENCE, else a
+"reference" directory beside this repository's root):
 
     python tests/golden/make_golden.py
 
@@ -41,7 +41,7 @@ from oracle import build as obuild  # noqa: E402
 
 import patterns as P  # noqa: E402
 
-REFERENCE = Path(os.environ.get("CUJPEGXL_REFERENCE", "/root/reference"))
+REFERENCE = Path(os.environ.get("CUJPEGXL_REFERENCE", REPO.parent / "reference"))
 
 
 def f32bits(x) -> list[int]:
