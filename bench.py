@@ -1,28 +1,44 @@
 #!/usr/bin/env python
-"""4K NV12 -> JPEG XL VarDCT encode throughput on B200.
+"""4K NV12 -> JPEG XL VarDCT encode throughput on B200, with every workload of
+the benchmark set measured in the same run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--streams S]
+                    [--no-extras] [--workload 4k|mixed64]
 
-Workload: the seeded synthetic 3840x2160 NV12 frame (seed 0), distance 1.0,
-the plain path (XYB, AQ, gaborish, transform selection, DCT, CfL, quantise,
-histograms, prefix codes, packing, headers). One step encodes a batch of 16
-device-resident copies of that frame, frame i on encoder i % S (S encoders,
-each with its own CUDA stream and device arena, default 4); the 16 distinct
-input buffers (199 MB) exceed the 126 MB L2, so no step reads its input from
-L2.
-
-value: frames/s over exactly K steps, CUDA events (start on the first
+Headline (`value`): the seeded synthetic 3840x2160 NV12 frame (seed 0),
+distance 1.0, the plain path (XYB, AQ, gaborish, transform selection, DCT,
+CfL, quantise, histograms, prefix codes, packing, headers). One step encodes
+a batch of 16 device-resident copies of that frame, frame i on encoder i % S
+(S encoders, each with its own CUDA stream and device arena, default 4); the
+16 distinct input buffers (199 MB) exceed the 126 MB L2, so no step reads its
+input from L2. frames/s over exactly K steps, CUDA events (start on the first
 encoder's stream, the others wait on it and are joined back before the stop
 event), barrier + synchronize on both sides, max over ranks (one process per
 GPU, independent replicas: frames do not shard, so there is no collective).
-p50/p99 frame latency and the frontend/entropy split: one encoder alone,
-events around each stage of each frame.
-e2e: the same metric through the public C ABI with host buffers, one host
-thread per encoder: every frame is copied host->device from pinned memory,
-encoded with cujpegxl_encoder_encode and its file copied back to pinned host
-memory.
+
+latency: one encoder alone, 128 frames back to back, events around each
+frame (and its frontend stage); n/mean/stddev/min/p50/p99/max as the
+reference's benchmark prints them (tools/benchmark/encode_bench.cc:376-390).
+e2e: the same metric through the reference's C ABI with host buffers, one
+host thread per encoder: every frame is copied host->device from pinned
+memory, encoded with cujpegxl_encoder_encode and its file copied back to
+pinned host memory.
 roofline: the fused frontend kernel, its algorithmic bytes per 4K frame over
 its event-timed duration, against the measured HBM copy bandwidth.
+
+Extras (N = 1, rank 0; --no-extras skips them), each timed in this run:
+  distances: the 4K frame at d = 0.5, 2 and 4 (frames/s over the same step,
+    bpp, PSNR-Y through the in-repo decoder);
+  learned: the 4K step with the shipped transform-decision network (split
+    only, and split + quant field), and the bpp change at equal PSNR-Y against
+    the plain heuristic at d = 1 and 2 on held-out frames (log-bpp
+    interpolated over the network's encodes at d x 0.8 .. 1.25);
+  mixed64: the 64-frame uneven-resolution batch in one launch per step,
+    plain and learned;
+  serving: the 8-stream serving workload (2 x 4K@30, 4 x 1080p@60,
+    2 x 720p@60, Poisson arrivals, 40 GB budget) at 1x for 3 s (>= 1000
+    frames) and at rising speeds until it no longer keeps up, plain and
+    learned; p50/p99 latency and sustained frames/s.
 --impl reference: the CPU encoder restated from the reference (the reference
 has no CPU implementation of its device stages) run with every host core on
 the same frame, rank 0 only.
@@ -37,6 +53,7 @@ import statistics
 import subprocess
 import sys
 import time
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -46,7 +63,9 @@ sys.path.insert(0, str(REPO))
 
 W_4K, H_4K = 3840, 2160
 BATCH = 16
+LATENCY_FRAMES = 128
 PUBLISHED_FPS = 15.0  # reference README.md:17, GTX 1080 Ti, 4K sustained
+HELD_OUT = [(3840, 2160, 0), (1920, 1080, 424242)]  # frames outside the network's training and validation seeds
 
 
 def frontend_algorithmic_bytes(w: int, h: int) -> int:
@@ -95,7 +114,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"bench_clocks_{os.getpid()}.csv"
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"bench_clocks_{os.getpid()}_{id(self)}.csv"
 
     def __enter__(self):
         try:
@@ -166,6 +185,15 @@ def dist_setup():
     return world, rank, local
 
 
+def psnr_many(pairs: list[tuple[np.ndarray, bytes]]) -> list[float]:
+    """PSNR-Y of each (nv12, file) through the in-repo decoder, decoded on every
+    host core at once (the decoder releases the interpreter while it runs)."""
+    from cujpegxl_b200.decode import psnr_y
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(pairs), os.cpu_count() or 1))) as pool:
+        return list(pool.map(lambda p: psnr_y(p[0], p[1]), pairs))
+
+
 def cpu_baseline(nv12, w, h, d, runs: int) -> dict:
     from oracle import api
 
@@ -211,6 +239,75 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+class Step:
+    """S encoders over one set of device frames; one step = BATCH frames,
+    frame i on encoder i % S."""
+
+    def __init__(self, encs, frames, W, H):
+        import torch
+
+        self.encs, self.frames, self.W, self.H = encs, frames, W, H
+        self.streams = [torch.cuda.ExternalStream(e.stream()) for e in encs]
+        self.joins = [torch.cuda.Event() for _ in encs]
+
+    def enqueue(self):
+        S = len(self.encs)
+        for i, (lm, ch) in enumerate(self.frames):
+            self.encs[i % S].enqueue(lm.data_ptr(), ch.data_ptr(), self.W, self.W)
+
+    def drain(self):
+        for e in self.encs:
+            e.result()
+
+    def timed(self, steps: int, warmup: int, pg=None) -> float:
+        """ms for `steps` steps after `warmup` untimed ones, CUDA events on the
+        first stream (the others fork from and join into it)."""
+        import torch
+
+        for _ in range(warmup):
+            self.enqueue()
+        self.drain()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        start.record(self.streams[0])
+        for st in self.streams[1:]:
+            st.wait_event(start)
+        for _ in range(steps):
+            self.enqueue()
+        for ev, st in zip(self.joins[1:], self.streams[1:]):
+            ev.record(st)
+            self.streams[0].wait_event(ev)
+        stop.record(self.streams[0])
+        self.drain()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        return start.elapsed_time(stop)
+
+    def stage_times(self, n: int) -> tuple[list[float], list[float]]:
+        """(frontend ms, whole-frame ms) of n frames on the first encoder alone."""
+        import torch
+
+        enc, stream = self.encs[0], self.streams[0]
+        ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(n + 1)]
+        ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        torch.cuda.synchronize()
+        for i in range(n):
+            lm, ch = self.frames[i % len(self.frames)]
+            ev_a[i].record(stream)
+            enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), self.W, self.W, 1)
+            ev_b[i].record(stream)
+            enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), self.W, self.W, 2)
+        ev_a[n].record(stream)
+        enc.result()
+        torch.cuda.synchronize()
+        return ([ev_a[i].elapsed_time(ev_b[i]) for i in range(n)],
+                [ev_a[i].elapsed_time(ev_a[i + 1]) for i in range(n)])
+
+
 def run_ours(args) -> None:
     import threading
 
@@ -228,6 +325,7 @@ def run_ours(args) -> None:
         pg = dist
 
     from cujpegxl_b200 import Encoder, _capi
+    from cujpegxl_b200.serve import latency_stats
     from cujpegxl_b200.synth import make_nv12
 
     W, H, d = args.width, args.height, args.distance
@@ -242,63 +340,21 @@ def run_ours(args) -> None:
     # step goes to encoder i % S, so one frame's small entropy kernels overlap
     # another frame's frontend.
     encs = [Encoder(W, H, d, local) for _ in range(S)]
-    streams = [torch.cuda.ExternalStream(e.stream()) for e in encs]
+    step = Step(encs, frames, W, H)
+    streams = step.streams
     kernels = int(_capi.lib().cujpegxl_b200_kernels_per_encode())
 
-    def enqueue_step():
-        for i, (lm, ch) in enumerate(frames):
-            encs[i % S].enqueue(lm.data_ptr(), ch.data_ptr(), W, W)
-
-    for _ in range(args.warmup):
-        enqueue_step()
-    size = encs[0].result()[0]
-    for e in encs[1:]:
-        e.result()
-
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
-    joins = [torch.cuda.Event() for _ in streams]
     with ClockSampler(local) as clocks:
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
-        start.record(streams[0])
-        for st in streams[1:]:
-            st.wait_event(start)
-        for _ in range(args.steps):
-            enqueue_step()
-        for ev, st in zip(joins[1:], streams[1:]):
-            ev.record(st)
-            streams[0].wait_event(ev)
-        stop.record(streams[0])
-        for e in encs:
-            e.result()
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-    total_ms = start.elapsed_time(stop)
+        total_ms = step.timed(args.steps, args.warmup, pg)
     clock_summary = clocks.summary()
     clocks_mhz = clock_summary.get("sm_mhz")
+    size = encs[0].result()[0]
     n = args.steps * BATCH
     total_ms = max_over_ranks(total_ms, pg, "cuda")
     value = whole_job_rate(n, world, total_ms)
 
-    # Per-frame latency and the frontend/entropy split: one encoder alone,
-    # events around each stage of each frame.
-    enc, stream = encs[0], streams[0]
-    ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(BATCH + 1)]
-    ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(BATCH)]
-    torch.cuda.synchronize()
-    for i, (lm, ch) in enumerate(frames):
-        ev_a[i].record(stream)
-        enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 1)
-        ev_b[i].record(stream)
-        enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 2)
-    ev_a[BATCH].record(stream)
-    enc.result()
-    torch.cuda.synchronize()
-    front = [ev_a[i].elapsed_time(ev_b[i]) for i in range(BATCH)]
-    frame_ms = [ev_a[i].elapsed_time(ev_a[i + 1]) for i in range(BATCH)]
+    # Per-frame latency and the frontend/entropy split: one encoder alone.
+    front, frame_ms = step.stage_times(LATENCY_FRAMES)
 
     # End to end through the C ABI with host buffers, one host thread per
     # encoder: pinned host NV12 -> device, cujpegxl_encoder_encode, file -> host.
@@ -337,62 +393,13 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(max(e0.elapsed_time(dn) for dn in dones), pg, "cuda")
     e2e = whole_job_rate((e2e_n // S) * S, world, e2e_ms)
-
-    # The same step with learned transform decisions (the shipped network at
-    # its default margin, split only): device-resident throughput, the
-    # frontend stage with the network's inference in front of it, and the
-    # share of regions the network decided.
-    from cujpegxl_b200.acsnet import DEFAULT_MARGIN, DEFAULT_WEIGHTS, SPLIT, AcsNet
-
-    net = AcsNet.load(device_ordinal=local)
-    for e in encs:
-        e.set_acsnet(net, DEFAULT_MARGIN, SPLIT)
-    for _ in range(args.warmup):
-        enqueue_step()
-    for e in encs:
-        e.result()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    l0 = torch.cuda.Event(enable_timing=True)
-    l1 = torch.cuda.Event(enable_timing=True)
-    l0.record(streams[0])
-    for st in streams[1:]:
-        st.wait_event(l0)
-    for _ in range(args.steps):
-        enqueue_step()
-    for ev, st in zip(joins[1:], streams[1:]):
-        ev.record(st)
-        streams[0].wait_event(ev)
-    l1.record(streams[0])
-    for e in encs:
-        e.result()
-    torch.cuda.synchronize()
-    learned_ms = max_over_ranks(l0.elapsed_time(l1), pg, "cuda")
-    lf = []
-    for lm, ch in frames:
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        enc.enqueue_stages(lm.data_ptr(), ch.data_ptr(), W, W, 1)
-        b.record(stream)
-        lf.append((a, b))
-    enc.result()
-    torch.cuda.synchronize()
-    learned_front = statistics.mean(a.elapsed_time(b) for a, b in lf)
-    decided, regions = enc.acsnet_stats()
-    learned_data = enc.encode_device(frames[0][0].data_ptr(), frames[0][1].data_ptr(), W, W) if rank == 0 else b""
-    for e in encs:
-        e.set_acsnet(None)
-    net.close()
+    e2e_bytes = bytes(outs[0][:d2h[0]].numpy())
 
     front_ms = statistics.mean(front)
     alg = frontend_algorithmic_bytes(W, H)
     achieved = alg / (front_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
-    sorted_ms = sorted(frame_ms)
-    p50 = sorted_ms[len(sorted_ms) // 2]
-    p99 = sorted_ms[min(len(sorted_ms) - 1, int(round(0.99 * (len(sorted_ms) - 1))))]
+    lat = latency_stats(frame_ms)
     in_bytes = BATCH * W * H * 3 // 2
     # The frontend is bound by instruction issue, not HBM: warp instructions
     # per launch (one-pass ncu count at 4K, committed with the DRAM figure)
@@ -406,10 +413,13 @@ def run_ours(args) -> None:
                  "basis": "smsp__inst_executed.sum per 4K frontend launch / event-timed launch; peak = SMs x 4 "
                           "schedulers x median SM clock under load"}
 
+    line = None
     if rank == 0:
         from cujpegxl_b200.decode import psnr_y
 
         data = encs[0].encode_device(frames[0][0].data_ptr(), frames[0][1].data_ptr(), W, W)
+        if e2e_bytes != data:
+            raise AssertionError("the end-to-end file differs from the device-resident encode")
         quality = {"psnr_y_db": psnr_y(nv12, data), "bpp": 8.0 * len(data) / (W * H),
                    "decoder": "in-repo subset decoder, plain dequantisation, BT.709 Y' against the input luma"}
         cpu = None
@@ -427,7 +437,9 @@ def run_ours(args) -> None:
                        "parallelism": f"{world} independent replica(s), {S} streams each"},
             "mp_per_s": value * W * H / 1e6,
             "bytes_per_frame": size, "bpp": 8.0 * size / (W * H), "quality": quality,
-            "p50_frame_ms": p50, "p99_frame_ms": p99, "latency": "one encoder alone, per frame",
+            "p50_frame_ms": lat["p50"], "p99_frame_ms": lat["p99"],
+            "latency": dict(lat, unit="ms", basis=f"one encoder alone, {LATENCY_FRAMES} frames back to back, "
+                                                  "CUDA events around each frame"),
             "frontend_ms": front_ms, "entropy_ms": statistics.mean(frame_ms) - front_ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(),
@@ -440,61 +452,149 @@ def run_ours(args) -> None:
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
-        report = json.loads(DEFAULT_WEIGHTS.with_suffix(".json").read_text())
-        lq = psnr_y(nv12, learned_data)
-        line["learned"] = {
-            "fps": whole_job_rate(n, world, learned_ms), "unit": "frames/s", "frontend_ms": learned_front,
-            "decided_regions": decided, "regions": regions, "margin": DEFAULT_MARGIN,
-            "bpp": 8.0 * len(learned_data) / (W * H), "psnr_y_db": lq,
-            "bpp_delta_pct": 100.0 * (len(learned_data) / len(data) - 1.0),
-            "psnr_delta_db": lq - quality["psnr_y_db"],
-            "bpp_delta_at_equal_psnr_pct": {
-                f"{r['frame']} d={r['distance']}": round(r["bpp_delta_at_equal_psnr_pct"], 3)
-                for r in report["codec_split"]},
-            "basis": "same step with the shipped network attached (split decisions, margin 0.2); the "
-                     "equal-PSNR bpp changes are from the weights' training report (held-out frames)",
-        }
-        print(json.dumps(line), flush=True)
+
+    extras = rank == 0 and world == 1 and not args.no_extras
+    if extras:
+        line["distances"] = bench_distances(step, nv12, args)
+        line["learned"] = bench_learned(step, nv12, data, quality, args, local)
     # Torch's allocators record events on the streams their blocks were used
     # on when they are freed, so release every torch object that touched the
     # encoders' streams before the encoders destroy those streams.
     torch.cuda.synchronize()
-    del frames, pinned_l, pinned_c, outs, ev_a, ev_b, start, stop, e0, dones, joins, stream, streams
+    del frames, pinned_l, pinned_c, outs, e0, dones, streams, step
     import gc
 
     gc.collect()
     torch.cuda.synchronize()
     for e in encs:
         e.close()
+    if extras:
+        line["mixed64"] = bench_mixed64(args, local, value)
+        line["serving"] = bench_serving(args, local)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
+
+
+def bench_distances(step: Step, nv12, args) -> dict:
+    """The headline step at d = 0.5, 2 and 4 (d = 1 is the headline)."""
+    W, H = step.W, step.H
+    out = {}
+    pairs = []
+    for d in (0.5, 2.0, 4.0):
+        for e in step.encs:
+            e.configure(W, H, d)
+        steps = max(3, args.steps // 2)
+        ms = step.timed(steps, args.warmup)
+        front, frame_ms = step.stage_times(16)
+        data = step.encs[0].encode_device(step.frames[0][0].data_ptr(), step.frames[0][1].data_ptr(), W, W)
+        pairs.append((nv12, data))
+        out[str(d)] = {"fps": steps * BATCH / (ms / 1000.0), "steps": steps, "bpp": 8.0 * len(data) / (W * H),
+                       "frontend_ms": statistics.mean(front), "frame_ms": statistics.mean(frame_ms)}
+    for (k, v), p in zip(out.items(), psnr_many(pairs)):
+        v["psnr_y_db"] = p
+    for e in step.encs:
+        e.configure(W, H, args.distance)
+    return out
+
+
+def bench_learned(step: Step, nv12, plain_data: bytes, quality: dict, args, device: int) -> dict:
+    """The headline step with the shipped network attached, and the live
+    equal-PSNR bpp change on held-out frames."""
+    from cujpegxl_b200 import Encoder
+    from cujpegxl_b200.acsnet import DEFAULT_MARGIN, QF, SPLIT, AcsNet
+    from cujpegxl_b200.synth import make_nv12
+
+    W, H = step.W, step.H
+    net = AcsNet.load(device_ordinal=device)
+    res = {"margin": DEFAULT_MARGIN, "unit": "frames/s"}
+    pairs = []
+    try:
+        for name, flags in (("split", SPLIT), ("split_qf", SPLIT | QF)):
+            for e in step.encs:
+                e.set_acsnet(net, DEFAULT_MARGIN, flags)
+            ms = step.timed(args.steps, args.warmup)
+            front, _ = step.stage_times(16)
+            data = step.encs[0].encode_device(step.frames[0][0].data_ptr(), step.frames[0][1].data_ptr(), W, W)
+            decided, regions = step.encs[0].acsnet_stats()
+            res[name] = {"fps": args.steps * BATCH / (ms / 1000.0), "frontend_ms": statistics.mean(front),
+                         "decided_regions": decided, "regions": regions, "bpp": 8.0 * len(data) / (W * H),
+                         "bpp_delta_pct": 100.0 * (len(data) / len(plain_data) - 1.0)}
+            pairs.append((nv12, data))
+        for e in step.encs:
+            e.set_acsnet(None)
+        for (name, v), p in zip([(k, res[k]) for k in ("split", "split_qf")], psnr_many(pairs)):
+            v["psnr_y_db"] = p
+            v["psnr_delta_db"] = p - quality["psnr_y_db"]
+
+        # Equal-PSNR bpp change, measured now: per held-out frame and distance,
+        # the plain encode and the network's encodes at d x 0.8 .. 1.25.
+        scales = (0.8, 0.9, 1.0, 1.12, 1.25)
+        jobs = []   # (key, nv12, data, bpp, kind)
+        for (w, h, seed) in HELD_OUT:
+            nv = make_nv12(w, h, seed)
+            for d in (1.0, 2.0):
+                key = f"{w}x{h}#{seed} d={d}"
+                with Encoder(w, h, d, device) as enc:
+                    data = enc.encode_host(nv)
+                jobs.append((key, nv, data, 8.0 * len(data) / (w * h), "plain"))
+                for s in scales:
+                    with Encoder(w, h, d * s, device) as enc:
+                        enc.set_acsnet(net, DEFAULT_MARGIN, SPLIT | QF)
+                        data = enc.encode_host(nv)
+                        enc.set_acsnet(None)
+                    jobs.append((key, nv, data, 8.0 * len(data) / (w * h), s))
+        psnrs = psnr_many([(j[1], j[2]) for j in jobs])
+        table = {}
+        for (key, _, _, bpp, kind), p in zip(jobs, psnrs):
+            t = table.setdefault(key, {"curve": []})
+            if kind == "plain":
+                t["bpp_plain"], t["psnr_plain"] = bpp, p
+            else:
+                t["curve"].append((kind, bpp, p))
+        for key, t in table.items():
+            ps = np.array([c[2] for c in t["curve"]])
+            lb = np.log(np.array([c[1] for c in t["curve"]]))
+            order = np.argsort(ps)
+            pp = t["psnr_plain"]
+            at = float(np.exp(np.interp(pp, ps[order], lb[order]))) if ps.min() <= pp <= ps.max() else float("nan")
+            mid = [c for c in t["curve"] if c[0] == 1.0][0]
+            t.update(bpp_learned=mid[1], psnr_learned=mid[2],
+                     bpp_delta_at_equal_psnr_pct=100.0 * (at / t["bpp_plain"] - 1.0))
+            del t["curve"]
+        res["equal_psnr"] = table
+        res["equal_psnr_basis"] = ("measured in this run: split + quant-field decisions, margin 0.2, held-out "
+                                   "seeds; log-bpp interpolated at the plain encode's PSNR-Y over the network's "
+                                   "encodes at d x 0.8, 0.9, 1, 1.12, 1.25")
+    finally:
+        for e in step.encs:
+            e.set_acsnet(None)
+        net.close()
+    return res
 
 
 MIXED64 = ([(1280, 720)] * 16 + [(1920, 1080)] * 16 + [(2560, 1440)] * 16 + [(3840, 2160)] * 8
            + [(4096, 2160)] * 8)
 
 
-def run_batch(args) -> None:
-    """The 64-frame uneven-resolution batch (16 x 720p, 16 x 1080p, 16 x 1440p,
-    8 x 3840x2160, 8 x 4096x2160; frame i from seed i, d=1.0): one CUDA graph
-    launch per step through cujpegxl_b200_batch_encode."""
-    from concurrent.futures import ThreadPoolExecutor
-
+def mixed64_frames(device: int):
     import torch
 
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    from cujpegxl_b200 import Batch
     from cujpegxl_b200.synth import make_nv12
 
-    d = args.distance
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as pool:
         nvs = list(pool.map(lambda i: make_nv12(MIXED64[i][0], MIXED64[i][1], i), range(len(MIXED64))))
-    dev = [torch.from_numpy(nv).cuda() for nv in nvs]
+    dev = [torch.from_numpy(nv).cuda(device) for nv in nvs]
     torch.cuda.synchronize()
     inputs = [(t.data_ptr(), t.data_ptr() + w * h, w, w) for t, (w, h) in zip(dev, MIXED64)]
-    batch = Batch([(w, h, d) for w, h in MIXED64], local)
-    for _ in range(args.warmup):
+    return dev, inputs
+
+
+def time_batch(batch, inputs, steps: int, warmup: int) -> tuple[float, list[int]]:
+    import torch
+
+    for _ in range(warmup):
         batch.encode(inputs)
         batch.sync()
     stream = torch.cuda.ExternalStream(batch.stream())
@@ -502,53 +602,101 @@ def run_batch(args) -> None:
     stop = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     start.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         batch.encode(inputs)
     stop.record(stream)
     sizes = batch.sync()
     torch.cuda.synchronize()
-    dt = start.elapsed_time(stop) / 1000.0
-    n = args.steps * len(MIXED64)
-    mp = sum(w * h for w, h in MIXED64) * args.steps / 1e6
+    return start.elapsed_time(stop), sizes
 
-    # The same batch with learned transform decisions (the shipped network,
-    # split and quant field, margin 0.2): the graph is captured and tuned
-    # again, then timed the same way.
+
+def bench_mixed64(args, device: int, single_fps: float) -> dict:
+    """The 64-frame uneven-resolution batch (16 x 720p, 16 x 1080p, 16 x 1440p,
+    8 x 3840x2160, 8 x 4096x2160; frame i from seed i, d=1.0), one launch
+    per step, plain then learned (split and quant field, margin 0.2)."""
+    from cujpegxl_b200 import Batch
     from cujpegxl_b200.acsnet import DEFAULT_MARGIN, QF, SPLIT, AcsNet
 
-    net = AcsNet.load(device_ordinal=local)
-    batch.set_acsnet(net, DEFAULT_MARGIN, SPLIT | QF)
-    for _ in range(args.warmup):
-        batch.encode(inputs)
-        batch.sync()
-    torch.cuda.synchronize()
-    start.record(stream)
-    for _ in range(args.steps):
-        batch.encode(inputs)
-    stop.record(stream)
-    lsizes = batch.sync()
-    torch.cuda.synchronize()
-    ldt = start.elapsed_time(stop) / 1000.0
-    learned = {"value": n / ldt, "unit": "frames/s", "mp_per_s": mp / ldt, "bytes_per_step": sum(lsizes),
-               "lanes": batch.lanes, "decisions": "split and quant field, margin 0.2"}
-    batch.set_acsnet(None)
-    net.close()
+    dev, inputs = mixed64_frames(device)
+    steps = max(3, args.steps // 2)
+    mp = sum(w * h for w, h in MIXED64) / 1e6
+    res = {"frames": len(MIXED64), "steps": steps, "distance": 1.0,
+           "workload": "16x1280x720, 16x1920x1080, 16x2560x1440, 8x3840x2160, 8x4096x2160, frame i seed i",
+           "timing": "CUDA events on the batch's stream around K launches"}
+    with Batch([(w, h, 1.0) for w, h in MIXED64], device) as batch:
+        ms, sizes = time_batch(batch, inputs, steps, args.warmup)
+        res["plain"] = {"fps": steps * len(MIXED64) / (ms / 1000.0), "mp_per_s": steps * mp / (ms / 1000.0),
+                        "bytes_per_step": sum(sizes), "schedule": batch.schedule()}
+        net = AcsNet.load(device_ordinal=device)
+        batch.set_acsnet(net, DEFAULT_MARGIN, SPLIT | QF)
+        ms, sizes = time_batch(batch, inputs, steps, args.warmup)
+        res["learned"] = {"fps": steps * len(MIXED64) / (ms / 1000.0), "mp_per_s": steps * mp / (ms / 1000.0),
+                          "bytes_per_step": sum(sizes), "schedule": batch.schedule(),
+                          "decisions": "split and quant field, margin 0.2"}
+        batch.set_acsnet(None)
+        net.close()
+    res["single_frame_plain_4k_fps"] = single_fps
+    del dev
+    return res
+
+
+def bench_serving(args, device: int) -> dict:
+    """The 8-stream serving workload, plain and learned: 1x for 3 s, then
+    rising speeds for 1.5 s each until a run no longer keeps up."""
+    from cujpegxl_b200.acsnet import QF, SPLIT, AcsNet
+    from cujpegxl_b200.serve import DEFAULT_STREAMS, AdmissionError, Server
+
+    def one(net) -> dict:
+        srv = Server(device, 40e9, depth=2, net=net, net_flags=SPLIT | QF, frames=4)
+        try:
+            rejected = []
+            for i, spec in enumerate(DEFAULT_STREAMS):
+                try:
+                    srv.admit(spec, seed=i)
+                except AdmissionError as e:
+                    rejected.append(str(e))
+            srv.run(0.3, seed=99, speed=1.0)   # warm-up
+            base = srv.run(3.0, seed=0, speed=1.0)
+            best = None
+            for speed in (4.0, 6.0, 8.0, 10.0, 12.0):
+                r = srv.run(1.5, seed=int(speed), speed=speed)
+                if not r["kept_up"]:
+                    break
+                best = r
+            trim = lambda r: None if r is None else {k: r[k] for k in (
+                "speed", "duration_s", "offered_frames", "frames", "wall_s", "kept_up", "sustained_fps",
+                "sustained_mp_per_s", "p50_ms", "p99_ms", "latency_ms", "clock_offset_bound_ms")}
+            return {"at_1x": trim(base), "fastest_kept_up": trim(best), "rejected": rejected,
+                    "device_bytes_admitted": base["device_bytes_admitted"]}
+        finally:
+            srv.close()
+
+    res = {"workload": "2x3840x2160@30, 4x1920x1080@60, 2x1280x720@60 frames/s, Poisson arrivals, "
+                       "4 distinct seeded frames per stream, 2 slots per stream, 40 GB budget, d=1.0",
+           "latency_basis": "arrival (host clock) to the file in host memory (device event)"}
+    res["plain"] = one(None)
+    net = AcsNet.load(device_ordinal=device)
+    try:
+        res["learned"] = one(net)
+    finally:
+        net.close()
+    return res
+
+
+def run_batch(args) -> None:
+    """The 64-frame uneven-resolution batch as the headline line."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    r = bench_mixed64(args, local, float("nan"))
     if rank == 0:
         print(json.dumps({
-            "metric": "mixed-resolution batch frames/s", "value": n / dt, "unit": "frames/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 frames: 16x1280x720, 16x1920x1080, 16x2560x1440, 8x3840x2160, "
-                                   f"8x4096x2160, frame i seed i, d={d}",
-                       "step": "one CUDA graph launch of the whole batch", "lanes": batch.lanes},
-            "mp_per_s": mp / dt, "bytes_per_step": sum(sizes),
-            "timing": "CUDA events on the batch's stream around K graph launches (each ends with the "
-                      "device-to-host copy of every frame's size)",
-            "learned": learned,
+            "metric": "mixed-resolution batch frames/s", "value": r["plain"]["fps"], "unit": "frames/s",
+            "n_gpus": world, "steps": r["steps"], "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": r["workload"], "step": "one launch of the whole batch"}, "mixed64": r,
         }), flush=True)
-    torch.cuda.synchronize()
-    del start, stop, stream
-    batch.close()
 
 
 def main() -> None:
@@ -562,9 +710,11 @@ def main() -> None:
     ap.add_argument("--distance", type=float, default=1.0)
     ap.add_argument("--cpu-runs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="only the headline line: skip the distance, learned, batch and serving workloads")
     ap.add_argument("--streams", type=int, default=4, help="encoders (CUDA streams) per GPU")
     ap.add_argument("--workload", default="4k", choices=["4k", "mixed64"],
-                    help="mixed64: the 64-frame uneven-resolution batch in one graph launch per step")
+                    help="mixed64: the 64-frame uneven-resolution batch as the headline")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

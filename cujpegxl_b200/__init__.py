@@ -262,6 +262,10 @@ class Batch:
     def lanes(self) -> int:
         return int(self._L.cujpegxl_b200_batch_lanes(self._h))
 
+    def schedule(self) -> dict:
+        """The launch schedule the batch's autotuner chose."""
+        return {"lanes": self.lanes}
+
     def stream(self) -> int:
         s = ctypes.c_size_t(0)
         check("batch_stream", self._L.cujpegxl_b200_batch_stream(self._h, ctypes.byref(s)))

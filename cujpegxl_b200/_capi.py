@@ -43,6 +43,7 @@ EXPORTS = (
     "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params", "cujpegxl_b200_batch_set_acsnet",
     "cujpegxl_b200_encoder_create_ex", "cujpegxl_b200_max_output_size_ex",
     "cujpegxl_b200_debug_fail_allocation", "cujpegxl_b200_debug_live_allocations",
+    "cujpegxl_b200_encoder_enqueue_readback",
 )
 
 
@@ -108,6 +109,7 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_encoder_result.argtypes = [E, P(ctypes.c_size_t), P(ctypes.c_size_t)]
     L.cujpegxl_b200_encoder_stream.argtypes = [E, P(ctypes.c_size_t)]
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
+    L.cujpegxl_b200_encoder_enqueue_readback.argtypes = [E, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     L.cujpegxl_b200_debug_fail_allocation.argtypes = [ctypes.c_uint32]
     L.cujpegxl_b200_debug_fail_allocation.restype = None
     L.cujpegxl_b200_debug_live_allocations.restype = ctypes.c_uint64

@@ -408,8 +408,10 @@ bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp
     return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, st);
 }
 
+cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output);
+
 // Waits for the encode and copies the file into `output`.
-cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output) {
+cujpegxl_status finish_pageable(cujpegxl_encoder* e, cujpegxl_output* output) {
     if (cudaMemcpyAsync(e->result_pinned, e->ed.result, 4 * 8, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
         cudaStreamSynchronize(e->stream) != cudaSuccess) {
         return CUJPEGXL_INTERNAL_ERROR;
@@ -458,6 +460,75 @@ __global__ void nz_kernel(const std::int16_t* ac, const std::int8_t* acs, int bw
         }
         nzc[c * nb + blk] = static_cast<std::uint16_t>(cnt);
     }
+}
+
+// Copies a finished file from device memory into pinned host memory that the
+// device reaches through unified addressing, with the file's size taken from
+// the result words on the device, so that no host round trip sits between the
+// encode and the copy. words_out receives {file bytes, status}: status 0 =
+// copied, 1 = the file exceeds `capacity` (nothing copied), 2 = the encode
+// failed.
+__global__ void __launch_bounds__(256) readback_kernel(const unsigned long long* result, const std::uint8_t* src,
+                                                       std::uint8_t* dst, unsigned long long capacity,
+                                                       unsigned long long* words_out) {
+    const unsigned long long total{result[0]};
+    const unsigned long long status{result[2] != 0 ? 2ull : (total > capacity ? 1ull : 0ull)};
+    const unsigned long long tid{static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x};
+    const unsigned long long stride{static_cast<unsigned long long>(gridDim.x) * blockDim.x};
+    if (status == 0) {
+        if ((reinterpret_cast<std::uintptr_t>(dst) & 15u) == 0) {
+            const unsigned long long nvec{total / 16};
+            const uint4* s4{reinterpret_cast<const uint4*>(src)};
+            uint4* d4{reinterpret_cast<uint4*>(dst)};
+            for (unsigned long long i{tid}; i < nvec; i += stride) d4[i] = s4[i];
+            for (unsigned long long i{nvec * 16 + tid}; i < total; i += stride) dst[i] = src[i];
+        } else {
+            for (unsigned long long i{tid}; i < total; i += stride) dst[i] = src[i];
+        }
+    }
+    if (tid == 0) {
+        words_out[0] = total;
+        words_out[1] = status;
+    }
+}
+
+constexpr unsigned kReadbackBlocks = 64;
+
+// True when [p, p + bytes) starts in page-locked host memory that the current
+// device can address (cudaHostAlloc / cudaHostRegister / torch pin_memory).
+bool device_reachable_host(const void* p) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (attr.type != cudaMemoryTypeHost) return false;
+    void* dp{nullptr};
+    if (cudaHostGetDevicePointer(&dp, const_cast<void*>(p), 0) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return dp == p;
+}
+
+bool enqueue_readback(cujpegxl_encoder* e, std::uint8_t* dst, std::size_t capacity, unsigned long long* words,
+                      cudaStream_t st) {
+    readback_kernel<<<kReadbackBlocks, 256, 0, st>>>(e->ed.result, e->ed.out, dst, capacity, words);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+// Waits for the encode and copies the file into `output`. A page-locked
+// output buffer is written by readback_kernel right behind the encode, so the
+// call waits once; other buffers take the result words first, then the copy.
+cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output) {
+    if (!device_reachable_host(output->data)) return finish_pageable(e, output);
+    if (!enqueue_readback(e, output->data, output->capacity, e->result_pinned, e->stream) ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    if (e->result_pinned[1] == 2) return CUJPEGXL_INTERNAL_ERROR;
+    output->size = static_cast<std::size_t>(e->result_pinned[0]);
+    return e->result_pinned[1] == 1 ? CUJPEGXL_BUFFER_TOO_SMALL : CUJPEGXL_OK;
 }
 
 }  // namespace
@@ -787,6 +858,23 @@ cujpegxl_status cujpegxl_b200_encoder_result(cujpegxl_encoder* encoder, size_t* 
     *out_size = static_cast<std::size_t>(encoder->result_pinned[0]);
     if (out_device_bytes != nullptr) *out_device_bytes = reinterpret_cast<uintptr_t>(encoder->ed.out);
     return CUJPEGXL_OK;
+}
+
+cujpegxl_status cujpegxl_b200_encoder_enqueue_readback(cujpegxl_encoder* encoder, uint8_t* host_dst,
+                                                      size_t capacity, uint64_t* host_words) {
+    if (encoder == nullptr || host_dst == nullptr || host_words == nullptr || encoder->arena == nullptr) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    DeviceScope scope{encoder->device};
+    if (!scope.ok()) return CUJPEGXL_INTERNAL_ERROR;
+    if ((reinterpret_cast<std::uintptr_t>(host_words) & 7u) != 0 || !device_reachable_host(host_dst) ||
+        !device_reachable_host(host_words)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    return enqueue_readback(encoder, host_dst, capacity, reinterpret_cast<unsigned long long*>(host_words),
+                            encoder->stream)
+               ? CUJPEGXL_OK
+               : CUJPEGXL_INTERNAL_ERROR;
 }
 
 cujpegxl_status cujpegxl_b200_encoder_stream(cujpegxl_encoder* encoder, uintptr_t* out_stream) {

@@ -86,6 +86,20 @@ cujpegxl_status cujpegxl_b200_encoder_enqueue(cujpegxl_encoder* encoder,
 cujpegxl_status cujpegxl_b200_encoder_result(cujpegxl_encoder* encoder, size_t* out_size,
                                              uintptr_t* out_device_bytes);
 
+/* Enqueues, behind the encoder's last enqueued encode, the copy of its file
+ * into page-locked host memory (cudaHostAlloc, cudaHostRegister or torch's
+ * pin_memory; other memory gives CUJPEGXL_INVALID_ARGUMENT) and returns
+ * without waiting. The copy is made by a kernel that reads the file's size on
+ * the device, so no host round trip separates encode and copy. When the
+ * encoder's stream has reached it, host_words[0] holds the file's size and
+ * host_words[1] a status: 0 = copied into host_dst, 1 = larger than
+ * `capacity` (nothing copied), 2 = the encode failed. host_words is 8-byte
+ * aligned page-locked memory of two words. cujpegxl_encoder_encode takes the
+ * same path by itself when its output buffer is page-locked. Replaces no
+ * reference interface. */
+cujpegxl_status cujpegxl_b200_encoder_enqueue_readback(cujpegxl_encoder* encoder, uint8_t* host_dst,
+                                                      size_t capacity, uint64_t* host_words);
+
 /* As cujpegxl_b200_encoder_enqueue, restricted to the stages in `stages`
  * (bit 0: the fused frontend kernel, bit 1: entropy coding and assembly).
  * For timing one stage in isolation. Replaces no reference interface. */

@@ -1,5 +1,6 @@
 """Builds the CPU restatement (oracle/liboracle.so) and, when the reference
-checkout is present, the reference checker library (oracle/_ref/libjxlref.so).
+checkout is present, the reference checker libraries (oracle/_ref/libjxlref.so
+from its host code, oracle/_ref/libjxlref_gpu.so from its device code).
 
 Test infrastructure only. The restatement is compiled without floating-point
 contraction so that fmaf appears exactly where the source writes it.
@@ -31,8 +32,10 @@ def build(force: bool = False) -> None:
     build_oracle(force)
     sys.path.insert(0, str(HERE))
     import build_ref  # noqa: E402  (sibling module)
+    import build_ref_gpu  # noqa: E402
 
     build_ref.build(force)
+    build_ref_gpu.build(force)
 
 
 if __name__ == "__main__":

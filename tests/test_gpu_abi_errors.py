@@ -91,3 +91,40 @@ def test_failed_allocation_at_configure_keeps_encoder_usable():
         enc.configure(w, h, 1.0)
         with Encoder(w, h, 1.0) as ref:
             assert enc.encode_device(luma, chroma, lp, cp) == ref.encode_device(luma, chroma, lp, cp)
+
+
+def test_page_locked_output_takes_the_one_wait_path():
+    """cujpegxl_encoder_encode into page-locked memory (the device-side copy
+    behind the encode) gives the same file as into pageable memory, and the
+    same BUFFER_TOO_SMALL answer for a 16-byte page-locked buffer."""
+    import torch
+
+    w, h = 1280, 720
+    nv = make_nv12(w, h, 8)
+    keep, luma, chroma, lp, cp = device_nv12(nv, w, h)
+    L = _capi.lib()
+    inp = _capi.Nv12Input(luma, chroma, lp, cp)
+    with Encoder(w, h, 1.0) as enc:
+        pageable = enc.encode_device(luma, chroma, lp, cp)
+        for offset in (0, 3):   # 16-byte aligned and unaligned destinations
+            pinned = torch.zeros(len(pageable) + 64, dtype=torch.uint8).pin_memory()
+            out = _capi.Output(pinned.data_ptr() + offset, 0, len(pageable))
+            assert L.cujpegxl_encoder_encode(enc.handle, ctypes.byref(inp), ctypes.byref(out)) == _capi.OK
+            assert out.size == len(pageable)
+            got = pinned.numpy()
+            assert got[offset:offset + out.size].tobytes() == pageable
+            assert not got[:offset].any() and not got[offset + out.size:].any()
+        tiny = torch.zeros(16, dtype=torch.uint8).pin_memory()
+        out = _capi.Output(tiny.data_ptr(), 0, 16)
+        assert L.cujpegxl_encoder_encode(enc.handle, ctypes.byref(inp), ctypes.byref(out)) == _capi.BUFFER_TOO_SMALL
+        assert out.size == len(pageable) and not tiny.numpy().any()
+
+
+def test_enqueue_readback_rejects_pageable_memory():
+    w, h = 512, 384
+    L = _capi.lib()
+    with Encoder(w, h, 1.0) as enc:
+        buf = np.zeros(1 << 16, np.uint8)
+        words = np.zeros(2, np.uint64)
+        code = L.cujpegxl_b200_encoder_enqueue_readback(enc.handle, buf.ctypes.data, buf.size, words.ctypes.data)
+        assert code == _capi.INVALID_ARGUMENT
