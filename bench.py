@@ -455,6 +455,7 @@ def run_ours(args) -> None:
 
     extras = rank == 0 and world == 1 and not args.no_extras
     if extras:
+        line["reference_device"] = bench_reference_device(step, args)
         line["distances"] = bench_distances(step, nv12, args)
         line["learned"] = bench_learned(step, nv12, data, quality, args, local)
     # Torch's allocators record events on the streams their blocks were used
@@ -475,6 +476,66 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
+
+
+def bench_reference_device(step: Step, args) -> dict | None:
+    """The reference's own device stages on the same 4K frame, timed per call
+    (CUDA events on the legacy default stream around each entry point, which
+    launches its kernels there and synchronises the device before returning):
+    nv12_to_xyb (src/xyb.cu), the fused adaptive-quantisation kernel
+    (src/frontend_fused.cu encode_frontend) and XYB + inverse gaborish + the
+    variable DCT (src/frontend_transform.cu) on this encoder's transform
+    decisions. The reference's selection, CfL, quantiser and entropy coder are
+    not built (src/transform_select.cu, src/frontend_quantize.cu and
+    src/entropy.cu do not compile with nvcc)."""
+    import ctypes
+
+    import torch
+
+    lib_path = REPO / "oracle" / "_ref" / "libjxlref_gpu.so"
+    if not lib_path.exists():
+        return None
+    L = ctypes.CDLL(str(lib_path))
+    U = ctypes.c_size_t
+    L.refgpu_nv12_to_xyb.argtypes = [U, U, U, U, U, U, U]
+    L.refgpu_encode_frontend.argtypes = [U, U, U, U, U, U, ctypes.c_float, U]
+    L.refgpu_frontend_transform.argtypes = [U, U, U, U, U, U, ctypes.c_float, U, U, U]
+    W, H = step.W, step.H
+    nb = (W // 8) * (H // 8)
+    lm, ch = step.frames[0]
+    acs = torch.from_numpy(step.encs[0].read_planes(keys=("acs",))["acs"]).cuda()
+    xyb = torch.empty(3 * W * H, dtype=torch.float32, device="cuda")
+    qf = torch.empty(nb, dtype=torch.int32, device="cuda")
+    coef = torch.empty(3 * nb * 64, dtype=torch.float16, device="cuda")
+    acs_out = torch.empty(nb, dtype=torch.int8, device="cuda")
+    calls = {
+        "nv12_to_xyb": lambda: L.refgpu_nv12_to_xyb(lm.data_ptr(), W, ch.data_ptr(), W, W, H, xyb.data_ptr()),
+        "aq_field": lambda: L.refgpu_encode_frontend(lm.data_ptr(), W, ch.data_ptr(), W, W, H, args.distance,
+                                                     qf.data_ptr()),
+        "xyb_gaborish_dct": lambda: L.refgpu_frontend_transform(lm.data_ptr(), W, ch.data_ptr(), W, W, H,
+                                                                args.distance, coef.data_ptr(), acs_out.data_ptr(),
+                                                                acs.data_ptr()),
+    }
+    out = {}
+    stream = torch.cuda.default_stream()
+    for name, fn in calls.items():
+        times = []
+        for i in range(3 + 10):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            if fn() != 1:
+                raise RuntimeError(f"reference {name} failed")
+            b.record(stream)
+            torch.cuda.synchronize()
+            if i >= 3:
+                times.append(a.elapsed_time(b))
+        out[name + "_ms"] = statistics.median(times)
+    out["sum_ms"] = sum(out.values())
+    out["basis"] = ("the reference's device entry points built from its sources for sm_100a, median of 10 calls "
+                    "after 3; each call includes its own allocation, texture set-up and device synchronise")
+    return out
 
 
 def bench_distances(step: Step, nv12, args) -> dict:
