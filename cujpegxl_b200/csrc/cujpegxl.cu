@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -249,6 +250,10 @@ bool allocate(cujpegxl_encoder* e) {
     const std::size_t o_to{a.take(static_cast<std::size_t>(tiles + 1) * 8)};
     const std::size_t o_sp{a.take(plan.sections.size() * 8)};
     const std::size_t o_res{a.take(4 * 8)};
+    const std::uint32_t tok_cap{static_cast<std::uint32_t>(std::min<std::size_t>(nb * jxb::kTokensPerBlock, 0xfffffff0u))};
+    const std::size_t o_tok{a.take(static_cast<std::size_t>(tok_cap) * 4)};
+    const std::size_t o_tokn{a.take(4)};
+    const std::size_t o_stok{a.take(plan.stripes.size() * 8)};
     const std::size_t o_out{a.take(out_cap)};
     const std::size_t o_nv12{a.take(static_cast<std::size_t>(W) * H * 3 / 2)};
     const std::size_t o_ncls{a.take(((bw + 3) / 4) * ((bh + 3) / 4))};
@@ -337,6 +342,10 @@ bool allocate(cujpegxl_encoder* e) {
     ed.tile_off = reinterpret_cast<unsigned long long*>(b + o_to);
     ed.sec_pos = reinterpret_cast<unsigned long long*>(b + o_sp);
     ed.result = reinterpret_cast<unsigned long long*>(b + o_res);
+    ed.tok_pool = reinterpret_cast<std::uint32_t*>(b + o_tok);
+    ed.tok_capacity = tok_cap;
+    ed.tok_count = reinterpret_cast<std::uint32_t*>(b + o_tokn);
+    ed.stripe_tok = reinterpret_cast<std::uint32_t*>(b + o_stok);
     ed.out = b + o_out;
     ed.out_capacity = out_cap;
     e->nv12_dev = b + o_nv12;

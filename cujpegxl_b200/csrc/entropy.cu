@@ -355,12 +355,92 @@ __device__ __forceinline__ std::uint32_t warp_incl_scan(std::uint32_t v, int lan
     return v;
 }
 
+// An AC token in 32 bits: symbol (6 bits), cluster (5), extra-bit count (4)
+// and extra bits (at most 13: packed coefficients stay below 2^16).
+__device__ __forceinline__ std::uint32_t pack_ac_token(int cl, std::uint32_t sym, std::uint32_t nb,
+                                                       std::uint32_t bits) {
+    return (bits << 15) | (nb << 11) | (static_cast<std::uint32_t>(cl) << 6) | sym;
+}
+__device__ __forceinline__ std::uint32_t token_table_index(std::uint32_t t) {
+    return ((t >> 6) & 31u) * 256u + (t & 63u);
+}
+__device__ __forceinline__ std::uint32_t token_extra_count(std::uint32_t t) { return (t >> 11) & 15u; }
+__device__ __forceinline__ std::uint32_t token_extra_bits(std::uint32_t t) { return t >> 15; }
+
+// Number of coefficient tokens of an item: the scan positions from `covered`
+// through its last non-zero coefficient, exactly those on which
+// coeff_tokens reports `has` (all positions to the end of the transform when
+// the staged coefficients hold fewer non-zeros than the item's count).
+__device__ std::uint32_t coeff_extent(const StripeStage& s, const StripeItem& it, int lane) {
+    const int n{it.n};
+    const int side{n >> 3};
+    const int lside{side == 1 ? 0 : (side == 2 ? 1 : 2)};
+    const std::uint32_t covered{static_cast<std::uint32_t>(side * side)};
+    const std::uint32_t size{static_cast<std::uint32_t>(n * n)};
+    const std::uint16_t* ord{s.order + (n == 8 ? 0 : (n == 16 ? 64 : 320))};
+    const std::int16_t* plane{&s.coef[it.c][it.by][it.bx * kCoeffsPerBlock]};
+    std::uint32_t remaining{it.nz};
+    if (remaining == 0) return 0;
+    const unsigned upto{(2u << lane) - 1u};  // lanes 0..lane
+    for (std::uint32_t k0{covered}; k0 < size; k0 += 32) {
+        const std::uint32_t k{k0 + static_cast<std::uint32_t>(lane)};
+        std::int32_t val{0};
+        if (k < size) {
+            const int raw{ord[k]};
+            const int q{raw >> 6};
+            const int qy{q >> lside};
+            const int qx{q & (side - 1)};
+            if (it.by + qy < kStripeRows && it.bx + qx < kAcGroupBlocks) {
+                val = plane[qy * kRowSlots + qx * kCoeffsPerBlock + (raw & 63)];
+            }
+        }
+        const unsigned m{__ballot_sync(kFull, val != 0)};
+        const std::uint32_t pc{static_cast<std::uint32_t>(__popc(m))};
+        if (pc >= remaining) {
+            // The lane holding the remaining-th non-zero of this chunk.
+            const bool last{val != 0 && static_cast<std::uint32_t>(__popc(m & upto)) == remaining};
+            const unsigned who{__ballot_sync(kFull, last)};
+            return k0 + static_cast<std::uint32_t>(__ffs(who) - 1) - covered + 1;
+        }
+        remaining -= pc;
+    }
+    return size - covered;
+}
+
+// Exclusive scan over a CTA of kAcThreads threads; `warp_sums` holds
+// kAcWarps + 1 words and receives the total in its last entry.
+__device__ std::uint32_t cta_exclusive_scan(std::uint32_t v, std::uint32_t* warp_sums, std::uint32_t& total) {
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const int warp{static_cast<int>(threadIdx.x) >> 5};
+    const std::uint32_t incl{warp_incl_scan(v, lane)};
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const std::uint32_t ws{lane < kAcWarps ? warp_sums[lane] : 0u};
+        const std::uint32_t wi{warp_incl_scan(ws, lane)};
+        if (lane < kAcWarps) warp_sums[lane] = wi - ws;
+        if (lane == kAcWarps - 1) warp_sums[kAcWarps] = wi;
+    }
+    __syncthreads();
+    const std::uint32_t off{warp_sums[warp] + incl - v};
+    total = warp_sums[kAcWarps];
+    __syncthreads();
+    return off;
+}
+
 // ---- pass 1: histograms ---------------------------------------------------------
 
-__global__ void __launch_bounds__(kAcThreads) ac_hist_kernel(EntropyDev e) {
+// One CTA per stripe: the stripe's coefficient planes are read once, its
+// tokens counted into the 32-cluster histogram and written, in stream order,
+// to a run of the token pool that the stripe reserves once it knows their
+// number (count tokens first sized, then the coefficient extents).
+__global__ void __launch_bounds__(kAcThreads) ac_tok_kernel(EntropyDev e) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
     std::uint32_t* hist{reinterpret_cast<std::uint32_t*>(ac_smem + sizeof(StripeStage))};  // [32][64]
+    __shared__ std::uint32_t sh_scan[kAcWarps + 1];
+    __shared__ std::uint32_t sh_base;
+    __shared__ int sh_stored;
     const int tid{static_cast<int>(threadIdx.x)};
     const int lane{tid & 31};
     const Stripe st{e.stripes[blockIdx.x]};
@@ -371,20 +451,67 @@ __global__ void __launch_bounds__(kAcThreads) ac_hist_kernel(EntropyDev e) {
     const int nitems{3 * st.rows * gg.gw};
     for (int j{tid}; j < nitems; j += kAcThreads) {
         const StripeItem it{stripe_item(s, gg.gw, j)};
-        if (it.n == 0) continue;
+        if (it.n == 0) {
+            s.aux[j] = 0;
+            continue;
+        }
         int cl;
         std::uint32_t tok, nb, bits;
         count_token(s, st, it, cl, tok, nb, bits);
         atomicAdd(&hist[cl * kAcSymbols + tok], 1u);
+        s.aux[j] = 1;
         if (it.nz != 0) s.active[atomicAdd(&s.nactive, 1)] = static_cast<std::uint16_t>(j);
     }
     __syncthreads();
     for (int a{tid >> 5}; a < s.nactive; a += kAcWarps) {
-        const StripeItem it{stripe_item(s, gg.gw, s.active[a])};
-        coeff_tokens(s, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t, std::uint32_t) {
+        const int j{s.active[a]};
+        const std::uint32_t ext{coeff_extent(s, stripe_item(s, gg.gw, j), lane)};
+        if (lane == 0) s.aux[j] += ext;
+    }
+    __syncthreads();
+    // Token offsets of the items: each thread scans two adjacent items.
+    const int j0{2 * tid};
+    const std::uint32_t c0{j0 < nitems ? s.aux[j0] : 0u};
+    const std::uint32_t c1{j0 + 1 < nitems ? s.aux[j0 + 1] : 0u};
+    std::uint32_t total{0};
+    const std::uint32_t off{cta_exclusive_scan(c0 + c1, sh_scan, total)};
+    if (j0 < nitems) s.aux[j0] = off;
+    if (j0 + 1 < nitems) s.aux[j0 + 1] = off + c0;
+    if (tid == 0) {
+        std::uint32_t base{0};
+        bool stored{true};
+        if (total != 0) {
+            base = atomicAdd(e.tok_count, total);
+            stored = base <= e.tok_capacity && total <= e.tok_capacity - base;
+        }
+        sh_base = base;
+        sh_stored = stored ? 1 : 0;
+        e.stripe_tok[2 * blockIdx.x] = stored ? base : kNoTokens;
+        e.stripe_tok[2 * blockIdx.x + 1] = total;
+    }
+    __syncthreads();
+    const bool stored{sh_stored != 0};
+    std::uint32_t* pool{e.tok_pool + sh_base};
+    if (stored) {
+        for (int j{tid}; j < nitems; j += kAcThreads) {
+            const StripeItem it{stripe_item(s, gg.gw, j)};
+            if (it.n == 0) continue;
+            int cl;
+            std::uint32_t tok, nb, bits;
+            count_token(s, st, it, cl, tok, nb, bits);
+            pool[s.aux[j]] = pack_ac_token(cl, tok, nb, bits);
+        }
+    }
+    for (int a{tid >> 5}; a < s.nactive; a += kAcWarps) {
+        const int j{s.active[a]};
+        const StripeItem it{stripe_item(s, gg.gw, j)};
+        std::uint32_t* dst{pool + s.aux[j] + 1 + static_cast<std::uint32_t>(lane)};
+        coeff_tokens(s, it, lane, [&](bool has, int cl, std::uint32_t sym, std::uint32_t nb, std::uint32_t bits) {
             const unsigned key{has ? static_cast<unsigned>(cl * kAcSymbols + sym) : 0xffffffffu};
             const unsigned peers{__match_any_sync(kFull, key)};
             if (has && (__ffs(peers) - 1) == lane) atomicAdd(&hist[key], static_cast<unsigned>(__popc(peers)));
+            if (has && stored) *dst = pack_ac_token(cl, sym, nb, bits);
+            dst += 32;
         });
     }
     __syncthreads();
@@ -608,10 +735,31 @@ __global__ void __launch_bounds__(32) codes_kernel(EntropyDev e) {
 __global__ void __launch_bounds__(kAcThreads) ac_bits_kernel(EntropyDev e) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
+    __shared__ std::uint32_t sh_sum[kAcWarps];
     const int tid{static_cast<int>(threadIdx.x)};
     const int lane{tid & 31};
     const Stripe st{e.stripes[blockIdx.x]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
+    const std::uint32_t tbase{e.stripe_tok[2 * blockIdx.x]};
+    if (tbase != kNoTokens) {
+        // Stored tokens: the stripe's whole length goes on its first item
+        // (the scan only needs sums at stripe and section starts).
+        const std::uint32_t ntok{e.stripe_tok[2 * blockIdx.x + 1]};
+        const std::uint32_t* pool{e.tok_pool + tbase};
+        std::uint32_t sum{0};
+        for (std::uint32_t t{static_cast<std::uint32_t>(tid)}; t < ntok; t += kAcThreads) {
+            const std::uint32_t tk{pool[t]};
+            sum += __ldg(&e.ac_depth[token_table_index(tk)]) + token_extra_count(tk);
+        }
+        sum = warp_sum(sum);
+        if (lane == 0) sh_sum[tid >> 5] = sum;
+        __syncthreads();
+        const int nitems{3 * st.rows * gg.gw};
+        std::uint32_t total{0};
+        for (int w{0}; w < kAcWarps; ++w) total += sh_sum[w];
+        for (int j{tid}; j < nitems; j += kAcThreads) e.item_bits[st.item0 + j] = j == 0 ? total : 0u;
+        return;
+    }
     stage_stripe(e, st, gg, s);
     __syncthreads();
     const int nitems{3 * st.rows * gg.gw};
@@ -1034,7 +1182,11 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     const Stripe st{e.stripes[blockIdx.x]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
     const int nitems{3 * st.rows * gg.gw};
-    stage_stripe(e, st, gg, s);
+    if (e.stripe_tok[2 * blockIdx.x] == kNoTokens) {
+        stage_stripe(e, st, gg, s);
+    } else if (tid == 0) {
+        s.nactive = 0;
+    }
     if (tid == 0) {
         const Section sec{e.sections[st.section]};
         const unsigned long long p0{prefix_at(e, st.item0)};
@@ -1048,12 +1200,51 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     __syncthreads();
     const int nwords{sh_words};
     for (int i{tid}; i < nwords; i += kAcThreads) win[i] = 0;
+    unsigned int* words{nwords >= 0 ? win : reinterpret_cast<unsigned int*>(e.out)};
+    const unsigned long long base{nwords >= 0 ? (sh_start & 31) : sh_start};
+    const std::uint32_t tbase{e.stripe_tok[2 * blockIdx.x]};
+    if (tbase != kNoTokens) {
+        // Stored tokens in stream order: their lengths, a CTA scan for their
+        // offsets, and their bits, kAcThreads * kPer tokens per round.
+        __shared__ std::uint32_t sh_scan[kAcWarps + 1];
+        constexpr int kPer{4};
+        const std::uint32_t ntok{e.stripe_tok[2 * blockIdx.x + 1]};
+        const std::uint32_t* pool{e.tok_pool + tbase};
+        __syncthreads();
+        unsigned long long run{base};
+        for (std::uint32_t t0{0}; t0 < ntok; t0 += kAcThreads * kPer) {
+            std::uint32_t tk[kPer];
+            std::uint32_t len[kPer];
+            std::uint32_t local{0};
+#pragma unroll
+            for (int i{0}; i < kPer; ++i) {
+                const std::uint32_t t{t0 + static_cast<std::uint32_t>(tid) * kPer + i};
+                tk[i] = t < ntok ? pool[t] : 0u;
+                len[i] = t < ntok ? __ldg(&e.ac_depth[token_table_index(tk[i])]) + token_extra_count(tk[i]) : 0u;
+                local += len[i];
+            }
+            std::uint32_t total{0};
+            unsigned long long at{run + cta_exclusive_scan(local, sh_scan, total)};
+#pragma unroll
+            for (int i{0}; i < kPer; ++i) {
+                if (len[i] == 0) continue;
+                const std::uint32_t idx{token_table_index(tk[i])};
+                const std::uint32_t d{__ldg(&e.ac_depth[idx])};
+                put_bits_at(words, at, d, __ldg(&e.ac_bits[idx]));
+                const std::uint32_t nb{token_extra_count(tk[i])};
+                if (nb) put_bits_at(words, at + d, nb, token_extra_bits(tk[i]));
+                at += len[i];
+            }
+            run += total;
+        }
+        __syncthreads();
+        if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
+        return;
+    }
     for (int j{tid}; j < nitems; j += kAcThreads) {
         s.aux[j] = static_cast<std::uint32_t>(prefix_at(e, st.item0 + static_cast<std::uint32_t>(j)) - sh_p0);
     }
     __syncthreads();
-    unsigned int* words{nwords >= 0 ? win : reinterpret_cast<unsigned int*>(e.out)};
-    const unsigned long long base{nwords >= 0 ? (sh_start & 31) : sh_start};
     for (int j{tid}; j < nitems; j += kAcThreads) {
         const StripeItem it{stripe_item(s, gg.gw, j)};
         if (it.n == 0) continue;
@@ -1222,13 +1413,14 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     if (cudaMemsetAsync(e.ac_hist, 0, kNumClusters * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
         cudaMemsetAsync(e.dc_hist, 0, static_cast<std::size_t>(e.ndc) * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
         cudaMemsetAsync(e.am_hist, 0, static_cast<std::size_t>(e.ndc) * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
-        cudaMemsetAsync(e.fb_count, 0, static_cast<std::size_t>(e.ndc) * sizeof(std::uint32_t), st) != cudaSuccess) {
+        cudaMemsetAsync(e.fb_count, 0, static_cast<std::size_t>(e.ndc) * sizeof(std::uint32_t), st) != cudaSuccess ||
+        cudaMemsetAsync(e.tok_count, 0, sizeof(std::uint32_t), st) != cudaSuccess) {
         return false;
     }
     const unsigned misc{(e.ac_first + 255) / 256};
     const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
-    ac_hist_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(e);
+    ac_tok_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(e);
     misc_hist_kernel<<<misc, 256, 0, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
     ac_bits_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
@@ -1247,7 +1439,7 @@ bool entropy_kernels_init() {
                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(ac_tok_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kHistSmem)) == cudaSuccess &&
            cudaFuncSetAttribute(ac_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&

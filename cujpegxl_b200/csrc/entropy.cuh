@@ -97,12 +97,25 @@ struct EntropyDev {
     unsigned long long* tile_off;    // [num_tiles + 1]
     unsigned long long* sec_pos;     // [nsec] absolute bit offset of each section in `out`
     unsigned long long* result;      // [4]: total bytes, body start, status, 0
+
+    // AC tokens, written once by the histogram pass and read by the bit-length
+    // and emission passes: each stripe reserves a contiguous run of the pool
+    // (stream order); a stripe that finds the pool full keeps its tokens
+    // unstored and the later passes tokenise its coefficients again.
+    std::uint32_t* tok_pool;         // [tok_capacity] packed tokens (pack_ac_token)
+    std::uint32_t tok_capacity;
+    std::uint32_t* tok_count;        // [1] pool fill, zeroed per frame
+    std::uint32_t* stripe_tok;       // [2 * nstripes]: pool offset or kNoTokens, token count
     std::uint8_t* out;               // output buffer (container + codestream)
     std::size_t out_capacity;
 };
 
 constexpr int kDescBytes = 256;
 constexpr int kScanTile = 4096;
+// Token pool capacity per 8x8 block: 4K frames at distance 0.5 use about 27,
+// at distance 1 about 11.
+constexpr std::uint32_t kTokensPerBlock = 32;
+constexpr std::uint32_t kNoTokens = 0xffffffffu;
 
 // Shared memory of the layout kernel: one 32-bit size per section, then the
 // codestream header, which is at most 64 bytes before the TOC plus 4 bytes

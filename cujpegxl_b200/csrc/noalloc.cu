@@ -155,7 +155,14 @@ cujpegxl_status cujpegxl_b200_encode_planes_noalloc(const cujpegxl_b200_device_p
     e.tile_off = c.take<unsigned long long>(tiles + 1);
     e.sec_pos = c.take<unsigned long long>(plan.sections.size());
     e.result = c.take<unsigned long long>(4);
+    e.tok_count = c.take<std::uint32_t>(1);
+    e.stripe_tok = c.take<std::uint32_t>(2 * plan.stripes.size());
     if (!c.ok) return CUJPEGXL_UNSUPPORTED_RESOLUTION;
+    // The rest of the array holds AC tokens; stripes that find it full are
+    // tokenised again from their coefficients.
+    const std::size_t tok_at{(c.used + 255) & ~static_cast<std::size_t>(255)};
+    e.tok_capacity = tok_at < kScratchBytes ? static_cast<std::uint32_t>((kScratchBytes - tok_at) / 4) : 0u;
+    e.tok_pool = reinterpret_cast<std::uint32_t*>(base + (tok_at < kScratchBytes ? tok_at : 0));
 
     e.sections = sections;
     e.stripes = stripes;
