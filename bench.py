@@ -38,7 +38,8 @@ Extras (N = 1, rank 0; --no-extras skips them), each timed in this run:
   serving: the 8-stream serving workload (2 x 4K@30, 4 x 1080p@60,
     2 x 720p@60, Poisson arrivals, 40 GB budget) at 1x for 3 s (>= 1000
     frames) and at rising speeds until it no longer keeps up, plain and
-    learned; p50/p99 latency and sustained frames/s.
+    learned; p50/p99 latency and sustained frames/s, and the fastest speed
+    whose p99 stays within 8 ms.
 --impl reference: the CPU encoder restated from the reference (the reference
 has no CPU implementation of its device stages) run with every host core on
 the same frame, rank 0 only.
@@ -66,6 +67,7 @@ BATCH = 16
 LATENCY_FRAMES = 128
 PUBLISHED_FPS = 15.0  # reference README.md:17, GTX 1080 Ti, 4K sustained
 HELD_OUT = [(3840, 2160, 0), (1920, 1080, 424242)]  # frames outside the network's training and validation seeds
+P99_TARGET_MS = 8.0  # serving-loop latency target per 4K frame
 
 
 def frontend_algorithmic_bytes(w: int, h: int) -> int:
@@ -703,7 +705,9 @@ def bench_mixed64(args, device: int, single_fps: float) -> dict:
 
 def bench_serving(args, device: int) -> dict:
     """The 8-stream serving workload, plain and learned: 1x for 3 s, then
-    rising speeds for 1.5 s each until a run no longer keeps up."""
+    rising speeds (2x .. 12x) for 1.5 s each until a run no longer keeps up
+    (every offered frame done within 0.1 s of the last arrival); reports the
+    fastest run that kept up and the fastest whose p99 stayed within 8 ms."""
     from cujpegxl_b200.acsnet import QF, SPLIT, AcsNet
     from cujpegxl_b200.serve import DEFAULT_STREAMS, AdmissionError, Server
 
@@ -718,17 +722,22 @@ def bench_serving(args, device: int) -> dict:
                     rejected.append(str(e))
             srv.run(0.3, seed=99, speed=1.0)   # warm-up
             base = srv.run(3.0, seed=0, speed=1.0)
-            best = None
-            for speed in (4.0, 6.0, 8.0, 10.0, 12.0):
-                r = srv.run(1.5, seed=int(speed), speed=speed)
-                if not r["kept_up"]:
-                    break
-                best = r
             trim = lambda r: None if r is None else {k: r[k] for k in (
                 "speed", "duration_s", "offered_frames", "frames", "wall_s", "kept_up", "sustained_fps",
                 "sustained_mp_per_s", "p50_ms", "p99_ms", "latency_ms", "clock_offset_bound_ms")}
-            return {"at_1x": trim(base), "fastest_kept_up": trim(best), "rejected": rejected,
-                    "device_bytes_admitted": base["device_bytes_admitted"]}
+            sweep = []
+            for speed in (2.0, 4.0, 6.0, 8.0, 10.0, 12.0):
+                r = srv.run(1.5, seed=int(speed), speed=speed)
+                sweep.append(r)
+                if not r["kept_up"]:
+                    break
+            kept = [r for r in sweep if r["kept_up"]]
+            within = [r for r in kept if r["p99_ms"] is not None and r["p99_ms"] <= P99_TARGET_MS]
+            return {"at_1x": trim(base), "fastest_kept_up": trim(kept[-1] if kept else None),
+                    "fastest_p99_within_8ms": trim(within[-1] if within else None),
+                    "sweep": [{k: r[k] for k in ("speed", "frames", "kept_up", "sustained_fps", "p50_ms", "p99_ms")}
+                              for r in sweep],
+                    "rejected": rejected, "device_bytes_admitted": base["device_bytes_admitted"]}
         finally:
             srv.close()
 

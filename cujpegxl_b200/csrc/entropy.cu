@@ -581,20 +581,27 @@ __global__ void __launch_bounds__(256) misc_hist_kernel(EntropyDev e) {
 
 struct WarpCodeSmem {
     std::uint32_t hist[256];
-    HuffNode pool[2 * 256 + 4];
-    std::uint8_t level[2 * 256 + 4];
+    std::uint32_t cnt[2 * 256];        // leaf counts in rank order, then internal nodes
+    std::int16_t parent[2 * 256];      // parent node of every leaf and internal node
+    std::uint16_t leaf_sym[256];       // symbol of the leaf of each rank
     std::uint8_t depth[256];
     std::uint16_t bits[256];
-    std::uint16_t used[256];   // compacted list of used symbols
-    std::uint8_t desc[kDescBytes];
+    std::uint16_t used[256];           // compacted list of used symbols
+    std::uint32_t len_count[18];       // depths per code length (canonical codes, header)
+    std::uint32_t len_next[18];
+    alignas(4) std::uint8_t desc[kDescBytes];
     CodeLengthScratch cl;
 };
 
-// Depths for a histogram with at least two used symbols, warp-cooperative:
-// the used symbols are compacted, each lane ranks its share by (clamped count
-// ascending, symbol descending) -- the order the reference's stable sort gives
-// leaves pushed in descending symbol order -- and lane 0 merges and assigns
-// levels (src/bitstream/prefix_code.cc:65-125).
+// Depths for a histogram with at least two used symbols, warp-cooperative and
+// equal to the reference's serial construction
+// (src/bitstream/prefix_code.cc:65-125): the used symbols are compacted and
+// each lane ranks its share by (clamped count ascending, symbol descending),
+// the order the reference's stable sort gives leaves pushed in descending
+// symbol order; lane 0 runs the two-queue merge (a leaf wins ties) recording
+// only each node's parent; then every lane walks its leaves to the root. The
+// whole construction repeats with the count floor doubled until no depth
+// exceeds `limit`.
 __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lane) {
     int n{0};
     for (int base{0}; base < length; base += 32) {
@@ -617,30 +624,202 @@ __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lan
                 const std::uint32_t ct{ht > floor - 1 ? ht : floor - 1};
                 rank += (ct < c || (ct == c && ts > sym)) ? 1 : 0;
             }
-            s.pool[rank].count = c;
-            s.pool[rank].left = -1;
-            s.pool[rank].right_or_value = static_cast<std::int16_t>(sym);
+            s.cnt[rank] = c;
+            s.leaf_sym[rank] = static_cast<std::uint16_t>(sym);
         }
         __syncwarp();
-        int mx{0};
         if (lane == 0) {
-            merge_pool(s.pool, n);
-            depths_from_pool(s.pool, n, s.level, s.depth);
-            for (int i{0}; i < n; ++i) mx = max(mx, static_cast<int>(s.depth[s.used[i]]));
+            // Leaves are cnt[0..n), internal node t is cnt[n + t]; the heads of
+            // both queues stay in registers.
+            constexpr std::uint32_t kInf{0xffffffffu};
+            int i{0};
+            int j{0};
+            std::uint32_t li{s.cnt[0]};
+            std::uint32_t lj{kInf};
+            for (int t{0}; t < n - 1; ++t) {
+                int pick[2];
+                std::uint32_t sum{0};
+#pragma unroll
+                for (int k{0}; k < 2; ++k) {
+                    if (li <= lj) {
+                        pick[k] = i;
+                        sum += li;
+                        ++i;
+                        li = i < n ? s.cnt[i] : kInf;
+                    } else {
+                        pick[k] = n + j;
+                        sum += lj;
+                        ++j;
+                        lj = j < t ? s.cnt[n + j] : kInf;
+                    }
+                }
+                s.cnt[n + t] = sum;
+                s.parent[pick[0]] = static_cast<std::int16_t>(n + t);
+                s.parent[pick[1]] = static_cast<std::int16_t>(n + t);
+                if (j == t) lj = sum;  // the internal queue was empty: its head is the new node
+            }
         }
-        mx = __shfl_sync(kFull, mx, 0);
+        __syncwarp();
+        const int root{2 * n - 2};
+        int mx{0};
+        for (int r{lane}; r < n; r += 32) {
+            int d{0};
+            for (int v{r}; v != root; v = s.parent[v]) ++d;
+            s.depth[s.leaf_sym[r]] = static_cast<std::uint8_t>(d);
+            mx = max(mx, d);
+        }
+#pragma unroll
+        for (int off{16}; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, off));
         __syncwarp();
         if (mx <= limit) return;
     }
 }
 
+// Canonical codes of depth[0..len) (canonical_codes in prefix_code.cuh),
+// warp-cooperative: codes of equal length are handed out in symbol order.
+__device__ void warp_canonical_codes(WarpCodeSmem& s, int len, int lane) {
+    if (lane < 18) s.len_count[lane] = 0;
+    __syncwarp();
+    for (int base{0}; base < len; base += 32) {
+        const int sym{base + lane};
+        const int d{sym < len ? s.depth[sym] : 0};
+        const unsigned peers{__match_any_sync(kFull, d)};
+        if (d != 0 && (__ffs(peers) - 1) == lane) s.len_count[d] += static_cast<std::uint32_t>(__popc(peers));
+    }
+    __syncwarp();
+    if (lane == 0) {
+        std::uint32_t code{0};
+        s.len_next[0] = 0;
+        for (int i{1}; i < 16; ++i) {
+            code = (code + (i - 1 == 0 ? 0u : s.len_count[i - 1])) << 1;
+            s.len_next[i] = code;
+        }
+    }
+    __syncwarp();
+    const unsigned below{(1u << lane) - 1u};
+    for (int base{0}; base < len; base += 32) {
+        const int sym{base + lane};
+        const int d{sym < len ? s.depth[sym] : 0};
+        const unsigned peers{__match_any_sync(kFull, d)};
+        const std::uint32_t code{d != 0 ? s.len_next[d] + static_cast<std::uint32_t>(__popc(peers & below)) : 0u};
+        __syncwarp();
+        if (d != 0 && (__ffs(peers) - 1) == lane) s.len_next[d] += static_cast<std::uint32_t>(__popc(peers));
+        if (sym < len) s.bits[sym] = d != 0 ? static_cast<std::uint16_t>(__brev(code) >> (32 - d)) : 0;
+        __syncwarp();
+    }
+}
+
+// ORs `n` (<= 32) bits of `v` at bit `pos` of a zeroed little-endian byte
+// buffer held as 32-bit words; bits at or past `cap` are dropped.
+__device__ __forceinline__ void or_bits(std::uint8_t* buf, std::uint32_t pos, std::uint32_t n, std::uint32_t v,
+                                        std::uint32_t cap) {
+    if (n == 0) return;
+    if (n < 32) v &= (1u << n) - 1u;
+    unsigned int* words{reinterpret_cast<unsigned int*>(buf)};
+    const std::uint32_t off{pos & 31u};
+    if (pos < cap) atomicOr(&words[pos >> 5], v << off);
+    if (off + n > 32 && pos + (32 - off) < cap) atomicOr(&words[(pos >> 5) + 1], v >> (32 - off));
+}
+
+// store_complex (prefix_code.cuh) with the per-symbol depth codes written by
+// the whole warp: lane 0 builds the code-length code and writes its part of
+// the header, then every lane places its symbols' codes at offsets from a
+// warp scan.
+__device__ void warp_store_complex(WarpCodeSmem& s, int num, BitSink& w, int lane) {
+    int new_len{0};
+    for (int i{lane}; i < num; i += 32) {
+        if (s.depth[i] != 0) new_len = i + 1;
+    }
+#pragma unroll
+    for (int off{16}; off > 0; off >>= 1) new_len = max(new_len, __shfl_xor_sync(kFull, new_len, off));
+    CodeLengthScratch& scr{s.cl};
+    if (lane < 18) scr.hist[lane] = 0;
+    __syncwarp();
+    for (int base{0}; base < new_len; base += 32) {
+        const int i{base + lane};
+        const int d{i < new_len ? s.depth[i] : -1};
+        const unsigned peers{__match_any_sync(kFull, d)};
+        if (d >= 0 && (__ffs(peers) - 1) == lane) scr.hist[d] += static_cast<std::uint32_t>(__popc(peers));
+    }
+    __syncwarp();
+    std::uint32_t pos{0};
+    if (lane == 0) {
+        std::uint32_t* hist{scr.hist};
+        int num_codes{0};
+        int code{0};
+        for (int i{0}; i < 18; ++i) {
+            if (hist[i]) {
+                if (num_codes == 0) {
+                    code = i;
+                    num_codes = 1;
+                } else if (num_codes == 1) {
+                    num_codes = 2;
+                    break;
+                }
+            }
+        }
+        std::uint8_t* cl_depth{scr.cl_depth};
+        std::uint16_t* cl_bits{scr.cl_bits};
+        for (int i{0}; i < 18; ++i) {
+            cl_depth[i] = 0;
+            cl_bits[i] = 0;
+        }
+        create_tree_serial(hist, 18, 5, cl_depth, scr.pool, scr.level);
+        canonical_codes(cl_depth, 18, cl_bits);
+        constexpr std::uint8_t kOrder[18]{1, 2, 3, 4, 0, 5, 17, 6, 16, 7, 8, 9, 10, 11, 12, 13, 14, 15};
+        constexpr std::uint8_t kSym[6]{0, 7, 3, 2, 1, 15};
+        constexpr std::uint8_t kLen[6]{2, 4, 3, 2, 2, 4};
+        int to_store{18};
+        if (num_codes > 1) {
+            for (; to_store > 0; --to_store) {
+                if (cl_depth[kOrder[to_store - 1]] != 0) break;
+            }
+        }
+        std::uint32_t skip{0};
+        if (cl_depth[kOrder[0]] == 0 && cl_depth[kOrder[1]] == 0) {
+            skip = 2;
+            if (cl_depth[kOrder[2]] == 0) skip = 3;
+        }
+        w.put(2, skip);
+        for (int i{static_cast<int>(skip)}; i < to_store; ++i) {
+            const int l{cl_depth[kOrder[i]]};
+            w.put(kLen[l], kSym[l]);
+        }
+        if (num_codes == 1) cl_depth[code] = 0;
+        pos = w.pos;
+    }
+    pos = __shfl_sync(kFull, pos, 0);
+    __syncwarp();
+    const std::uint32_t cap{w.cap};
+    for (int base{0}; base < new_len; base += 32) {
+        const int i{base + lane};
+        const int d{i < new_len ? s.depth[i] : 0};
+        const std::uint32_t n{i < new_len ? scr.cl_depth[d] : 0u};
+        const std::uint32_t incl{warp_incl_scan(n, lane)};
+        or_bits(w.buf, pos + incl - n, n, scr.cl_bits[d], cap);
+        pos += __shfl_sync(kFull, incl, 31);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        if (pos > cap) w.overflow = true;
+        w.pos = pos;
+    }
+}
+
 // build_and_store for s.hist[0..length) (src/bitstream/prefix_code.cc:387-426);
-// lane 0 writes the header into w.
+// the header goes to w (lane 0's copy holds the final position).
 __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, int lane) {
     int s4[4]{0, 0, 0, 0};
     int count{0};
-    if (lane == 0) count = symbol_census(s.hist, length, s4);
-    count = __shfl_sync(kFull, count, 0);
+    for (int base{0}; base < length && count <= 4; base += 32) {
+        const int sym{base + lane};
+        unsigned m{__ballot_sync(kFull, sym < length && s.hist[sym] != 0)};
+        while (m != 0 && count <= 4) {
+            if (count < 4) s4[count] = base + __ffs(m) - 1;
+            ++count;
+            m &= m - 1;
+        }
+    }
     if (count <= 1) {
         if (lane == 0) {
             w.put(4, 1);
@@ -650,11 +829,13 @@ __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, in
         return;
     }
     warp_create_tree(s, length, 15, lane);
-    if (lane == 0) {
-        canonical_codes(s.depth, length, s.bits);
-        store_code_header(count, s4, length, s.depth, w, s.cl);
+    warp_canonical_codes(s, length, lane);
+    if (count <= 4) {
+        if (lane == 0) store_code_header(count, s4, length, s.depth, w, s.cl);
+        __syncwarp();
+        return;
     }
-    __syncwarp();
+    warp_store_complex(s, length, w, lane);
 }
 
 // One single-warp CTA per histogram (the 32 AC clusters, then the DC and the
