@@ -43,7 +43,7 @@ EXPORTS = (
     "cujpegxl_b200_acsnet_trainer_step", "cujpegxl_b200_acsnet_trainer_params", "cujpegxl_b200_batch_set_acsnet",
     "cujpegxl_b200_encoder_create_ex", "cujpegxl_b200_max_output_size_ex",
     "cujpegxl_b200_debug_fail_allocation", "cujpegxl_b200_debug_live_allocations",
-    "cujpegxl_b200_encoder_enqueue_readback",
+    "cujpegxl_b200_encoder_enqueue_readback", "cujpegxl_b200_batch_schedule",
 )
 
 
@@ -70,6 +70,12 @@ class NetBatch(ctypes.Structure):
     _fields_ = [("tiles", ctypes.c_size_t), ("tile_index", ctypes.c_size_t), ("log2_distance", ctypes.c_size_t),
                 ("label_class", ctypes.c_size_t), ("label_qf", ctypes.c_size_t), ("n", ctypes.c_uint32),
                 ("label_soft", ctypes.c_size_t)]
+
+
+class BatchSchedule(ctypes.Structure):
+    _fields_ = [("frontend_ctas", ctypes.c_uint32), ("tiles_per_claim", ctypes.c_uint32),
+                ("dynamic_claims", ctypes.c_uint32), ("largest_first", ctypes.c_uint32),
+                ("from_cache", ctypes.c_uint32), ("candidates", ctypes.c_uint32), ("tuned_ms", ctypes.c_float)]
 
 
 class DevicePlanes(ctypes.Structure):
@@ -110,6 +116,7 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_encoder_stream.argtypes = [E, P(ctypes.c_size_t)]
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
     L.cujpegxl_b200_encoder_enqueue_readback.argtypes = [E, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    L.cujpegxl_b200_batch_schedule.argtypes = [E, P(BatchSchedule)]
     L.cujpegxl_b200_debug_fail_allocation.argtypes = [ctypes.c_uint32]
     L.cujpegxl_b200_debug_fail_allocation.restype = None
     L.cujpegxl_b200_debug_live_allocations.restype = ctypes.c_uint64

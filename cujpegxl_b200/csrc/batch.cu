@@ -1,19 +1,28 @@
 // Batched encode: many frames, each with its own geometry and distance, in one
 // CUDA graph launch.
 //
-// Every frame has its own encoder (arena, tables, output buffer). The graph
-// forks from a root stream into L lanes, encodes the frames on the lanes
-// (largest frames first, each to the lane with the least work so far), joins
-// the lanes, gathers every frame's result words with one small kernel and
-// copies them to pinned host memory. L is chosen on the first encode by
-// timing graphs with 1, 2, 4 and 8 lanes. A later encode with the same input
-// addresses relaunches the graph as it is; new addresses are captured again
-// and the executable graph is updated in place.
+// Every frame keeps its own encoder (arena, tables, output buffer), but the
+// work is not run frame by frame: the graph holds one persistent frontend
+// launch whose resident CTAs take the 64x64 tiles of all frames from one work
+// list (frontend_batch_launch), then one launch per entropy pass that runs
+// every frame's blocks of that pass (entropy_batch_launch), then a gather of
+// every frame's result words and their copy to pinned host memory. With a
+// transform-decision network attached, each frame's inference runs in front of
+// the frontend launch.
+//
+// The schedule of the frontend launch (resident CTAs, tiles per claim,
+// claims from a counter or round-robin, frames largest-first or in the given
+// order) is picked on the first encode by timing every candidate graph, and
+// cached per geometry mix for later batches. A later encode with the same
+// input addresses relaunches the graph as it is; new addresses are captured
+// again and the executable graph is updated in place.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <vector>
@@ -24,7 +33,6 @@
 
 namespace {
 
-constexpr int kMaxLanes = 8;
 constexpr int kResultWords = 3;  // total bytes, body start, status
 
 __global__ void gather_results(const unsigned long long* const* src, int count, unsigned long long* dst) {
@@ -56,24 +64,38 @@ bool same_inputs(const std::vector<cujpegxl_nv12_input>& a, const cujpegxl_nv12_
     return true;
 }
 
+// The frontend launch schedule the autotuner chooses among.
+struct Schedule {
+    int ctas_per_sm{2};
+    int chunk{1};
+    bool dynamic{true};
+    bool largest_first{true};
+    float ms{0.0f};  // measured time of one batch with it
+};
+
+// Tuned schedules of earlier batches, keyed by device, network use and the
+// frames' geometries in order.
+std::mutex g_cache_mutex;
+std::map<std::vector<std::uint64_t>, Schedule> g_cache;
+
 }  // namespace
 
 struct cujpegxl_b200_batch {
     int device{0};
+    int sms{0};
     std::vector<cujpegxl_encoder*> encs;
-    std::vector<std::size_t> order;  // frames by pixel count, largest first
     std::vector<std::size_t> pixels;
     std::vector<std::uint32_t> widths;
     cudaStream_t root{nullptr};
-    cudaStream_t lanes[kMaxLanes]{};
-    cudaEvent_t fork{nullptr};
-    cudaEvent_t join[kMaxLanes]{};
+    std::uint32_t* counters{nullptr};                 // device, one frontend claim counter per group
     const unsigned long long** result_ptrs{nullptr};  // device [count]
     unsigned long long* gathered{nullptr};            // device [count][3]
     unsigned long long* gathered_host{nullptr};       // pinned [count][3]
     cudaGraphExec_t exec{nullptr};
     std::vector<cujpegxl_nv12_input> bound;
-    int lanes_used{0};
+    Schedule schedule{};
+    bool tuned{false};
+    bool from_cache{false};
     bool launched{false};
 };
 
@@ -83,37 +105,62 @@ void release(cujpegxl_b200_batch* b) {
     DeviceScope scope{b->device};
     if (b->root) cudaStreamSynchronize(b->root);
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    for (int l{0}; l < kMaxLanes; ++l) {
-        if (b->lanes[l]) cudaStreamDestroy(b->lanes[l]);
-        if (b->join[l]) cudaEventDestroy(b->join[l]);
-    }
-    if (b->fork) cudaEventDestroy(b->fork);
     if (b->root) cudaStreamDestroy(b->root);
+    if (b->counters) cudaFree(b->counters);
     if (b->result_ptrs) cudaFree(b->result_ptrs);
     if (b->gathered) cudaFree(b->gathered);
     if (b->gathered_host) cudaFreeHost(b->gathered_host);
     for (cujpegxl_encoder* e : b->encs) cujpegxl_encoder_destroy(e);
 }
 
-// Records the whole batch on the root stream as a graph with `lanes` lanes.
-bool capture(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, int lanes, cudaGraph_t* graph) {
+std::size_t groups_of(std::size_t count) {
+    return (count + jxb::kBatchFrames - 1) / jxb::kBatchFrames;
+}
+
+// Records the whole batch on the root stream as a graph with schedule `sc`:
+// frames in groups of at most kBatchFrames, each group one frontend launch
+// and one launch per entropy pass.
+bool capture(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, const Schedule& sc, cudaGraph_t* graph) {
+    const std::size_t count{b->encs.size()};
+    std::vector<std::size_t> order(count);
+    std::iota(order.begin(), order.end(), std::size_t{0});
+    if (sc.largest_first) {
+        std::stable_sort(order.begin(), order.end(),
+                         [&](std::size_t x, std::size_t y) { return b->pixels[x] > b->pixels[y]; });
+    }
     if (cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
-    bool ok{cudaEventRecord(b->fork, b->root) == cudaSuccess};
-    for (int l{0}; ok && l < lanes; ++l) ok = cudaStreamWaitEvent(b->lanes[l], b->fork, 0) == cudaSuccess;
-    std::vector<std::size_t> load(static_cast<std::size_t>(lanes), 0);
-    for (std::size_t k{0}; ok && k < b->order.size(); ++k) {
-        const std::size_t i{b->order[k]};
-        const int l{static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin())};
-        load[static_cast<std::size_t>(l)] += b->pixels[i];
-        ok = jxb::encoder_launch(b->encs[i], inputs[i], b->lanes[l]);
+    bool ok{true};
+    auto* fb{new (std::nothrow) jxb::FrontendBatch{}};
+    auto* eb{new (std::nothrow) jxb::EntropyBatch{}};
+    ok = fb != nullptr && eb != nullptr;
+    for (std::size_t g0{0}, grp{0}; ok && g0 < count; g0 += jxb::kBatchFrames, ++grp) {
+        const std::size_t n{std::min<std::size_t>(jxb::kBatchFrames, count - g0)};
+        std::uint32_t tiles{0};
+        for (std::size_t k{0}; ok && k < n; ++k) {
+            const std::size_t i{order[g0 + k]};
+            jxb::FrontendJob& job{fb->jobs[k]};
+            ok = jxb::encoder_frontend_job(b->encs[i], inputs[i], b->root, &job, &fb->tb);
+            job.tile_begin = tiles;
+            const std::uint32_t th{(static_cast<std::uint32_t>(job.in.height) + 63) / 64};
+            tiles += static_cast<std::uint32_t>(job.tiles_x) * th;
+            eb->frames[k] = jxb::encoder_entropy(b->encs[i]);
+        }
+        if (!ok) break;
+        fb->nframes = static_cast<int>(n);
+        fb->chunk = sc.chunk;
+        fb->total_tiles = tiles;
+        fb->counter = sc.dynamic ? b->counters + grp : nullptr;
+        eb->nframes = static_cast<int>(n);
+        jxb::entropy_batch_plan(*eb);
+        ok = (!sc.dynamic || cudaMemsetAsync(fb->counter, 0, sizeof(std::uint32_t), b->root) == cudaSuccess) &&
+             jxb::frontend_batch_launch(*fb, sc.ctas_per_sm * b->sms, b->root) &&
+             jxb::entropy_batch_launch(*eb, b->root);
     }
-    for (int l{0}; ok && l < lanes; ++l) {
-        ok = cudaEventRecord(b->join[l], b->lanes[l]) == cudaSuccess &&
-             cudaStreamWaitEvent(b->root, b->join[l], 0) == cudaSuccess;
-    }
-    const int count{static_cast<int>(b->encs.size())};
+    delete fb;
+    delete eb;
+    const int icount{static_cast<int>(count)};
     if (ok) {
-        gather_results<<<(count + 127) / 128, 128, 0, b->root>>>(b->result_ptrs, count, b->gathered);
+        gather_results<<<(icount + 127) / 128, 128, 0, b->root>>>(b->result_ptrs, icount, b->gathered);
         ok = cudaGetLastError() == cudaSuccess &&
              cudaMemcpyAsync(b->gathered_host, b->gathered, sizeof(unsigned long long) * kResultWords * count,
                              cudaMemcpyDeviceToHost, b->root) == cudaSuccess;
@@ -129,28 +176,66 @@ bool capture(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, int lane
     return true;
 }
 
-bool instantiate(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, int lanes, cudaGraphExec_t* exec) {
+bool instantiate(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, const Schedule& sc,
+                 cudaGraphExec_t* exec) {
     cudaGraph_t g{nullptr};
-    if (!capture(b, inputs, lanes, &g)) return false;
+    if (!capture(b, inputs, sc, &g)) return false;
     const bool ok{cudaGraphInstantiate(exec, g, 0) == cudaSuccess};
     cudaGraphDestroy(g);
     return ok;
 }
 
-// Times candidate lane counts on the given inputs and keeps the fastest graph.
+std::vector<std::uint64_t> cache_key(const cujpegxl_b200_batch* b) {
+    std::vector<std::uint64_t> key{static_cast<std::uint64_t>(b->device)};
+    for (cujpegxl_encoder* e : b->encs) {
+        const jxb::EntropyDev& ed{jxb::encoder_entropy(e)};
+        key.push_back((static_cast<std::uint64_t>(ed.width) << 32) | static_cast<std::uint64_t>(ed.height));
+    }
+    key.push_back(jxb::encoder_has_network(b->encs.front()) ? 1u : 0u);
+    return key;
+}
+
+// The candidates: dynamic claims of 1, 2 or 4 tiles with one or two CTAs per
+// SM, and round-robin claims of single tiles with two, each with the frames
+// largest-first and in the given order.
+std::vector<Schedule> candidates() {
+    std::vector<Schedule> out;
+    for (const bool largest : {true, false}) {
+        for (const int per_sm : {2, 1}) {
+            for (const int chunk : {1, 2, 4}) out.push_back(Schedule{per_sm, chunk, true, largest, 0.0f});
+        }
+        out.push_back(Schedule{2, 1, false, largest, 0.0f});
+    }
+    return out;
+}
+
+// Times every candidate schedule on the given inputs (one warm-up and two
+// timed launches each) and keeps the fastest graph; a geometry mix tuned
+// before reuses its schedule without timing.
 bool autotune(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs) {
-    const int count{static_cast<int>(b->encs.size())};
+    const std::vector<std::uint64_t> key{cache_key(b)};
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        const auto it{g_cache.find(key)};
+        if (it != g_cache.end()) {
+            cudaGraphExec_t exec{nullptr};
+            if (!instantiate(b, inputs, it->second, &exec)) return false;
+            b->exec = exec;
+            b->schedule = it->second;
+            b->tuned = true;
+            b->from_cache = true;
+            return true;
+        }
+    }
     cudaEvent_t t0{nullptr};
     cudaEvent_t t1{nullptr};
     if (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess) return false;
-    float best_ms{0.0f};
     cudaGraphExec_t best{nullptr};
-    int best_lanes{0};
+    Schedule best_sc{};
     bool ok{true};
-    for (int lanes{1}; ok && lanes <= kMaxLanes; lanes *= 2) {
-        if (lanes > 1 && lanes > count) break;
+    for (Schedule sc : candidates()) {
         cudaGraphExec_t exec{nullptr};
-        if (!instantiate(b, inputs, lanes, &exec)) {
+        if (!instantiate(b, inputs, sc, &exec)) {
             ok = false;
             break;
         }
@@ -159,11 +244,15 @@ bool autotune(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs) {
         for (int r{0}; ok && r < 2; ++r) ok = cudaGraphLaunch(exec, b->root) == cudaSuccess;
         ok = ok && cudaEventRecord(t1, b->root) == cudaSuccess && cudaEventSynchronize(t1) == cudaSuccess &&
              cudaEventElapsedTime(&ms, t0, t1) == cudaSuccess;
-        if (ok && (best == nullptr || ms < best_ms)) {
+        if (!ok) {
+            cudaGraphExecDestroy(exec);
+            break;
+        }
+        sc.ms = ms / 2.0f;
+        if (best == nullptr || sc.ms < best_sc.ms) {
             if (best) cudaGraphExecDestroy(best);
             best = exec;
-            best_ms = ms;
-            best_lanes = lanes;
+            best_sc = sc;
         } else {
             cudaGraphExecDestroy(exec);
         }
@@ -175,7 +264,11 @@ bool autotune(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs) {
         return false;
     }
     b->exec = best;
-    b->lanes_used = best_lanes;
+    b->schedule = best_sc;
+    b->tuned = true;
+    b->from_cache = false;
+    std::lock_guard<std::mutex> lock(g_cache_mutex);
+    g_cache[key] = best_sc;
     return true;
 }
 
@@ -205,20 +298,14 @@ cujpegxl_status cujpegxl_b200_batch_create(const cujpegxl_config* frames, size_t
         b->pixels.push_back(static_cast<std::size_t>(frames[i].width) * frames[i].height);
         b->widths.push_back(frames[i].width);
     }
-    b->order.resize(count);
-    std::iota(b->order.begin(), b->order.end(), std::size_t{0});
-    std::stable_sort(b->order.begin(), b->order.end(),
-                     [&](std::size_t x, std::size_t y) { return b->pixels[x] > b->pixels[y]; });
     DeviceScope scope{b->device};
     bool ok{scope.ok() && cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess};
-    for (int l{0}; ok && l < kMaxLanes; ++l) {
-        ok = cudaStreamCreateWithFlags(&b->lanes[l], cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&b->join[l], cudaEventDisableTiming) == cudaSuccess;
-    }
+            cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device) == cudaSuccess};
     std::vector<const unsigned long long*> ptrs(count);
     for (size_t i{0}; i < count; ++i) ptrs[i] = jxb::encoder_result_words(b->encs[i]);
-    ok = ok && cudaMalloc(reinterpret_cast<void**>(&b->result_ptrs), sizeof(void*) * count) == cudaSuccess &&
+    ok = ok && cudaMalloc(reinterpret_cast<void**>(&b->counters), sizeof(std::uint32_t) * groups_of(count)) ==
+                   cudaSuccess &&
+         cudaMalloc(reinterpret_cast<void**>(&b->result_ptrs), sizeof(void*) * count) == cudaSuccess &&
          cudaMalloc(reinterpret_cast<void**>(&b->gathered), sizeof(unsigned long long) * kResultWords * count) ==
              cudaSuccess &&
          cudaHostAlloc(reinterpret_cast<void**>(&b->gathered_host), sizeof(unsigned long long) * kResultWords * count,
@@ -251,7 +338,7 @@ cujpegxl_status cujpegxl_b200_batch_encode(cujpegxl_b200_batch* batch, const cuj
         batch->bound.assign(inputs, inputs + batch->encs.size());
     } else if (!same_inputs(batch->bound, inputs)) {
         cudaGraph_t g{nullptr};
-        if (!capture(batch, inputs, batch->lanes_used, &g)) return CUJPEGXL_INTERNAL_ERROR;
+        if (!capture(batch, inputs, batch->schedule, &g)) return CUJPEGXL_INTERNAL_ERROR;
         cudaGraphExecUpdateResultInfo info{};
         if (cudaGraphExecUpdate(batch->exec, g, &info) != cudaSuccess) {
             cudaGetLastError();
@@ -345,7 +432,20 @@ cujpegxl_status cujpegxl_b200_batch_stream(const cujpegxl_b200_batch* batch, uin
 }
 
 uint32_t cujpegxl_b200_batch_lanes(const cujpegxl_b200_batch* batch) {
-    return batch == nullptr ? 0u : static_cast<uint32_t>(batch->lanes_used);
+    return batch == nullptr || !batch->tuned ? 0u : 1u;
+}
+
+cujpegxl_status cujpegxl_b200_batch_schedule(const cujpegxl_b200_batch* batch,
+                                             cujpegxl_b200_batch_schedule_info* out) {
+    if (batch == nullptr || out == nullptr || !batch->tuned) return CUJPEGXL_INVALID_ARGUMENT;
+    out->frontend_ctas = static_cast<uint32_t>(batch->schedule.ctas_per_sm * batch->sms);
+    out->tiles_per_claim = static_cast<uint32_t>(batch->schedule.chunk);
+    out->dynamic_claims = batch->schedule.dynamic ? 1u : 0u;
+    out->largest_first = batch->schedule.largest_first ? 1u : 0u;
+    out->from_cache = batch->from_cache ? 1u : 0u;
+    out->candidates = static_cast<uint32_t>(candidates().size());
+    out->tuned_ms = batch->schedule.ms;
+    return CUJPEGXL_OK;
 }
 
 void cujpegxl_b200_batch_destroy(cujpegxl_b200_batch* batch) {

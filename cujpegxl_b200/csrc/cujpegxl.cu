@@ -558,6 +558,33 @@ bool encoder_launch(cujpegxl_encoder* e, const cujpegxl_nv12_input& input, cudaS
                          reinterpret_cast<const std::uint8_t*>(input.chroma), input.chroma_pitch, 3u, stream);
 }
 
+bool encoder_frontend_job(cujpegxl_encoder* e, const cujpegxl_nv12_input& input, cudaStream_t stream,
+                          FrontendJob* job, FrontendTables* tables) {
+    if (!device_tables(e->device, tables)) return false;
+    FrontendInputs in{reinterpret_cast<const std::uint8_t*>(input.luma), reinterpret_cast<const std::uint8_t*>(input.chroma),
+                      input.luma_pitch, input.chroma_pitch, static_cast<int>(e->config.width),
+                      static_cast<int>(e->config.height), nullptr, nullptr};
+    if (e->net != nullptr) {
+        const NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr};
+        if (!acsnet_infer_launch(in, *acsnet_params(e->net), std::log2(e->config.distance), e->net_margin, dec,
+                                 stream)) {
+            return false;
+        }
+        in.net_class = dec.cls;
+        in.net_qf = dec.qf;
+    }
+    job->in = in;
+    job->sc = e->fs;
+    job->out = e->fo;
+    job->tiles_x = static_cast<int>((e->config.width + 63) / 64);
+    job->tile_begin = 0;
+    return true;
+}
+
+const EntropyDev& encoder_entropy(const cujpegxl_encoder* e) { return e->ed; }
+
+bool encoder_has_network(const cujpegxl_encoder* e) { return e->net != nullptr; }
+
 const unsigned long long* encoder_result_words(const cujpegxl_encoder* e) { return e->ed.result; }
 
 const std::uint8_t* encoder_output(const cujpegxl_encoder* e) { return e->ed.out; }

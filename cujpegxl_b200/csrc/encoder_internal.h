@@ -9,6 +9,8 @@
 
 #include "cujpegxl/cujpegxl.h"
 #include "cujpegxl_b200/cujpegxl_b200.h"
+#include "entropy.cuh"
+#include "frontend.cuh"
 
 namespace jxb {
 
@@ -31,5 +33,18 @@ const unsigned long long* encoder_result_words(const cujpegxl_encoder* e);
 
 // Device address of the encoded file.
 const std::uint8_t* encoder_output(const cujpegxl_encoder* e);
+
+// The frontend work of one encode of `input` (validated by the caller) as a
+// job of a batched frontend launch, and the device tables it uses. With a
+// network attached, its inference is enqueued on `stream` here and the job
+// reads the decisions. Issues only kernel launches, so it may be captured.
+bool encoder_frontend_job(cujpegxl_encoder* e, const cujpegxl_nv12_input& input, cudaStream_t stream,
+                          FrontendJob* job, FrontendTables* tables);
+
+// The encoder's entropy-stage state (valid after encoder_prepare).
+const EntropyDev& encoder_entropy(const cujpegxl_encoder* e);
+
+// Whether a transform-decision network is attached.
+bool encoder_has_network(const cujpegxl_encoder* e);
 
 }  // namespace jxb

@@ -18,6 +18,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "entropy.cuh"
@@ -434,7 +435,7 @@ __device__ std::uint32_t cta_exclusive_scan(std::uint32_t v, std::uint32_t* warp
 // tokens counted into the 32-cluster histogram and written, in stream order,
 // to a run of the token pool that the stripe reserves once it knows their
 // number (count tokens first sized, then the coefficient extents).
-__global__ void __launch_bounds__(kAcThreads) ac_tok_kernel(EntropyDev e) {
+__device__ __forceinline__ void ac_tok_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
     std::uint32_t* hist{reinterpret_cast<std::uint32_t*>(ac_smem + sizeof(StripeStage))};  // [32][64]
@@ -443,7 +444,7 @@ __global__ void __launch_bounds__(kAcThreads) ac_tok_kernel(EntropyDev e) {
     __shared__ int sh_stored;
     const int tid{static_cast<int>(threadIdx.x)};
     const int lane{tid & 31};
-    const Stripe st{e.stripes[blockIdx.x]};
+    const Stripe st{e.stripes[blk]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
     for (int i{tid}; i < kNumClusters * kAcSymbols; i += kAcThreads) hist[i] = 0;
     stage_stripe(e, st, gg, s);
@@ -486,8 +487,8 @@ __global__ void __launch_bounds__(kAcThreads) ac_tok_kernel(EntropyDev e) {
         }
         sh_base = base;
         sh_stored = stored ? 1 : 0;
-        e.stripe_tok[2 * blockIdx.x] = stored ? base : kNoTokens;
-        e.stripe_tok[2 * blockIdx.x + 1] = total;
+        e.stripe_tok[2 * blk] = stored ? base : kNoTokens;
+        e.stripe_tok[2 * blk + 1] = total;
     }
     __syncthreads();
     const bool stored{sh_stored != 0};
@@ -550,12 +551,12 @@ struct HistVisitor {
     }
 };
 
-__global__ void __launch_bounds__(256) misc_hist_kernel(EntropyDev e) {
+__device__ __forceinline__ void misc_hist_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     __shared__ std::uint32_t sh_g[4 * 256];
     __shared__ std::uint32_t sh_fb[2];
     if (threadIdx.x < 2) sh_fb[threadIdx.x] = 0;
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) sh_g[i] = 0;
-    const std::uint32_t first{blockIdx.x * blockDim.x};
+    const std::uint32_t first{blk * blockDim.x};
     const std::uint32_t last{min(first + blockDim.x, e.ac_first) - 1};
     const Section s0{e.sections[find_section(e.sections, 0, misc_hi(e), first)]};
     const Section s1{e.sections[find_section(e.sections, 0, misc_hi(e), last)]};
@@ -841,7 +842,7 @@ __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, in
 // One single-warp CTA per histogram (the 32 AC clusters, then the DC and the
 // AcMetadata histogram of every DC group): the construction is a long serial
 // chain on lane 0, so each chain gets an SM to itself.
-__global__ void __launch_bounds__(32) codes_kernel(EntropyDev e) {
+__device__ __forceinline__ void codes_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char code_smem[];
     const int lane{static_cast<int>(threadIdx.x) & 31};
     WarpCodeSmem& s{*reinterpret_cast<WarpCodeSmem*>(code_smem)};
@@ -851,16 +852,16 @@ __global__ void __launch_bounds__(32) codes_kernel(EntropyDev e) {
     std::uint16_t* dst_bits;
     bool clustered;
     std::uint32_t extra0{0};
-    if (blockIdx.x < kNumClusters) {
-        const int c{static_cast<int>(blockIdx.x)};
+    if (blk < kNumClusters) {
+        const int c{static_cast<int>(blk)};
         idx = c;
         src = e.ac_hist + c * 256;
         dst_depth = e.ac_depth + c * 256;
         dst_bits = e.ac_bits + c * 256;
         clustered = true;
     } else {
-        const int g{(static_cast<int>(blockIdx.x) - kNumClusters) >> 1};
-        const int warp{(static_cast<int>(blockIdx.x) - kNumClusters) & 1};
+        const int g{(static_cast<int>(blk) - kNumClusters) >> 1};
+        const int warp{(static_cast<int>(blk) - kNumClusters) & 1};
         if (warp == 0) {
             idx = 32 + g;
             src = e.dc_hist + g * 256;
@@ -913,19 +914,19 @@ __global__ void __launch_bounds__(32) codes_kernel(EntropyDev e) {
 
 // ---- pass 3: bit lengths and scan ----------------------------------------------------
 
-__global__ void __launch_bounds__(kAcThreads) ac_bits_kernel(EntropyDev e) {
+__device__ __forceinline__ void ac_bits_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
     __shared__ std::uint32_t sh_sum[kAcWarps];
     const int tid{static_cast<int>(threadIdx.x)};
     const int lane{tid & 31};
-    const Stripe st{e.stripes[blockIdx.x]};
+    const Stripe st{e.stripes[blk]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
-    const std::uint32_t tbase{e.stripe_tok[2 * blockIdx.x]};
+    const std::uint32_t tbase{e.stripe_tok[2 * blk]};
     if (tbase != kNoTokens) {
         // Stored tokens: the stripe's whole length goes on its first item
         // (the scan only needs sums at stripe and section starts).
-        const std::uint32_t ntok{e.stripe_tok[2 * blockIdx.x + 1]};
+        const std::uint32_t ntok{e.stripe_tok[2 * blk + 1]};
         const std::uint32_t* pool{e.tok_pool + tbase};
         std::uint32_t sum{0};
         for (std::uint32_t t{static_cast<std::uint32_t>(tid)}; t < ntok; t += kAcThreads) {
@@ -992,8 +993,8 @@ struct BitsVisitor {
     }
 };
 
-__global__ void __launch_bounds__(256) misc_bits_kernel(EntropyDev e) {
-    const std::uint32_t item{blockIdx.x * blockDim.x + threadIdx.x};
+__device__ __forceinline__ void misc_bits_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    const std::uint32_t item{blk * blockDim.x + threadIdx.x};
     if (item >= e.ac_first) return;
     BitsVisitor v{&e, 0};
     visit_misc(e, item, v);
@@ -1001,9 +1002,9 @@ __global__ void __launch_bounds__(256) misc_bits_kernel(EntropyDev e) {
 }
 
 // Exclusive scan of item_bits inside tiles of kScanTile items (1024 threads x 4).
-__global__ void __launch_bounds__(1024) scan_tile_kernel(EntropyDev e) {
+__device__ __forceinline__ void scan_tile_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     __shared__ std::uint32_t warp_sums[32];
-    const std::uint32_t base{blockIdx.x * kScanTile + threadIdx.x * 4};
+    const std::uint32_t base{blk * kScanTile + threadIdx.x * 4};
     std::uint32_t v[4];
     std::uint32_t local{0};
 #pragma unroll
@@ -1030,7 +1031,7 @@ __global__ void __launch_bounds__(1024) scan_tile_kernel(EntropyDev e) {
             if (lane >= off) wi += t;
         }
         warp_sums[lane] = wi - ws;
-        if (lane == 31) e.tile_sum[blockIdx.x] = wi;
+        if (lane == 31) e.tile_sum[blk] = wi;
     }
     __syncthreads();
     std::uint32_t run{warp_sums[warp] + incl - local};
@@ -1041,7 +1042,7 @@ __global__ void __launch_bounds__(1024) scan_tile_kernel(EntropyDev e) {
     }
 }
 
-__global__ void __launch_bounds__(1024) scan_top_kernel(EntropyDev e) {
+__device__ __forceinline__ void scan_top_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     __shared__ unsigned long long warp_sums[32];
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
@@ -1173,7 +1174,7 @@ __device__ unsigned long long block_scan(unsigned long long v, unsigned long lon
 // (src/bitstream/codestream.cc:57-135, src/bitstream/container.cc:35-62).
 // Dynamic shared memory: the section sizes, then the header words
 // (layout_head_bytes).
-__global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
+__device__ __forceinline__ void layout_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char layout_smem[];
     __shared__ unsigned long long scan_sums[33];
     __shared__ unsigned long long sh_start, sh_status, sh_head;
@@ -1315,13 +1316,13 @@ __global__ void __launch_bounds__(kLayoutThreads) layout_kernel(EntropyDev e) {
     }
 }
 
-__global__ void zero_body_kernel(EntropyDev e) {
+__device__ __forceinline__ void zero_body_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     if (e.result[2] != 0) return;
     const unsigned long long start{e.result[1]};
     const unsigned long long end{e.result[0]};
     const unsigned long long a{(start + 15) & ~15ull};
-    const unsigned long long stride{static_cast<unsigned long long>(gridDim.x) * blockDim.x};
-    const unsigned long long tid{static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x};
+    const unsigned long long stride{static_cast<unsigned long long>(nblk) * blockDim.x};
+    const unsigned long long tid{static_cast<unsigned long long>(blk) * blockDim.x + threadIdx.x};
     if (tid < a - start && start + tid < end) e.out[start + tid] = 0;
     const unsigned long long nvec{end > a ? (end - a) / 16 : 0};
     uint4* v{reinterpret_cast<uint4*>(e.out + a)};
@@ -1350,7 +1351,7 @@ __device__ void flush_window(const unsigned int* win, int nwords, unsigned int* 
 // Writes a stripe's tokens. The stripe's bits are contiguous in its section;
 // they are assembled in a shared-memory window and written out with plain
 // stores (global atomics only when the stripe exceeds the window).
-__global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
+__device__ __forceinline__ void ac_emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
     unsigned int* win{reinterpret_cast<unsigned int*>(ac_smem + sizeof(StripeStage))};
@@ -1360,10 +1361,10 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     if (e.result[2] != 0) return;
     const int tid{static_cast<int>(threadIdx.x)};
     const int lane{tid & 31};
-    const Stripe st{e.stripes[blockIdx.x]};
+    const Stripe st{e.stripes[blk]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
     const int nitems{3 * st.rows * gg.gw};
-    if (e.stripe_tok[2 * blockIdx.x] == kNoTokens) {
+    if (e.stripe_tok[2 * blk] == kNoTokens) {
         stage_stripe(e, st, gg, s);
     } else if (tid == 0) {
         s.nactive = 0;
@@ -1383,13 +1384,13 @@ __global__ void __launch_bounds__(kAcThreads) ac_emit_kernel(EntropyDev e) {
     for (int i{tid}; i < nwords; i += kAcThreads) win[i] = 0;
     unsigned int* words{nwords >= 0 ? win : reinterpret_cast<unsigned int*>(e.out)};
     const unsigned long long base{nwords >= 0 ? (sh_start & 31) : sh_start};
-    const std::uint32_t tbase{e.stripe_tok[2 * blockIdx.x]};
+    const std::uint32_t tbase{e.stripe_tok[2 * blk]};
     if (tbase != kNoTokens) {
         // Stored tokens in stream order: their lengths, a CTA scan for their
         // offsets, and their bits, kAcThreads * kPer tokens per round.
         __shared__ std::uint32_t sh_scan[kAcWarps + 1];
         constexpr int kPer{4};
-        const std::uint32_t ntok{e.stripe_tok[2 * blockIdx.x + 1]};
+        const std::uint32_t ntok{e.stripe_tok[2 * blk + 1]};
         const std::uint32_t* pool{e.tok_pool + tbase};
         __syncthreads();
         unsigned long long run{base};
@@ -1529,7 +1530,7 @@ constexpr int kMiscWindowWords = 2048;
 
 // One thread per non-AC item; the bits of the block's items that share the
 // first item's section are assembled in a shared-memory window.
-__global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
+__device__ __forceinline__ void misc_emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     __shared__ unsigned int win[kMiscWindowWords];
     __shared__ DeferredBlob deferred[kMaxDeferred];
     __shared__ unsigned long long sh_start;
@@ -1537,7 +1538,7 @@ __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
     __shared__ int sh_words;
     __shared__ int sh_ndeferred;
     if (e.result[2] != 0) return;
-    const std::uint32_t first{blockIdx.x * blockDim.x};
+    const std::uint32_t first{blk * blockDim.x};
     const std::uint32_t item{first + threadIdx.x};
     if (threadIdx.x == 0) {
         sh_ndeferred = 0;
@@ -1582,11 +1583,73 @@ __global__ void __launch_bounds__(256) misc_emit_kernel(EntropyDev e) {
     if (nwords > 0) flush_window(win, nwords, reinterpret_cast<unsigned int*>(e.out), sh_start >> 5);
 }
 
+// Clears a frame's histograms and counters (the first step of every encode).
+__device__ __forceinline__ void clear_body(const EntropyDev& e) {
+    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) e.ac_hist[i] = 0;
+    for (int i{static_cast<int>(threadIdx.x)}; i < e.ndc * 256; i += blockDim.x) {
+        e.dc_hist[i] = 0;
+        e.am_hist[i] = 0;
+    }
+    for (int i{static_cast<int>(threadIdx.x)}; i < e.ndc; i += blockDim.x) e.fb_count[i] = 0;
+    if (threadIdx.x == 0) *e.tok_count = 0;
+}
+
+// ---- kernels: one frame per launch, and every frame of a batch per launch -----------
+
+// Blocks of a single-frame launch of the body-zeroing pass.
+constexpr unsigned kZeroBlocks = 296;
+// Blocks per frame of the body-zeroing pass in a batched launch.
+constexpr unsigned kZeroBlocksBatched = 32;
+
+#define JXB_ENTROPY_KERNELS(NAME, BOUNDS, PHASE, NBLK)                                                     \
+    __global__ void BOUNDS NAME##_kernel(const __grid_constant__ EntropyDev e) {                              \
+        NAME##_body(e, blockIdx.x, gridDim.x);                                                                \
+    }                                                                                                         \
+    __global__ void BOUNDS NAME##_batch_kernel(const __grid_constant__ EntropyBatch b) {                      \
+        const int f{batch_frame(b, PHASE, blockIdx.x)};                                                      \
+        NAME##_body(b.frames[f], blockIdx.x - b.begin[PHASE][f], NBLK);                                       \
+    }
+
+// Frame of block `blk` of a batched launch of `phase` (binary search over the
+// frames' first blocks).
+__device__ __forceinline__ int batch_frame(const EntropyBatch& b, int phase, unsigned blk) {
+    int lo{0};
+    int hi{b.nframes - 1};
+    while (lo < hi) {
+        const int mid{(lo + hi + 1) >> 1};
+        if (b.begin[phase][mid] <= blk) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+JXB_ENTROPY_KERNELS(ac_tok, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
+JXB_ENTROPY_KERNELS(misc_hist, __launch_bounds__(256), kPhaseMisc, 0u)
+JXB_ENTROPY_KERNELS(codes, __launch_bounds__(32), kPhaseCodes, 0u)
+JXB_ENTROPY_KERNELS(ac_bits, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
+JXB_ENTROPY_KERNELS(misc_bits, __launch_bounds__(256), kPhaseMisc, 0u)
+JXB_ENTROPY_KERNELS(scan_tile, __launch_bounds__(1024), kPhaseScan, 0u)
+JXB_ENTROPY_KERNELS(scan_top, __launch_bounds__(1024), kPhaseFrame, 0u)
+JXB_ENTROPY_KERNELS(layout, __launch_bounds__(kLayoutThreads), kPhaseFrame, 0u)
+JXB_ENTROPY_KERNELS(zero_body, __launch_bounds__(256), kPhaseZero, kZeroBlocksBatched)
+JXB_ENTROPY_KERNELS(ac_emit, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
+JXB_ENTROPY_KERNELS(misc_emit, __launch_bounds__(256), kPhaseMisc, 0u)
+#undef JXB_ENTROPY_KERNELS
+
+__global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
+    clear_body(b.frames[blockIdx.x]);
+}
+
 constexpr std::size_t kHistSmem{sizeof(StripeStage) + kNumClusters * kAcSymbols * sizeof(std::uint32_t)};
 constexpr std::size_t kBitsSmem{sizeof(StripeStage)};
 constexpr std::size_t kEmitSmem{sizeof(StripeStage) + kWindowWords * sizeof(unsigned int)};
 
 }  // namespace
+
+static_assert(sizeof(EntropyBatch) <= 32000, "a batched entropy launch's parameters exceed the kernel parameter limit");
 
 bool entropy_launch(const EntropyDev& e, void* stream) {
     if (e.nsec > kMaxSections) return false;
@@ -1609,9 +1672,47 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
     layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
-    zero_body_kernel<<<296, 256, 0, st>>>(e);
+    zero_body_kernel<<<kZeroBlocks, 256, 0, st>>>(e);
     ac_emit_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(e);
     misc_emit_kernel<<<misc, 256, 0, st>>>(e);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+void entropy_batch_plan(EntropyBatch& b) {
+    for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][0] = 0;
+    for (int f{0}; f < b.nframes; ++f) {
+        const EntropyDev& e{b.frames[f]};
+        const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes), (e.ac_first + 255) / 256,
+                                                 static_cast<std::uint32_t>(kNumClusters + 2 * e.ndc), e.num_tiles,
+                                                 1u, kZeroBlocksBatched};
+        for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][f + 1] = b.begin[p][f] + per[p];
+    }
+}
+
+bool entropy_batch_launch(const EntropyBatch& b, void* stream) {
+    if (b.nframes <= 0 || b.nframes > kEntropyBatchFrames) return false;
+    std::uint32_t layout_smem{0};
+    for (int f{0}; f < b.nframes; ++f) {
+        const EntropyDev& e{b.frames[f]};
+        if (e.nsec > kMaxSections) return false;
+        layout_smem = std::max(layout_smem, layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec));
+    }
+    cudaStream_t st{static_cast<cudaStream_t>(stream)};
+    const int nf{b.nframes};
+    const unsigned stripes{b.begin[kPhaseStripes][nf]};
+    const unsigned misc{b.begin[kPhaseMisc][nf]};
+    clear_batch_kernel<<<static_cast<unsigned>(nf), 256, 0, st>>>(b);
+    ac_tok_batch_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(b);
+    misc_hist_batch_kernel<<<misc, 256, 0, st>>>(b);
+    codes_batch_kernel<<<b.begin[kPhaseCodes][nf], 32, sizeof(WarpCodeSmem), st>>>(b);
+    ac_bits_batch_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(b);
+    misc_bits_batch_kernel<<<misc, 256, 0, st>>>(b);
+    scan_tile_batch_kernel<<<b.begin[kPhaseScan][nf], 1024, 0, st>>>(b);
+    scan_top_batch_kernel<<<static_cast<unsigned>(nf), 1024, 0, st>>>(b);
+    layout_batch_kernel<<<static_cast<unsigned>(nf), kLayoutThreads, layout_smem, st>>>(b);
+    zero_body_batch_kernel<<<b.begin[kPhaseZero][nf], 256, 0, st>>>(b);
+    ac_emit_batch_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(b);
+    misc_emit_batch_kernel<<<misc, 256, 0, st>>>(b);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1625,6 +1726,16 @@ bool entropy_kernels_init() {
            cudaFuncSetAttribute(ac_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&
            cudaFuncSetAttribute(ac_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kEmitSmem)) == cudaSuccess &&
+           cudaFuncSetAttribute(codes_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
+           cudaFuncSetAttribute(layout_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_tok_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kHistSmem)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_bits_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kBitsSmem)) == cudaSuccess &&
+           cudaFuncSetAttribute(ac_emit_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kEmitSmem)) == cudaSuccess;
 }
 

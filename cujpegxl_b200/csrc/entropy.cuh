@@ -158,4 +158,29 @@ std::size_t worst_case_output(std::uint32_t width, std::uint32_t height);
 // capacity exceeded).
 bool entropy_launch(const EntropyDev& e, void* stream);
 
+// Several frames' entropy stages as one launch per pass: each pass runs the
+// blocks of every frame, frame f owning blocks begin[phase][f] ..
+// begin[phase][f + 1] - 1. The frames live in the launch's parameter block.
+constexpr int kEntropyBatchFrames = 64;
+enum EntropyPhase : int {
+    kPhaseStripes = 0,  // AC stripe passes: one block per stripe
+    kPhaseMisc = 1,     // other items: 256 per block
+    kPhaseCodes = 2,    // prefix codes: one block per histogram
+    kPhaseScan = 3,     // item scan tiles
+    kPhaseFrame = 4,    // one block per frame
+    kPhaseZero = 5,     // body zeroing
+    kEntropyPhases = 6
+};
+struct EntropyBatch {
+    int nframes;
+    std::uint32_t begin[kEntropyPhases][kEntropyBatchFrames + 1];
+    EntropyDev frames[kEntropyBatchFrames];
+};
+
+// Fills b.begin from b.frames[0 .. b.nframes).
+void entropy_batch_plan(EntropyBatch& b);
+
+// Enqueues every frame's entropy stage on `stream` (b planned).
+bool entropy_batch_launch(const EntropyBatch& b, void* stream);
+
 }  // namespace jxb

@@ -492,9 +492,12 @@ __device__ __forceinline__ void cfl_class(const __half* coef, const unsigned cha
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
-    frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
-    extern __shared__ __align__(16) float smem[];
+// The whole frontend of the 64x64 tile (tx, ty) of one frame; `smem` is the
+// CTA's dynamic shared memory (kSmemBytes). The caller synchronises before
+// the CTA starts another tile.
+__device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const FrontendScalars& sc,
+                                              const FrontendTables& tb, const FrontendOutputs& out, int tx,
+                                              int ty, float* smem) {
     // Region A: the XYB planes, later the selection and final-DCT row
     // scratch. Region B: the sharpened planes, later the FP16 coefficients
     // and the NV12 window before both.
@@ -510,8 +513,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int bw{W >> 3};
     const int bh{H >> 3};
     const int nblocks{bw * bh};
-    const int tx{static_cast<int>(blockIdx.x)};
-    const int ty{static_cast<int>(blockIdx.y)};
     const int px0{tx * kTile};
     const int py0{ty * kTile};
     const int bx0{tx * 8};
@@ -1362,7 +1363,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             mb = mb < -128 ? -128 : (mb > 127 ? 127 : mb);
             sm.mx = mx;
             sm.mb = mb;
-            const int tile{ty * static_cast<int>(gridDim.x) + tx};
+            const int tile{ty * ((W + kTile - 1) / kTile) + tx};
             out.ytox[tile] = static_cast<std::int8_t>(mx);
             out.ytob[tile] = static_cast<std::int8_t>(mb);
         }
@@ -1487,6 +1488,44 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         out.acs[blk] = sm.acs[lb];
         out.qf[blk] = sm.qf[lb];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
+    extern __shared__ __align__(16) float smem[];
+    frontend_tile(in, sc, tb, out, static_cast<int>(blockIdx.x), static_cast<int>(blockIdx.y), smem);
+}
+
+// Frames of a batch as one work list of tiles (frame j's tiles are items
+// tile_begin .. tile_begin + tiles - 1): resident CTAs take items until the
+// list is done, either claimed `chunk` at a time from a counter (dynamic) or
+// every gridDim-th chunk (static). The claimed item travels through the
+// Small::n32 word, which a tile writes before it reads it.
+__global__ void __launch_bounds__(kThreads, 2) frontend_batch_kernel(const __grid_constant__ FrontendBatch b) {
+    extern __shared__ __align__(16) float smem[];
+    Small& sm{*reinterpret_cast<Small*>(smem + kRegionAFloats + 3 * kSplane)};
+    const std::uint32_t chunk{static_cast<std::uint32_t>(b.chunk)};
+    for (std::uint32_t round{0};; ++round) {
+        std::uint32_t first;
+        if (b.counter != nullptr) {
+            if (threadIdx.x == 0) sm.n32 = static_cast<int>(atomicAdd(b.counter, chunk));
+            __syncthreads();
+            first = static_cast<std::uint32_t>(sm.n32);
+            __syncthreads();
+        } else {
+            first = (round * gridDim.x + blockIdx.x) * chunk;
+        }
+        if (first >= b.total_tiles) break;
+        const std::uint32_t last{min(first + chunk, b.total_tiles)};
+        for (std::uint32_t item{first}; item < last; ++item) {
+            int f{0};
+            while (f + 1 < b.nframes && b.jobs[f + 1].tile_begin <= item) ++f;
+            const FrontendJob& j{b.jobs[f]};
+            const int local{static_cast<int>(item - j.tile_begin)};
+            frontend_tile(j.in, j.sc, b.tb, j.out, local % j.tiles_x, local / j.tiles_x, smem);
+            __syncthreads();
+        }
     }
 }
 
@@ -1638,6 +1677,8 @@ bool frontend_tables_init(FrontendTables* tables) {
     tables->log2_1p = d_l2;
     tables->llf_basis = d_ob;
     return cudaFuncSetAttribute(frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(kSmemBytes)) == cudaSuccess &&
+           cudaFuncSetAttribute(frontend_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kSmemBytes)) == cudaSuccess;
 }
 
@@ -1646,6 +1687,12 @@ bool frontend_launch(const FrontendInputs& in, const FrontendScalars& s, const F
     const dim3 grid{static_cast<unsigned>((in.width + kTile - 1) / kTile),
                     static_cast<unsigned>((in.height + kTile - 1) / kTile)};
     frontend_kernel<<<grid, kThreads, kSmemBytes, static_cast<cudaStream_t>(stream)>>>(in, s, t, out);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+bool frontend_batch_launch(const FrontendBatch& b, int ctas, void* stream) {
+    if (b.nframes <= 0 || b.nframes > kBatchFrames || ctas <= 0 || b.chunk <= 0) return false;
+    frontend_batch_kernel<<<static_cast<unsigned>(ctas), kThreads, kSmemBytes, static_cast<cudaStream_t>(stream)>>>(b);
     return cudaGetLastError() == cudaSuccess;
 }
 

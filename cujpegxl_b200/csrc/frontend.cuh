@@ -79,4 +79,31 @@ FrontendScalars frontend_scalars(float distance, std::uint32_t* global_scale,
 bool frontend_launch(const FrontendInputs& in, const FrontendScalars& s, const FrontendTables& t,
                      const FrontendOutputs& out, void* stream);
 
+// Frames of one batched frontend launch (the launch's parameter block holds
+// them, so one launch takes at most kBatchFrames frames).
+constexpr int kBatchFrames = 64;
+
+struct FrontendJob {
+    FrontendInputs in;
+    FrontendScalars sc;
+    FrontendOutputs out;
+    int tiles_x;               // 64x64 tiles per row
+    std::uint32_t tile_begin;  // first work item of the frame
+};
+
+struct FrontendBatch {
+    FrontendTables tb;
+    int nframes;
+    int chunk;                   // tiles per claim
+    std::uint32_t total_tiles;
+    std::uint32_t* counter;      // claim counter, zero at launch; null: static round-robin claims
+    FrontendJob jobs[kBatchFrames];
+};
+
+// Launches `ctas` resident CTAs that run every tile of every frame in `b`.
+bool frontend_batch_launch(const FrontendBatch& b, int ctas, void* stream);
+
+// Frontend CTAs resident per SM (its launch bounds and shared memory).
+constexpr int kFrontendCtasPerSm = 2;
+
 }  // namespace jxb

@@ -178,13 +178,16 @@ cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* 
  * No reference counterpart (the reference encodes one frame per call). A batch
  * owns one encoder per frame (each frame may have its own width, height and
  * distance; all on one device). cujpegxl_b200_batch_encode enqueues the whole
- * batch as one graph launch: lanes (CUDA streams inside the graph) take the
- * frames largest first, each frame to the lane with the least work so far.
- * The first encode times graphs with 1, 2, 4 and 8 lanes and keeps the
- * fastest; later encodes with the same input addresses relaunch that graph,
- * new addresses are recaptured and the graph updated in place. The call is
- * asynchronous: cujpegxl_b200_batch_sync waits and reports every frame's size,
- * after which each file can be read on the device or copied to the host. */
+ * batch as one graph launch whose work is batched across frames: one
+ * persistent frontend launch takes the 64x64 tiles of all frames from one
+ * work list, then each entropy pass runs once for all frames (frames in
+ * groups of 64 per launch). The first encode times the candidate frontend
+ * schedules (cujpegxl_b200_batch_schedule) and keeps the fastest, and later
+ * batches of the same geometry mix reuse it; later encodes with the same
+ * input addresses relaunch that graph, new addresses are recaptured and the
+ * graph updated in place. The call is asynchronous:
+ * cujpegxl_b200_batch_sync waits and reports every frame's size, after which
+ * each file can be read on the device or copied to the host. */
 typedef struct cujpegxl_b200_batch cujpegxl_b200_batch;
 
 cujpegxl_status cujpegxl_b200_batch_create(const cujpegxl_config* frames, size_t count,
@@ -209,8 +212,25 @@ cujpegxl_status cujpegxl_b200_batch_copy(cujpegxl_b200_batch* batch, size_t inde
  * against it). */
 cujpegxl_status cujpegxl_b200_batch_stream(const cujpegxl_b200_batch* batch, uintptr_t* stream);
 
-/* Lanes the batch's graph uses (0 before the first encode). */
+/* 1 once the batch's graph exists (its work runs on one stream), else 0. */
 uint32_t cujpegxl_b200_batch_lanes(const cujpegxl_b200_batch* batch);
+
+/* The frontend schedule the batch's autotuner chose on its first encode (or
+ * took from an earlier batch of the same geometry mix): resident CTAs of the
+ * persistent frontend launch, tiles per claim, claims from a counter (1) or
+ * round-robin (0), frames largest-first (1) or in the given order (0), and
+ * the measured time of one batch with it. */
+typedef struct cujpegxl_b200_batch_schedule_info {
+    uint32_t frontend_ctas;
+    uint32_t tiles_per_claim;
+    uint32_t dynamic_claims;
+    uint32_t largest_first;
+    uint32_t from_cache;
+    uint32_t candidates;
+    float tuned_ms;
+} cujpegxl_b200_batch_schedule_info;
+cujpegxl_status cujpegxl_b200_batch_schedule(const cujpegxl_b200_batch* batch,
+                                             cujpegxl_b200_batch_schedule_info* out);
 
 void cujpegxl_b200_batch_destroy(cujpegxl_b200_batch* batch);
 

@@ -1,8 +1,11 @@
 """Batched encode (cujpegxl_b200_batch_*): frames of different sizes and
-distances in one CUDA graph launch must produce exactly the files that one
-encoder per frame produces, on the first launch (which autotunes the lane
-count), on a relaunch with the same inputs, and after the inputs move to new
-addresses (the graph is recaptured and updated in place)."""
+distances in one CUDA graph launch (one persistent frontend launch over all
+frames' tiles, one launch per entropy pass for all frames) must produce
+exactly the files that one encoder per frame produces, on the first launch
+(which autotunes the frontend schedule), on a relaunch with the same inputs,
+after the inputs move to new addresses (the graph is recaptured and updated
+in place), for a second batch of the same mix (its schedule comes from the
+cache) and for more frames than one launch takes (several groups)."""
 
 from __future__ import annotations
 
@@ -49,9 +52,38 @@ def test_batch_matches_single_encoders_across_relaunch_and_rebinding():
             assert sizes == [len(x) for x in expected]
             for i, x in enumerate(expected):
                 assert batch.read(i) == x
-        assert batch.lanes in (1, 2, 4, 8)
+        sched = batch.schedule()
+        assert batch.lanes == 1
+        assert sched["frontend_ctas"] > 0 and sched["tiles_per_claim"] in (1, 2, 4)
+        assert sched["candidates"] >= 8 and sched["tuned_ms"] > 0
     w, h, d = FRAMES[2]
     assert expected_a[2] == api.encode(nvs_a[2], w, h, d)
+    # A second batch of the same geometry mix takes the tuned schedule from
+    # the cache and gives the same files.
+    with Batch(FRAMES) as again:
+        again.encode(inputs_a)
+        assert again.sync() == [len(x) for x in expected_a]
+        assert [again.read(i) for i in range(len(FRAMES))] == expected_a
+        assert again.schedule()["from_cache"]
+
+
+def test_batch_of_more_frames_than_one_launch_takes():
+    """70 frames: two groups (64 + 6), every file equal to its lone encode."""
+    frames = [((264, 264, 1.0) if i % 2 else (512, 264, 2.0)) for i in range(70)]
+    keep, inputs, expected = [], [], []
+    for i, (w, h, d) in enumerate(frames):
+        nv = make_nv12(w, h, 500 + i)
+        k, luma, chroma, lp, cp = device_nv12(nv, w, h)
+        keep.append(k)
+        inputs.append((luma, chroma, lp, cp))
+        if i in (0, 1, 63, 64, 69):
+            expected.append((i, _single(nv, w, h, d)))
+    with Batch(frames) as batch:
+        batch.encode(inputs)
+        sizes = batch.sync()
+        for i, data in expected:
+            assert sizes[i] == len(data)
+            assert batch.read(i) == data
 
 
 def test_batch_with_learned_decisions_matches_single_encoders():
