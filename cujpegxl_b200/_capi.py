@@ -44,6 +44,7 @@ EXPORTS = (
     "cujpegxl_b200_encoder_create_ex", "cujpegxl_b200_max_output_size_ex",
     "cujpegxl_b200_debug_fail_allocation", "cujpegxl_b200_debug_live_allocations",
     "cujpegxl_b200_encoder_enqueue_readback", "cujpegxl_b200_batch_schedule",
+    "cujpegxl_b200_debug_prefix_code",
 )
 
 
@@ -117,6 +118,9 @@ def lib() -> ctypes.CDLL:
     L.cujpegxl_b200_kernels_per_encode.restype = ctypes.c_uint32
     L.cujpegxl_b200_encoder_enqueue_readback.argtypes = [E, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
     L.cujpegxl_b200_batch_schedule.argtypes = [E, P(BatchSchedule)]
+    L.cujpegxl_b200_debug_prefix_code.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                                  P(ctypes.c_uint32)]
     L.cujpegxl_b200_debug_fail_allocation.argtypes = [ctypes.c_uint32]
     L.cujpegxl_b200_debug_fail_allocation.restype = None
     L.cujpegxl_b200_debug_live_allocations.restype = ctypes.c_uint64

@@ -937,6 +937,23 @@ void cujpegxl_b200_debug_fail_allocation(uint32_t nth) { g_fail_countdown.store(
 
 uint64_t cujpegxl_b200_debug_live_allocations(void) { return g_live.load(); }
 
+cujpegxl_status cujpegxl_b200_debug_prefix_code(int32_t device_ordinal, const uint32_t* hist, uint32_t length,
+                                                uint8_t* depth, uint16_t* bits, uint8_t* header,
+                                                size_t header_cap, uint32_t* header_bits) {
+    if (hist == nullptr || depth == nullptr || bits == nullptr || header == nullptr || header_bits == nullptr ||
+        length == 0 || length > 256 || header_cap < static_cast<size_t>(jxb::kDescBytes)) {
+        return CUJPEGXL_INVALID_ARGUMENT;
+    }
+    int major{0};
+    int minor{0};
+    if (!device_exists(device_ordinal, &major, &minor)) return CUJPEGXL_NO_DEVICE;
+    DeviceScope scope{device_ordinal};
+    if (!scope.ok()) return CUJPEGXL_INTERNAL_ERROR;
+    return jxb::prefix_code_test(hist, static_cast<int>(length), depth, bits, header, header_cap, header_bits)
+               ? CUJPEGXL_OK
+               : CUJPEGXL_INTERNAL_ERROR;
+}
+
 cujpegxl_status cujpegxl_b200_encoder_set_acsnet(cujpegxl_encoder* encoder, const cujpegxl_b200_acsnet* net,
                                                  float margin, uint32_t flags) {
     if (encoder == nullptr) return CUJPEGXL_INVALID_ARGUMENT;

@@ -582,9 +582,9 @@ __device__ __forceinline__ void misc_hist_body(const EntropyDev& e, const unsign
 
 struct WarpCodeSmem {
     std::uint32_t hist[256];
-    std::uint32_t cnt[2 * 256];        // leaf counts in rank order, then internal nodes
-    std::int16_t parent[2 * 256];      // parent node of every leaf and internal node
+    std::uint32_t cnt[256];            // leaf counts in rank order (count floor 1)
     std::uint16_t leaf_sym[256];       // symbol of the leaf of each rank
+    std::uint16_t floor_sym[256];      // symbols of the clamped leaves in descending order
     std::uint8_t depth[256];
     std::uint16_t bits[256];
     std::uint16_t used[256];           // compacted list of used symbols
@@ -592,17 +592,27 @@ struct WarpCodeSmem {
     std::uint32_t len_next[18];
     alignas(4) std::uint8_t desc[kDescBytes];
     CodeLengthScratch cl;
+    // One tree per lane, lane-interleaved: internal node counts, heights and
+    // every node's parent, for the count floor 2^lane.
+    std::uint32_t icnt[256 * 32];
+    std::uint8_t height[256 * 32];
+    std::int16_t parent[512 * 32];
 };
 
-// Depths for a histogram with at least two used symbols, warp-cooperative and
-// equal to the reference's serial construction
-// (src/bitstream/prefix_code.cc:65-125): the used symbols are compacted and
-// each lane ranks its share by (clamped count ascending, symbol descending),
-// the order the reference's stable sort gives leaves pushed in descending
-// symbol order; lane 0 runs the two-queue merge (a leaf wins ties) recording
-// only each node's parent; then every lane walks its leaves to the root. The
-// whole construction repeats with the count floor doubled until no depth
-// exceeds `limit`.
+// Depths for a histogram with at least two used symbols, equal to the
+// reference's serial construction (src/bitstream/prefix_code.cc:65-125):
+// leaves ranked by (count ascending, symbol descending), two-queue merge (a
+// leaf wins ties), the whole construction repeated with the count floor
+// doubled until no depth exceeds `limit`.
+//
+// Warp-cooperative: the used symbols are compacted and ranked once. Raising
+// the floor to F only clamps the smallest counts to F - 1, so the leaves of
+// floor F are the same ranks with counts max(count, F - 1), the clamped ones
+// (count <= F - 1, a prefix of the ranks) re-ordered by descending symbol.
+// Every lane runs the merge for its own floor 2^lane at once, without
+// branches, recording parents and internal heights; the smallest floor whose
+// tree is no higher than `limit` is the one the serial loop stops at, and its
+// leaves are walked to the root.
 __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lane) {
     int n{0};
     for (int base{0}; base < length; base += 32) {
@@ -613,67 +623,76 @@ __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lan
         n += __popc(m);
     }
     __syncwarp();
-    for (std::uint32_t floor{1};; floor *= 2) {
-        for (int i{lane}; i < n; i += 32) {
-            const int sym{s.used[i]};
-            const std::uint32_t h{s.hist[sym]};
-            const std::uint32_t c{h > floor - 1 ? h : floor - 1};
-            int rank{0};
-            for (int t{0}; t < n; ++t) {
-                const int ts{s.used[t]};
-                const std::uint32_t ht{s.hist[ts]};
-                const std::uint32_t ct{ht > floor - 1 ? ht : floor - 1};
-                rank += (ct < c || (ct == c && ts > sym)) ? 1 : 0;
-            }
-            s.cnt[rank] = c;
-            s.leaf_sym[rank] = static_cast<std::uint16_t>(sym);
+    for (int i{lane}; i < n; i += 32) {
+        const int sym{s.used[i]};
+        const std::uint32_t c{s.hist[sym]};
+        int rank{0};
+        for (int t{0}; t < n; ++t) {
+            const int ts{s.used[t]};
+            const std::uint32_t ct{s.hist[ts]};
+            rank += (ct < c || (ct == c && ts > sym)) ? 1 : 0;
         }
-        __syncwarp();
-        if (lane == 0) {
-            // Leaves are cnt[0..n), internal node t is cnt[n + t]; the heads of
-            // both queues stay in registers.
-            constexpr std::uint32_t kInf{0xffffffffu};
-            int i{0};
-            int j{0};
-            std::uint32_t li{s.cnt[0]};
-            std::uint32_t lj{kInf};
-            for (int t{0}; t < n - 1; ++t) {
-                int pick[2];
-                std::uint32_t sum{0};
-#pragma unroll
-                for (int k{0}; k < 2; ++k) {
-                    if (li <= lj) {
-                        pick[k] = i;
-                        sum += li;
-                        ++i;
-                        li = i < n ? s.cnt[i] : kInf;
-                    } else {
-                        pick[k] = n + j;
-                        sum += lj;
-                        ++j;
-                        lj = j < t ? s.cnt[n + j] : kInf;
-                    }
-                }
-                s.cnt[n + t] = sum;
-                s.parent[pick[0]] = static_cast<std::int16_t>(n + t);
-                s.parent[pick[1]] = static_cast<std::int16_t>(n + t);
-                if (j == t) lj = sum;  // the internal queue was empty: its head is the new node
-            }
-        }
-        __syncwarp();
-        const int root{2 * n - 2};
-        int mx{0};
-        for (int r{lane}; r < n; r += 32) {
-            int d{0};
-            for (int v{r}; v != root; v = s.parent[v]) ++d;
-            s.depth[s.leaf_sym[r]] = static_cast<std::uint8_t>(d);
-            mx = max(mx, d);
-        }
-#pragma unroll
-        for (int off{16}; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, off));
-        __syncwarp();
-        if (mx <= limit) return;
+        s.cnt[rank] = c;
+        s.leaf_sym[rank] = static_cast<std::uint16_t>(sym);
     }
+    __syncwarp();
+    // Lane L: floor 2^L, leaf r has count max(cnt[r], 2^L - 1).
+    constexpr std::uint32_t kInf{0xffffffffu};
+    const std::uint32_t fm1{lane == 31 ? 0x7fffffffu : (1u << lane) - 1u};
+    std::uint32_t* icnt{s.icnt + lane};
+    std::uint8_t* height{s.height + lane};
+    std::int16_t* parent{s.parent + lane};
+    int i{0};
+    int j{0};
+    for (int t{0}; t < n - 1; ++t) {
+        int node[2];
+        std::uint32_t sum{0};
+        int h{0};
+#pragma unroll
+        for (int k{0}; k < 2; ++k) {
+            const std::uint32_t li{i < n ? max(s.cnt[i < n ? i : 0], fm1) : kInf};
+            const std::uint32_t lj{j < t ? icnt[32 * (j < t ? j : 0)] : kInf};
+            const bool leaf{li <= lj};
+            node[k] = leaf ? i : n + j;
+            // Saturating: only floors far above any that can fit reach it.
+            const std::uint32_t v{leaf ? li : lj};
+            sum = sum > kInf - 1u - v ? kInf - 1u : sum + v;
+            const int hk{leaf ? 0 : static_cast<int>(height[32 * (j < t ? j : 0)])};
+            h = max(h, hk);
+            i += leaf ? 1 : 0;
+            j += leaf ? 0 : 1;
+        }
+        icnt[32 * t] = sum;
+        height[32 * t] = static_cast<std::uint8_t>(h + 1);
+        parent[32 * node[0]] = static_cast<std::int16_t>(n + t);
+        parent[32 * node[1]] = static_cast<std::int16_t>(n + t);
+    }
+    const int root_h{static_cast<int>(height[32 * (n - 2)])};
+    const unsigned fit{__ballot_sync(kFull, root_h <= limit)};
+    __syncwarp();
+    const int best{__ffs(fit) - 1};  // a floor of 2^31 leaves every count equal: always fits
+    // Leaves clamped at the chosen floor, in descending symbol order.
+    const std::uint32_t bm1{best == 31 ? 0x7fffffffu : (1u << best) - 1u};
+    int m{0};
+    for (int base{0}; base < n; base += 32) {
+        const int r{base + lane};
+        m += __popc(__ballot_sync(kFull, r < n && s.cnt[r] <= bm1));
+    }
+    for (int q{lane}; q < m; q += 32) {
+        const int sym{s.leaf_sym[q]};
+        int rank{0};
+        for (int t{0}; t < m; ++t) rank += s.leaf_sym[t] > sym ? 1 : 0;
+        s.floor_sym[rank] = static_cast<std::uint16_t>(sym);
+    }
+    __syncwarp();
+    const std::int16_t* bp{s.parent + best};
+    const int root{2 * n - 2};
+    for (int r{lane}; r < n; r += 32) {
+        int d{0};
+        for (int v{r}; v != root; v = bp[32 * v]) ++d;
+        s.depth[r < m ? s.floor_sym[r] : s.leaf_sym[r]] = static_cast<std::uint8_t>(d);
+    }
+    __syncwarp();
 }
 
 // Canonical codes of depth[0..len) (canonical_codes in prefix_code.cuh),
@@ -910,6 +929,32 @@ __device__ __forceinline__ void codes_body(const EntropyDev& e, const unsigned b
         dst_depth[i] = s.depth[i];
         dst_bits[i] = s.bits[i];
     }
+}
+
+// One histogram through the device builder (test hook): `length` symbols,
+// depths, codes and the header (simple or code-length-code form) out.
+__global__ void __launch_bounds__(32) prefix_code_test_kernel(const std::uint32_t* hist, int length,
+                                                              std::uint8_t* depth, std::uint16_t* bits,
+                                                              std::uint8_t* header, std::uint32_t* nbits) {
+    extern __shared__ __align__(16) unsigned char code_smem[];
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    WarpCodeSmem& s{*reinterpret_cast<WarpCodeSmem*>(code_smem)};
+    for (int i{lane}; i < 256; i += 32) {
+        s.hist[i] = i < length ? hist[i] : 0u;
+        s.depth[i] = 0;
+        s.bits[i] = 0;
+    }
+    for (int i{lane}; i < kDescBytes; i += 32) s.desc[i] = 0;
+    __syncwarp();
+    BitSink w{s.desc, 0, kDescBytes * 8, false};
+    warp_build_and_store(s, length, w, lane);
+    __syncwarp();
+    for (int i{lane}; i < length; i += 32) {
+        depth[i] = s.depth[i];
+        bits[i] = s.bits[i];
+    }
+    for (int i{lane}; i < kDescBytes; i += 32) header[i] = s.desc[i];
+    if (lane == 0) *nbits = w.overflow ? 0xffffffffu : w.pos;
 }
 
 // ---- pass 3: bit lengths and scan ----------------------------------------------------
@@ -1714,6 +1759,32 @@ bool entropy_batch_launch(const EntropyBatch& b, void* stream) {
     ac_emit_batch_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(b);
     misc_emit_batch_kernel<<<misc, 256, 0, st>>>(b);
     return cudaGetLastError() == cudaSuccess;
+}
+
+bool prefix_code_test(const std::uint32_t* hist, int length, std::uint8_t* depth, std::uint16_t* bits,
+                      std::uint8_t* header, std::size_t header_cap, std::uint32_t* nbits) {
+    if (length < 1 || length > 256 || header_cap < static_cast<std::size_t>(kDescBytes)) return false;
+    unsigned char* dev{nullptr};
+    const std::size_t bytes{256 * 4 + 256 + 256 * 2 + kDescBytes + 4};
+    if (cudaMalloc(&dev, bytes) != cudaSuccess) return false;
+    auto* dh{reinterpret_cast<std::uint32_t*>(dev)};
+    auto* dd{dev + 1024};
+    auto* db{reinterpret_cast<std::uint16_t*>(dev + 1280)};
+    auto* dhead{dev + 1792};
+    auto* dn{reinterpret_cast<std::uint32_t*>(dev + 1792 + kDescBytes)};
+    bool ok{cudaFuncSetAttribute(prefix_code_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
+            cudaMemcpy(dh, hist, static_cast<std::size_t>(length) * 4, cudaMemcpyHostToDevice) == cudaSuccess};
+    if (ok) {
+        prefix_code_test_kernel<<<1, 32, sizeof(WarpCodeSmem)>>>(dh, length, dd, db, dhead, dn);
+        ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+             cudaMemcpy(depth, dd, static_cast<std::size_t>(length), cudaMemcpyDeviceToHost) == cudaSuccess &&
+             cudaMemcpy(bits, db, static_cast<std::size_t>(length) * 2, cudaMemcpyDeviceToHost) == cudaSuccess &&
+             cudaMemcpy(header, dhead, kDescBytes, cudaMemcpyDeviceToHost) == cudaSuccess &&
+             cudaMemcpy(nbits, dn, 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    }
+    cudaFree(dev);
+    return ok;
 }
 
 bool entropy_kernels_init() {

@@ -183,4 +183,10 @@ void entropy_batch_plan(EntropyBatch& b);
 // Enqueues every frame's entropy stage on `stream` (b planned).
 bool entropy_batch_launch(const EntropyBatch& b, void* stream);
 
+// The device prefix-code builder on one histogram of `length` (1..256)
+// symbols, synchronously on the current device (test hook): depths, codes and
+// the header (header_cap >= kDescBytes), its length in bits.
+bool prefix_code_test(const std::uint32_t* hist, int length, std::uint8_t* depth, std::uint16_t* bits,
+                      std::uint8_t* header, std::size_t header_cap, std::uint32_t* nbits);
+
 }  // namespace jxb

@@ -167,6 +167,16 @@ uint32_t cujpegxl_b200_kernels_per_encode(void);
 void cujpegxl_b200_debug_fail_allocation(uint32_t nth);
 uint64_t cujpegxl_b200_debug_live_allocations(void);
 
+/* Test hook: the device's prefix-code builder (the one every encode runs) on
+ * one histogram of `length` symbols (1..256, host memory), for comparison with
+ * the reference's build_and_store_huffman_tree (src/bitstream/prefix_code.cc):
+ * depth[length], bits[length] (bit-reversed canonical codes) and the code's
+ * header in header[header_cap >= 256], *header_bits its length in bits.
+ * Synchronous; allocates a small device buffer. */
+cujpegxl_status cujpegxl_b200_debug_prefix_code(int32_t device_ordinal, const uint32_t* hist, uint32_t length,
+                                                uint8_t* depth, uint16_t* bits, uint8_t* header,
+                                                size_t header_cap, uint32_t* header_bits);
+
 /* Device memory the encoder holds for its current geometry (one arena, all of
  * it allocated at create/configure) and its pinned host staging buffer
  * (`pinned_host_bytes` may be NULL), for admission control by callers that
