@@ -552,8 +552,9 @@ struct HistVisitor {
 };
 
 __device__ __forceinline__ void misc_hist_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
-    __shared__ std::uint32_t sh_g[4 * 256];
-    __shared__ std::uint32_t sh_fb[2];
+    extern __shared__ __align__(16) unsigned char misc_smem[];
+    std::uint32_t* sh_g{reinterpret_cast<std::uint32_t*>(misc_smem)};  // [4 * 256]
+    std::uint32_t* sh_fb{sh_g + 4 * 256};                              // [2]
     if (threadIdx.x < 2) sh_fb[threadIdx.x] = 0;
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) sh_g[i] = 0;
     const std::uint32_t first{blk * blockDim.x};
@@ -1576,8 +1577,9 @@ constexpr int kMiscWindowWords = 2048;
 // One thread per non-AC item; the bits of the block's items that share the
 // first item's section are assembled in a shared-memory window.
 __device__ __forceinline__ void misc_emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
-    __shared__ unsigned int win[kMiscWindowWords];
-    __shared__ DeferredBlob deferred[kMaxDeferred];
+    extern __shared__ __align__(16) unsigned char misc_smem[];
+    unsigned int* win{reinterpret_cast<unsigned int*>(misc_smem)};                              // [kMiscWindowWords]
+    DeferredBlob* deferred{reinterpret_cast<DeferredBlob*>(misc_smem + kMiscWindowWords * 4)};  // [kMaxDeferred]
     __shared__ unsigned long long sh_start;
     __shared__ std::uint32_t sh_end;
     __shared__ int sh_words;
@@ -1671,17 +1673,39 @@ __device__ __forceinline__ int batch_frame(const EntropyBatch& b, int phase, uns
     return lo;
 }
 
-JXB_ENTROPY_KERNELS(ac_tok, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
-JXB_ENTROPY_KERNELS(misc_hist, __launch_bounds__(256), kPhaseMisc, 0u)
+// The three item passes run the AC stripes (blocks 0 .. nstripes - 1, the
+// long ones, scheduled first) and the other items (the blocks after them) as
+// one launch: the two kinds are independent within a pass.
+__device__ __forceinline__ void tokens_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    if (blk < static_cast<unsigned>(e.nstripes)) {
+        ac_tok_body(e, blk, nblk);
+    } else {
+        misc_hist_body(e, blk - static_cast<unsigned>(e.nstripes), nblk);
+    }
+}
+__device__ __forceinline__ void lengths_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    if (blk < static_cast<unsigned>(e.nstripes)) {
+        ac_bits_body(e, blk, nblk);
+    } else {
+        misc_bits_body(e, blk - static_cast<unsigned>(e.nstripes), nblk);
+    }
+}
+__device__ __forceinline__ void emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    if (blk < static_cast<unsigned>(e.nstripes)) {
+        ac_emit_body(e, blk, nblk);
+    } else {
+        misc_emit_body(e, blk - static_cast<unsigned>(e.nstripes), nblk);
+    }
+}
+
+JXB_ENTROPY_KERNELS(tokens, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
 JXB_ENTROPY_KERNELS(codes, __launch_bounds__(32), kPhaseCodes, 0u)
-JXB_ENTROPY_KERNELS(ac_bits, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
-JXB_ENTROPY_KERNELS(misc_bits, __launch_bounds__(256), kPhaseMisc, 0u)
+JXB_ENTROPY_KERNELS(lengths, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
 JXB_ENTROPY_KERNELS(scan_tile, __launch_bounds__(1024), kPhaseScan, 0u)
 JXB_ENTROPY_KERNELS(scan_top, __launch_bounds__(1024), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(layout, __launch_bounds__(kLayoutThreads), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(zero_body, __launch_bounds__(256), kPhaseZero, kZeroBlocksBatched)
-JXB_ENTROPY_KERNELS(ac_emit, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
-JXB_ENTROPY_KERNELS(misc_emit, __launch_bounds__(256), kPhaseMisc, 0u)
+JXB_ENTROPY_KERNELS(emit, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
 #undef JXB_ENTROPY_KERNELS
 
 __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
@@ -1691,6 +1715,10 @@ __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant_
 constexpr std::size_t kHistSmem{sizeof(StripeStage) + kNumClusters * kAcSymbols * sizeof(std::uint32_t)};
 constexpr std::size_t kBitsSmem{sizeof(StripeStage)};
 constexpr std::size_t kEmitSmem{sizeof(StripeStage) + kWindowWords * sizeof(unsigned int)};
+// The other items' passes share these launches and their shared memory.
+static_assert(kHistSmem >= (4 * 256 + 2) * sizeof(std::uint32_t), "token pass shared memory");
+static_assert(kEmitSmem >= kMiscWindowWords * sizeof(unsigned int) + kMaxDeferred * sizeof(DeferredBlob),
+              "emit pass shared memory");
 
 }  // namespace
 
@@ -1709,17 +1737,14 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     const unsigned misc{(e.ac_first + 255) / 256};
     const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
-    ac_tok_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(e);
-    misc_hist_kernel<<<misc, 256, 0, st>>>(e);
+    tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
-    ac_bits_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
-    misc_bits_kernel<<<misc, 256, 0, st>>>(e);
+    lengths_kernel<<<stripes + misc, kAcThreads, kBitsSmem, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
     layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
     zero_body_kernel<<<kZeroBlocks, 256, 0, st>>>(e);
-    ac_emit_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(e);
-    misc_emit_kernel<<<misc, 256, 0, st>>>(e);
+    emit_kernel<<<stripes + misc, kAcThreads, kEmitSmem, st>>>(e);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1727,7 +1752,7 @@ void entropy_batch_plan(EntropyBatch& b) {
     for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][0] = 0;
     for (int f{0}; f < b.nframes; ++f) {
         const EntropyDev& e{b.frames[f]};
-        const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes), (e.ac_first + 255) / 256,
+        const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes) + (e.ac_first + 255) / 256,
                                                  static_cast<std::uint32_t>(kNumClusters + 2 * e.ndc), e.num_tiles,
                                                  1u, kZeroBlocksBatched};
         for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][f + 1] = b.begin[p][f] + per[p];
@@ -1744,20 +1769,16 @@ bool entropy_batch_launch(const EntropyBatch& b, void* stream) {
     }
     cudaStream_t st{static_cast<cudaStream_t>(stream)};
     const int nf{b.nframes};
-    const unsigned stripes{b.begin[kPhaseStripes][nf]};
-    const unsigned misc{b.begin[kPhaseMisc][nf]};
+    const unsigned items{b.begin[kPhaseItems][nf]};
     clear_batch_kernel<<<static_cast<unsigned>(nf), 256, 0, st>>>(b);
-    ac_tok_batch_kernel<<<stripes, kAcThreads, kHistSmem, st>>>(b);
-    misc_hist_batch_kernel<<<misc, 256, 0, st>>>(b);
+    tokens_batch_kernel<<<items, kAcThreads, kHistSmem, st>>>(b);
     codes_batch_kernel<<<b.begin[kPhaseCodes][nf], 32, sizeof(WarpCodeSmem), st>>>(b);
-    ac_bits_batch_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(b);
-    misc_bits_batch_kernel<<<misc, 256, 0, st>>>(b);
+    lengths_batch_kernel<<<items, kAcThreads, kBitsSmem, st>>>(b);
     scan_tile_batch_kernel<<<b.begin[kPhaseScan][nf], 1024, 0, st>>>(b);
     scan_top_batch_kernel<<<static_cast<unsigned>(nf), 1024, 0, st>>>(b);
     layout_batch_kernel<<<static_cast<unsigned>(nf), kLayoutThreads, layout_smem, st>>>(b);
     zero_body_batch_kernel<<<b.begin[kPhaseZero][nf], 256, 0, st>>>(b);
-    ac_emit_batch_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(b);
-    misc_emit_batch_kernel<<<misc, 256, 0, st>>>(b);
+    emit_batch_kernel<<<items, kAcThreads, kEmitSmem, st>>>(b);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1792,21 +1813,21 @@ bool entropy_kernels_init() {
                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_tok_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(tokens_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kHistSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_bits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(lengths_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kEmitSmem)) == cudaSuccess &&
            cudaFuncSetAttribute(codes_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(layout_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_tok_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(tokens_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kHistSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_bits_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(lengths_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(ac_emit_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(emit_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kEmitSmem)) == cudaSuccess;
 }
 

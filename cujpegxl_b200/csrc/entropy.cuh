@@ -6,15 +6,17 @@
 // lengths are data dependent but whose number is fixed by the frame geometry:
 // a header blob, one AC block-channel, one DC sample, one AcMetadata sample.
 // Per frame:
-//   1. histogram pass over all items (AC clusters, per-DC-group DC and
-//      AcMetadata histograms, first-block counts);
+//   1. token pass over all items: the AC stripes' tokens are counted into
+//      the 32 cluster histograms and stored once in a token pool; the other
+//      items fill the per-DC-group DC and AcMetadata histograms;
 //   2. prefix codes built on the device, one warp per histogram;
 //   3. bit-length pass over all items, then a two-level exclusive scan;
 //   4. a layout CTA sizes every section, writes the container, headers and
 //      TOC, and places the sections;
 //   5. an emit pass writes every item's bits at its final position.
-// Passes 1, 3 and 5 run as two kernels each: one warp per AC block-channel
-// (items from ac_first on) and one thread per other item.
+// Passes 1, 3 and 5 are one launch each: a CTA per AC stripe (one warp per
+// block-channel while tokenising, stored tokens afterwards), then a CTA per
+// 256 other items (one thread each).
 #pragma once
 
 #include <cstddef>
@@ -163,13 +165,12 @@ bool entropy_launch(const EntropyDev& e, void* stream);
 // begin[phase][f + 1] - 1. The frames live in the launch's parameter block.
 constexpr int kEntropyBatchFrames = 64;
 enum EntropyPhase : int {
-    kPhaseStripes = 0,  // AC stripe passes: one block per stripe
-    kPhaseMisc = 1,     // other items: 256 per block
-    kPhaseCodes = 2,    // prefix codes: one block per histogram
-    kPhaseScan = 3,     // item scan tiles
-    kPhaseFrame = 4,    // one block per frame
-    kPhaseZero = 5,     // body zeroing
-    kEntropyPhases = 6
+    kPhaseItems = 0,    // item passes: one block per AC stripe, then one per 256 other items
+    kPhaseCodes = 1,    // prefix codes: one block per histogram
+    kPhaseScan = 2,     // item scan tiles
+    kPhaseFrame = 3,    // one block per frame
+    kPhaseZero = 4,     // body zeroing
+    kEntropyPhases = 5
 };
 struct EntropyBatch {
     int nframes;
