@@ -960,6 +960,12 @@ __global__ void __launch_bounds__(32) prefix_code_test_kernel(const std::uint32_
 
 // ---- pass 3: bit lengths and scan ----------------------------------------------------
 
+// Which stripes a launch of the AC bit-length or emission pass takes: those
+// whose tokens are stored (no staging, small shared memory) or the others
+// (staged coefficients, tokenised again).
+enum StripeSet : int { kStoredStripes = 0, kUnstoredStripes = 1 };
+
+template <int kSet>
 __device__ __forceinline__ void ac_bits_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
@@ -969,6 +975,7 @@ __device__ __forceinline__ void ac_bits_body(const EntropyDev& e, const unsigned
     const Stripe st{e.stripes[blk]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
     const std::uint32_t tbase{e.stripe_tok[2 * blk]};
+    if ((tbase != kNoTokens) != (kSet == kStoredStripes)) return;
     if (tbase != kNoTokens) {
         // Stored tokens: the stripe's whole length goes on its first item
         // (the scan only needs sums at stripe and section starts).
@@ -1397,10 +1404,12 @@ __device__ void flush_window(const unsigned int* win, int nwords, unsigned int* 
 // Writes a stripe's tokens. The stripe's bits are contiguous in its section;
 // they are assembled in a shared-memory window and written out with plain
 // stores (global atomics only when the stripe exceeds the window).
+template <int kSet>
 __device__ __forceinline__ void ac_emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char ac_smem[];
     StripeStage& s{*reinterpret_cast<StripeStage*>(ac_smem)};
-    unsigned int* win{reinterpret_cast<unsigned int*>(ac_smem + sizeof(StripeStage))};
+    // Stored stripes need no staging: their window starts the allocation.
+    unsigned int* win{reinterpret_cast<unsigned int*>(ac_smem + (kSet == kStoredStripes ? 0 : sizeof(StripeStage)))};
     __shared__ unsigned long long sh_start;
     __shared__ unsigned long long sh_p0;
     __shared__ int sh_words;
@@ -1410,11 +1419,8 @@ __device__ __forceinline__ void ac_emit_body(const EntropyDev& e, const unsigned
     const Stripe st{e.stripes[blk]};
     const GroupGeom gg{ac_group_geom(e, st.group)};
     const int nitems{3 * st.rows * gg.gw};
-    if (e.stripe_tok[2 * blk] == kNoTokens) {
-        stage_stripe(e, st, gg, s);
-    } else if (tid == 0) {
-        s.nactive = 0;
-    }
+    if ((e.stripe_tok[2 * blk] != kNoTokens) != (kSet == kStoredStripes)) return;
+    if (kSet == kUnstoredStripes) stage_stripe(e, st, gg, s);
     if (tid == 0) {
         const Section sec{e.sections[st.section]};
         const unsigned long long p0{prefix_at(e, st.item0)};
@@ -1685,17 +1691,25 @@ __device__ __forceinline__ void tokens_body(const EntropyDev& e, const unsigned 
 }
 __device__ __forceinline__ void lengths_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     if (blk < static_cast<unsigned>(e.nstripes)) {
-        ac_bits_body(e, blk, nblk);
+        ac_bits_body<kStoredStripes>(e, blk, nblk);
     } else {
         misc_bits_body(e, blk - static_cast<unsigned>(e.nstripes), nblk);
     }
 }
 __device__ __forceinline__ void emit_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     if (blk < static_cast<unsigned>(e.nstripes)) {
-        ac_emit_body(e, blk, nblk);
+        ac_emit_body<kStoredStripes>(e, blk, nblk);
     } else {
         misc_emit_body(e, blk - static_cast<unsigned>(e.nstripes), nblk);
     }
+}
+// Stripes whose tokens did not fit the pool, with their coefficients staged
+// (their CTAs return at once for stored stripes).
+__device__ __forceinline__ void lengths_unstored_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    ac_bits_body<kUnstoredStripes>(e, blk, nblk);
+}
+__device__ __forceinline__ void emit_unstored_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
+    ac_emit_body<kUnstoredStripes>(e, blk, nblk);
 }
 
 JXB_ENTROPY_KERNELS(tokens, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
@@ -1706,6 +1720,8 @@ JXB_ENTROPY_KERNELS(scan_top, __launch_bounds__(1024), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(layout, __launch_bounds__(kLayoutThreads), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(zero_body, __launch_bounds__(256), kPhaseZero, kZeroBlocksBatched)
 JXB_ENTROPY_KERNELS(emit, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
+JXB_ENTROPY_KERNELS(lengths_unstored, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
+JXB_ENTROPY_KERNELS(emit_unstored, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
 #undef JXB_ENTROPY_KERNELS
 
 __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
@@ -1715,10 +1731,14 @@ __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant_
 constexpr std::size_t kHistSmem{sizeof(StripeStage) + kNumClusters * kAcSymbols * sizeof(std::uint32_t)};
 constexpr std::size_t kBitsSmem{sizeof(StripeStage)};
 constexpr std::size_t kEmitSmem{sizeof(StripeStage) + kWindowWords * sizeof(unsigned int)};
+// Emission of stored stripes and other items: the larger of their windows.
+constexpr std::size_t kEmitStoredSmem{kWindowWords * sizeof(unsigned int) >
+                                              kMiscWindowWords * sizeof(unsigned int) + kMaxDeferred * sizeof(DeferredBlob)
+                                          ? kWindowWords * sizeof(unsigned int)
+                                          : kMiscWindowWords * sizeof(unsigned int) + kMaxDeferred * sizeof(DeferredBlob)};
 // The other items' passes share these launches and their shared memory.
 static_assert(kHistSmem >= (4 * 256 + 2) * sizeof(std::uint32_t), "token pass shared memory");
-static_assert(kEmitSmem >= kMiscWindowWords * sizeof(unsigned int) + kMaxDeferred * sizeof(DeferredBlob),
-              "emit pass shared memory");
+
 
 }  // namespace
 
@@ -1739,12 +1759,14 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
     tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
-    lengths_kernel<<<stripes + misc, kAcThreads, kBitsSmem, st>>>(e);
+    lengths_kernel<<<stripes + misc, kAcThreads, 0, st>>>(e);
+    lengths_unstored_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
     layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
     zero_body_kernel<<<kZeroBlocks, 256, 0, st>>>(e);
-    emit_kernel<<<stripes + misc, kAcThreads, kEmitSmem, st>>>(e);
+    emit_kernel<<<stripes + misc, kAcThreads, kEmitStoredSmem, st>>>(e);
+    emit_unstored_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(e);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1754,7 +1776,7 @@ void entropy_batch_plan(EntropyBatch& b) {
         const EntropyDev& e{b.frames[f]};
         const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes) + (e.ac_first + 255) / 256,
                                                  static_cast<std::uint32_t>(kNumClusters + 2 * e.ndc), e.num_tiles,
-                                                 1u, kZeroBlocksBatched};
+                                                 1u, kZeroBlocksBatched, static_cast<std::uint32_t>(e.nstripes)};
         for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][f + 1] = b.begin[p][f] + per[p];
     }
 }
@@ -1773,12 +1795,14 @@ bool entropy_batch_launch(const EntropyBatch& b, void* stream) {
     clear_batch_kernel<<<static_cast<unsigned>(nf), 256, 0, st>>>(b);
     tokens_batch_kernel<<<items, kAcThreads, kHistSmem, st>>>(b);
     codes_batch_kernel<<<b.begin[kPhaseCodes][nf], 32, sizeof(WarpCodeSmem), st>>>(b);
-    lengths_batch_kernel<<<items, kAcThreads, kBitsSmem, st>>>(b);
+    lengths_batch_kernel<<<items, kAcThreads, 0, st>>>(b);
+    lengths_unstored_batch_kernel<<<b.begin[kPhaseStripes][nf], kAcThreads, kBitsSmem, st>>>(b);
     scan_tile_batch_kernel<<<b.begin[kPhaseScan][nf], 1024, 0, st>>>(b);
     scan_top_batch_kernel<<<static_cast<unsigned>(nf), 1024, 0, st>>>(b);
     layout_batch_kernel<<<static_cast<unsigned>(nf), kLayoutThreads, layout_smem, st>>>(b);
     zero_body_batch_kernel<<<b.begin[kPhaseZero][nf], 256, 0, st>>>(b);
-    emit_batch_kernel<<<items, kAcThreads, kEmitSmem, st>>>(b);
+    emit_batch_kernel<<<items, kAcThreads, kEmitStoredSmem, st>>>(b);
+    emit_unstored_batch_kernel<<<b.begin[kPhaseStripes][nf], kAcThreads, kEmitSmem, st>>>(b);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1815,9 +1839,9 @@ bool entropy_kernels_init() {
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
            cudaFuncSetAttribute(tokens_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kHistSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(lengths_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(lengths_unstored_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(emit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(emit_unstored_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kEmitSmem)) == cudaSuccess &&
            cudaFuncSetAttribute(codes_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
@@ -1825,9 +1849,9 @@ bool entropy_kernels_init() {
                                 static_cast<int>(kLayoutSmemLimit)) == cudaSuccess &&
            cudaFuncSetAttribute(tokens_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kHistSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(lengths_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(lengths_unstored_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kBitsSmem)) == cudaSuccess &&
-           cudaFuncSetAttribute(emit_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+           cudaFuncSetAttribute(emit_unstored_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kEmitSmem)) == cudaSuccess;
 }
 

@@ -16,7 +16,9 @@
 //   5. an emit pass writes every item's bits at its final position.
 // Passes 1, 3 and 5 are one launch each: a CTA per AC stripe (one warp per
 // block-channel while tokenising, stored tokens afterwards), then a CTA per
-// 256 other items (one thread each).
+// 256 other items (one thread each); passes 3 and 5 take stripes whose
+// tokens did not fit the pool in one more launch each, with their
+// coefficients staged again.
 #pragma once
 
 #include <cstddef>
@@ -170,7 +172,8 @@ enum EntropyPhase : int {
     kPhaseScan = 2,     // item scan tiles
     kPhaseFrame = 3,    // one block per frame
     kPhaseZero = 4,     // body zeroing
-    kEntropyPhases = 5
+    kPhaseStripes = 5,  // AC stripes whose tokens did not fit the pool
+    kEntropyPhases = 6
 };
 struct EntropyBatch {
     int nframes;

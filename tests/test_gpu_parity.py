@@ -128,3 +128,13 @@ def test_host_input_path_matches_device_path():
         a = enc.encode_device(luma, chroma, lp, cp)
         b = enc.encode_host(nv)
     assert a == b
+
+
+def test_token_pool_overflow_falls_back_bit_exact():
+    """At distance 0.05 a 520x392 frame needs about 65 AC tokens per block,
+    twice what the token pool holds: the stripes that find the pool full are
+    tokenised again from their coefficients, and the file is still the
+    restatement's, byte for byte."""
+    w, h, d = 520, 392, 0.05
+    nv, data, g = _frontend_and_file(w, h, d, 2)
+    assert data == api.encode(nv, w, h, d)
