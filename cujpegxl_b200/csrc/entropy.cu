@@ -551,21 +551,28 @@ struct HistVisitor {
     }
 };
 
+// Other items per CTA of the item passes (256 threads, two items each).
+constexpr std::uint32_t kMiscItemsPerBlock = 512;
+constexpr int kMiscPerThread = 2;
+
 __device__ __forceinline__ void misc_hist_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
     extern __shared__ __align__(16) unsigned char misc_smem[];
     std::uint32_t* sh_g{reinterpret_cast<std::uint32_t*>(misc_smem)};  // [4 * 256]
     std::uint32_t* sh_fb{sh_g + 4 * 256};                              // [2]
     if (threadIdx.x < 2) sh_fb[threadIdx.x] = 0;
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) sh_g[i] = 0;
-    const std::uint32_t first{blk * blockDim.x};
-    const std::uint32_t last{min(first + blockDim.x, e.ac_first) - 1};
+    const std::uint32_t first{blk * kMiscItemsPerBlock};
+    const std::uint32_t last{min(first + kMiscItemsPerBlock, e.ac_first) - 1};
     const Section s0{e.sections[find_section(e.sections, 0, misc_hi(e), first)]};
     const Section s1{e.sections[find_section(e.sections, 0, misc_hi(e), last)]};
     HistVisitor v{sh_g, sh_fb, s0.kind == kSecDcGroup ? s0.group : -1,
                   s1.kind == kSecDcGroup && s1.group != s0.group ? s1.group : -2, &e};
     __syncthreads();
-    const std::uint32_t item{first + threadIdx.x};
-    if (item < e.ac_first) visit_misc(e, item, v);
+#pragma unroll
+    for (int k{0}; k < kMiscPerThread; ++k) {
+        const std::uint32_t item{first + threadIdx.x + k * blockDim.x};
+        if (item < e.ac_first) visit_misc(e, item, v);
+    }
     __syncthreads();
     for (int i{static_cast<int>(threadIdx.x)}; i < 4 * 256; i += blockDim.x) {
         const int slot{i >> 9};
@@ -614,23 +621,33 @@ struct WarpCodeSmem {
 // branches, recording parents and internal heights; the smallest floor whose
 // tree is no higher than `limit` is the one the serial loop stops at, and its
 // leaves are walked to the root.
-__device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lane) {
+//
+// hist[0..length) is read, depth[] of the used symbols written (the caller
+// zeroes the rest); the rest of `s` other than hist and depth is scratch. A
+// single used symbol gets depth 1, as the serial builder gives it.
+__device__ void warp_create_tree(WarpCodeSmem& s, const std::uint32_t* hist, int length, int limit,
+                                 std::uint8_t* depth, int lane) {
     int n{0};
     for (int base{0}; base < length; base += 32) {
         const int sym{base + lane};
-        const bool used{sym < length && s.hist[sym] != 0};
+        const bool used{sym < length && hist[sym] != 0};
         const unsigned m{__ballot_sync(kFull, used)};
         if (used) s.used[n + __popc(m & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(sym);
         n += __popc(m);
     }
     __syncwarp();
+    if (n < 2) {
+        if (n == 1 && lane == 0) depth[s.used[0]] = 1;
+        __syncwarp();
+        return;
+    }
     for (int i{lane}; i < n; i += 32) {
         const int sym{s.used[i]};
-        const std::uint32_t c{s.hist[sym]};
+        const std::uint32_t c{hist[sym]};
         int rank{0};
         for (int t{0}; t < n; ++t) {
             const int ts{s.used[t]};
-            const std::uint32_t ct{s.hist[ts]};
+            const std::uint32_t ct{hist[ts]};
             rank += (ct < c || (ct == c && ts > sym)) ? 1 : 0;
         }
         s.cnt[rank] = c;
@@ -691,19 +708,20 @@ __device__ void warp_create_tree(WarpCodeSmem& s, int length, int limit, int lan
     for (int r{lane}; r < n; r += 32) {
         int d{0};
         for (int v{r}; v != root; v = bp[32 * v]) ++d;
-        s.depth[r < m ? s.floor_sym[r] : s.leaf_sym[r]] = static_cast<std::uint8_t>(d);
+        depth[r < m ? s.floor_sym[r] : s.leaf_sym[r]] = static_cast<std::uint8_t>(d);
     }
     __syncwarp();
 }
 
 // Canonical codes of depth[0..len) (canonical_codes in prefix_code.cuh),
 // warp-cooperative: codes of equal length are handed out in symbol order.
-__device__ void warp_canonical_codes(WarpCodeSmem& s, int len, int lane) {
+__device__ void warp_canonical_codes(WarpCodeSmem& s, const std::uint8_t* depth, int len, std::uint16_t* bits,
+                                     int lane) {
     if (lane < 18) s.len_count[lane] = 0;
     __syncwarp();
     for (int base{0}; base < len; base += 32) {
         const int sym{base + lane};
-        const int d{sym < len ? s.depth[sym] : 0};
+        const int d{sym < len ? depth[sym] : 0};
         const unsigned peers{__match_any_sync(kFull, d)};
         if (d != 0 && (__ffs(peers) - 1) == lane) s.len_count[d] += static_cast<std::uint32_t>(__popc(peers));
     }
@@ -720,12 +738,12 @@ __device__ void warp_canonical_codes(WarpCodeSmem& s, int len, int lane) {
     const unsigned below{(1u << lane) - 1u};
     for (int base{0}; base < len; base += 32) {
         const int sym{base + lane};
-        const int d{sym < len ? s.depth[sym] : 0};
+        const int d{sym < len ? depth[sym] : 0};
         const unsigned peers{__match_any_sync(kFull, d)};
         const std::uint32_t code{d != 0 ? s.len_next[d] + static_cast<std::uint32_t>(__popc(peers & below)) : 0u};
         __syncwarp();
         if (d != 0 && (__ffs(peers) - 1) == lane) s.len_next[d] += static_cast<std::uint32_t>(__popc(peers));
-        if (sym < len) s.bits[sym] = d != 0 ? static_cast<std::uint16_t>(__brev(code) >> (32 - d)) : 0;
+        if (sym < len) bits[sym] = d != 0 ? static_cast<std::uint16_t>(__brev(code) >> (32 - d)) : 0;
         __syncwarp();
     }
 }
@@ -763,6 +781,15 @@ __device__ void warp_store_complex(WarpCodeSmem& s, int num, BitSink& w, int lan
         if (d >= 0 && (__ffs(peers) - 1) == lane) scr.hist[d] += static_cast<std::uint32_t>(__popc(peers));
     }
     __syncwarp();
+    // The code-length code: the same construction (limit 5) and canonical
+    // codes, across the warp.
+    if (lane < 18) {
+        scr.cl_depth[lane] = 0;
+        scr.cl_bits[lane] = 0;
+    }
+    __syncwarp();
+    warp_create_tree(s, scr.hist, 18, 5, scr.cl_depth, lane);
+    warp_canonical_codes(s, scr.cl_depth, 18, scr.cl_bits, lane);
     std::uint32_t pos{0};
     if (lane == 0) {
         std::uint32_t* hist{scr.hist};
@@ -780,13 +807,6 @@ __device__ void warp_store_complex(WarpCodeSmem& s, int num, BitSink& w, int lan
             }
         }
         std::uint8_t* cl_depth{scr.cl_depth};
-        std::uint16_t* cl_bits{scr.cl_bits};
-        for (int i{0}; i < 18; ++i) {
-            cl_depth[i] = 0;
-            cl_bits[i] = 0;
-        }
-        create_tree_serial(hist, 18, 5, cl_depth, scr.pool, scr.level);
-        canonical_codes(cl_depth, 18, cl_bits);
         constexpr std::uint8_t kOrder[18]{1, 2, 3, 4, 0, 5, 17, 6, 16, 7, 8, 9, 10, 11, 12, 13, 14, 15};
         constexpr std::uint8_t kSym[6]{0, 7, 3, 2, 1, 15};
         constexpr std::uint8_t kLen[6]{2, 4, 3, 2, 2, 4};
@@ -849,8 +869,8 @@ __device__ void warp_build_and_store(WarpCodeSmem& s, int length, BitSink& w, in
         __syncwarp();
         return;
     }
-    warp_create_tree(s, length, 15, lane);
-    warp_canonical_codes(s, length, lane);
+    warp_create_tree(s, s.hist, length, 15, s.depth, lane);
+    warp_canonical_codes(s, s.depth, length, s.bits, lane);
     if (count <= 4) {
         if (lane == 0) store_code_header(count, s4, length, s.depth, w, s.cl);
         __syncwarp();
@@ -897,12 +917,17 @@ __device__ __forceinline__ void codes_body(const EntropyDev& e, const unsigned b
         }
         clustered = false;
     }
-    for (int i{lane}; i < 256; i += 32) {
-        s.hist[i] = src[i] + (i == 0 ? extra0 : 0u);
+    std::uint32_t hv[8];
+#pragma unroll
+    for (int k{0}; k < 8; ++k) hv[k] = src[lane + 32 * k];  // all eight loads in flight at once
+#pragma unroll
+    for (int k{0}; k < 8; ++k) {
+        const int i{lane + 32 * k};
+        s.hist[i] = hv[k] + (i == 0 ? extra0 : 0u);
         s.depth[i] = 0;
         s.bits[i] = 0;
     }
-    for (int i{lane}; i < kDescBytes; i += 32) s.desc[i] = 0;
+    for (int i{lane}; i < kDescBytes / 4; i += 32) reinterpret_cast<std::uint32_t*>(s.desc)[i] = 0;
     __syncwarp();
     int alpha{1};
     for (int i{lane}; i < 256; i += 32) {
@@ -1047,11 +1072,14 @@ struct BitsVisitor {
 };
 
 __device__ __forceinline__ void misc_bits_body(const EntropyDev& e, const unsigned blk, const unsigned nblk) {
-    const std::uint32_t item{blk * blockDim.x + threadIdx.x};
-    if (item >= e.ac_first) return;
-    BitsVisitor v{&e, 0};
-    visit_misc(e, item, v);
-    e.item_bits[item] = v.total;
+#pragma unroll
+    for (int k{0}; k < kMiscPerThread; ++k) {
+        const std::uint32_t item{blk * kMiscItemsPerBlock + threadIdx.x + k * blockDim.x};
+        if (item >= e.ac_first) return;
+        BitsVisitor v{&e, 0};
+        visit_misc(e, item, v);
+        e.item_bits[item] = v.total;
+    }
 }
 
 // Exclusive scan of item_bits inside tiles of kScanTile items (1024 threads x 4).
@@ -1591,13 +1619,12 @@ __device__ __forceinline__ void misc_emit_body(const EntropyDev& e, const unsign
     __shared__ int sh_words;
     __shared__ int sh_ndeferred;
     if (e.result[2] != 0) return;
-    const std::uint32_t first{blk * blockDim.x};
-    const std::uint32_t item{first + threadIdx.x};
+    const std::uint32_t first{blk * kMiscItemsPerBlock};
     if (threadIdx.x == 0) {
         sh_ndeferred = 0;
         const int s0{find_section(e.sections, 0, misc_hi(e), first)};
         const Section sec{e.sections[s0]};
-        const std::uint32_t end{min(min(first + blockDim.x, sec.first + sec.count), e.ac_first)};
+        const std::uint32_t end{min(min(first + kMiscItemsPerBlock, sec.first + sec.count), e.ac_first)};
         const unsigned long long p0{prefix_at(e, first)};
         const unsigned long long start{e.sec_pos[s0] + (p0 - prefix_at(e, sec.first))};
         const unsigned long long bits{prefix_at(e, end) - p0};
@@ -1610,14 +1637,18 @@ __device__ __forceinline__ void misc_emit_body(const EntropyDev& e, const unsign
     const int nwords{sh_words};
     for (int i{static_cast<int>(threadIdx.x)}; i < nwords; i += blockDim.x) win[i] = 0;
     __syncthreads();
-    if (item < e.ac_first) {
-        const int s{find_section(e.sections, 0, misc_hi(e), item)};
-        const Section sec{e.sections[s]};
-        const unsigned long long pos{e.sec_pos[s] + (prefix_at(e, item) - prefix_at(e, sec.first))};
-        const bool in_window{nwords >= 0 && item < sh_end};
-        EmitVisitor v{&e, in_window ? win : reinterpret_cast<unsigned int*>(e.out),
-                      in_window ? pos - ((sh_start >> 5) << 5) : pos, deferred, &sh_ndeferred};
-        visit_misc(e, item, v);
+#pragma unroll
+    for (int k{0}; k < kMiscPerThread; ++k) {
+        const std::uint32_t item{first + threadIdx.x + k * blockDim.x};
+        if (item < e.ac_first) {
+            const int s{find_section(e.sections, 0, misc_hi(e), item)};
+            const Section sec{e.sections[s]};
+            const unsigned long long pos{e.sec_pos[s] + (prefix_at(e, item) - prefix_at(e, sec.first))};
+            const bool in_window{nwords >= 0 && item < sh_end};
+            EmitVisitor v{&e, in_window ? win : reinterpret_cast<unsigned int*>(e.out),
+                          in_window ? pos - ((sh_start >> 5) << 5) : pos, deferred, &sh_ndeferred};
+            visit_misc(e, item, v);
+        }
     }
     __syncthreads();
     // Long blobs, one 32-bit word of each per thread.
@@ -1754,7 +1785,7 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
         cudaMemsetAsync(e.tok_count, 0, sizeof(std::uint32_t), st) != cudaSuccess) {
         return false;
     }
-    const unsigned misc{(e.ac_first + 255) / 256};
+    const unsigned misc{(e.ac_first + kMiscItemsPerBlock - 1) / kMiscItemsPerBlock};
     const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
     tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
@@ -1774,7 +1805,8 @@ void entropy_batch_plan(EntropyBatch& b) {
     for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][0] = 0;
     for (int f{0}; f < b.nframes; ++f) {
         const EntropyDev& e{b.frames[f]};
-        const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes) + (e.ac_first + 255) / 256,
+        const std::uint32_t per[kEntropyPhases]{static_cast<std::uint32_t>(e.nstripes) +
+                                                     (e.ac_first + kMiscItemsPerBlock - 1) / kMiscItemsPerBlock,
                                                  static_cast<std::uint32_t>(kNumClusters + 2 * e.ndc), e.num_tiles,
                                                  1u, kZeroBlocksBatched, static_cast<std::uint32_t>(e.nstripes)};
         for (int p{0}; p < kEntropyPhases; ++p) b.begin[p][f + 1] = b.begin[p][f] + per[p];
