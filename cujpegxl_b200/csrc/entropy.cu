@@ -1751,8 +1751,32 @@ JXB_ENTROPY_KERNELS(scan_top, __launch_bounds__(1024), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(layout, __launch_bounds__(kLayoutThreads), kPhaseFrame, 0u)
 JXB_ENTROPY_KERNELS(zero_body, __launch_bounds__(256), kPhaseZero, kZeroBlocksBatched)
 JXB_ENTROPY_KERNELS(emit, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
-JXB_ENTROPY_KERNELS(lengths_unstored, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
-JXB_ENTROPY_KERNELS(emit_unstored, __launch_bounds__(kAcThreads), kPhaseStripes, 0u)
+// Stripes whose tokens did not fit the pool are rare, so their passes run on
+// a few resident CTAs that skip the stored stripes with one load each.
+constexpr unsigned kUnstoredCtas = 148;
+
+#define JXB_UNSTORED_KERNELS(NAME)                                                                         \
+    __global__ void __launch_bounds__(kAcThreads) NAME##_kernel(const __grid_constant__ EntropyDev e) {       \
+        for (unsigned s{blockIdx.x}; s < static_cast<unsigned>(e.nstripes); s += gridDim.x) {                 \
+            if (e.stripe_tok[2 * s] != kNoTokens) continue;                                                   \
+            NAME##_body(e, s, 0u);                                                                            \
+            __syncthreads();                                                                                  \
+        }                                                                                                     \
+    }                                                                                                         \
+    __global__ void __launch_bounds__(kAcThreads) NAME##_batch_kernel(const __grid_constant__ EntropyBatch b) { \
+        const unsigned total{b.begin[kPhaseStripes][b.nframes]};                                              \
+        for (unsigned i{blockIdx.x}; i < total; i += gridDim.x) {                                             \
+            const int f{batch_frame(b, kPhaseStripes, i)};                                                    \
+            const unsigned s{i - b.begin[kPhaseStripes][f]};                                                  \
+            if (b.frames[f].stripe_tok[2 * s] != kNoTokens) continue;                                         \
+            NAME##_body(b.frames[f], s, 0u);                                                                  \
+            __syncthreads();                                                                                  \
+        }                                                                                                     \
+    }
+
+JXB_UNSTORED_KERNELS(lengths_unstored)
+JXB_UNSTORED_KERNELS(emit_unstored)
+#undef JXB_UNSTORED_KERNELS
 #undef JXB_ENTROPY_KERNELS
 
 __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
@@ -1791,13 +1815,13 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
     lengths_kernel<<<stripes + misc, kAcThreads, 0, st>>>(e);
-    lengths_unstored_kernel<<<stripes, kAcThreads, kBitsSmem, st>>>(e);
+    lengths_unstored_kernel<<<kUnstoredCtas, kAcThreads, kBitsSmem, st>>>(e);
     scan_tile_kernel<<<e.num_tiles, 1024, 0, st>>>(e);
     scan_top_kernel<<<1, 1024, 0, st>>>(e);
     layout_kernel<<<1, kLayoutThreads, layout_smem, st>>>(e);
     zero_body_kernel<<<kZeroBlocks, 256, 0, st>>>(e);
     emit_kernel<<<stripes + misc, kAcThreads, kEmitStoredSmem, st>>>(e);
-    emit_unstored_kernel<<<stripes, kAcThreads, kEmitSmem, st>>>(e);
+    emit_unstored_kernel<<<kUnstoredCtas, kAcThreads, kEmitSmem, st>>>(e);
     return cudaGetLastError() == cudaSuccess;
 }
 
@@ -1828,13 +1852,13 @@ bool entropy_batch_launch(const EntropyBatch& b, void* stream) {
     tokens_batch_kernel<<<items, kAcThreads, kHistSmem, st>>>(b);
     codes_batch_kernel<<<b.begin[kPhaseCodes][nf], 32, sizeof(WarpCodeSmem), st>>>(b);
     lengths_batch_kernel<<<items, kAcThreads, 0, st>>>(b);
-    lengths_unstored_batch_kernel<<<b.begin[kPhaseStripes][nf], kAcThreads, kBitsSmem, st>>>(b);
+    lengths_unstored_batch_kernel<<<kUnstoredCtas, kAcThreads, kBitsSmem, st>>>(b);
     scan_tile_batch_kernel<<<b.begin[kPhaseScan][nf], 1024, 0, st>>>(b);
     scan_top_batch_kernel<<<static_cast<unsigned>(nf), 1024, 0, st>>>(b);
     layout_batch_kernel<<<static_cast<unsigned>(nf), kLayoutThreads, layout_smem, st>>>(b);
     zero_body_batch_kernel<<<b.begin[kPhaseZero][nf], 256, 0, st>>>(b);
     emit_batch_kernel<<<items, kAcThreads, kEmitStoredSmem, st>>>(b);
-    emit_unstored_batch_kernel<<<b.begin[kPhaseStripes][nf], kAcThreads, kEmitSmem, st>>>(b);
+    emit_unstored_batch_kernel<<<kUnstoredCtas, kAcThreads, kEmitSmem, st>>>(b);
     return cudaGetLastError() == cudaSuccess;
 }
 
