@@ -383,56 +383,45 @@ __device__ __forceinline__ void dct_col(const float* rows_fx, __half* coef, int 
     }
 }
 
-// One CfL sum of a side-N first block lb over its non-LLF coefficients in raw
-// order, as the reference accumulates it (src/frontend_quantize.cu:63-74):
-// kWhich 0 sums x*y, 1 sums y*y and 2 sums (b - y)*y, each an FMA chain of
-// float(a) * float(y) + acc (kinds 0 and 1 on the FP16 operands directly). The
-// chain is sequential; its loads are issued ahead in groups of 16 slots. An
-// LLF slot contributes fma(0, y, acc) instead of being skipped: that adds an
-// exact zero, which can change only the sign of a zero sum, and the quantised
-// CfL maps do not see that sign. Only the first covered block (two for DCT32)
-// holds LLF slots: the first N/8 columns of its first rows.
+// One CfL sum of a side-N first block lb over its non-LLF coefficients
+// (src/frontend_quantize.cu:49-74 sums them in raw order in one chain), here
+// across a warp: lane l accumulates raw positions l, l + 32, l + 64, ... in
+// that order, then the 32 partial sums meet in an xor-butterfly tree (the same
+// total on every lane). kWhich 0 sums x*y, 1 sums y*y and 2 sums (b - y)*y,
+// each product an FMA of the widened FP16 operands into the lane's partial. An
+// LLF position contributes fma(0, y, acc): it adds an exact zero.
 template <int N, int kWhich>
-__device__ __forceinline__ float cfl_sum(const __half* coef, int lb) {
+__device__ __forceinline__ float cfl_sum_warp(const __half* coef, int lb, int lane) {
     constexpr int kSide{N / 8};
-    constexpr int kQLlf{kSide == 4 ? 2 : 1};
-    constexpr std::uint64_t kLlf{N == 8 ? 0x1ull : (N == 16 ? 0x30003ull : 0xF0000000Full)};
     float acc{0.0f};
-#pragma unroll 1
-    for (int q{0}; q < kSide * kSide; ++q) {
+#pragma unroll
+    for (int k{0}; k < N * N / 32; ++k) {
+        const int raw{lane + 32 * k};
+        const int q{raw >> 6};
         const int l{lb + (q / kSide) * 8 + q % kSide};
-        const std::uint32_t* py{reinterpret_cast<const std::uint32_t*>(coef + kCoefStride + l * kCoefBlock)};
-        const std::uint32_t* po{reinterpret_cast<const std::uint32_t*>(coef + (kWhich == 2 ? 2 * kCoefStride : 0) +
-                                                                       l * kCoefBlock)};
-        const std::uint64_t skip{q < kQLlf ? kLlf : 0ull};
-#pragma unroll
-        for (int c{0}; c < 4; ++c) {
-            std::uint32_t y[8];
-            std::uint32_t o[8];
-#pragma unroll
-            for (int j{0}; j < 8; ++j) {
-                y[j] = py[c * 8 + j];
-                if (kWhich != 1) o[j] = po[c * 8 + j];
-            }
-#pragma unroll
-            for (int j{0}; j < 16; ++j) {
-                const int sh{(j & 1) * 16};
-                const auto yh{static_cast<unsigned short>(y[j >> 1] >> sh)};
-                const bool llf{((kLlf >> (16 * c + j)) & 1ull) != 0 && ((skip >> (16 * c + j)) & 1ull) != 0};
-                if (kWhich == 2) {
-                    const float yr{__half2float(__ushort_as_half(yh))};
-                    float a{add_f16(static_cast<unsigned short>(o[j >> 1] >> sh), -yr)};
-                    if (((kLlf >> (16 * c + j)) & 1ull) != 0) a = llf ? 0.0f : a;
-                    acc = jx_fma(a, yr, acc);
-                } else {
-                    auto ah{kWhich == 0 ? static_cast<unsigned short>(o[j >> 1] >> sh) : yh};
-                    if (((kLlf >> (16 * c + j)) & 1ull) != 0) ah = llf ? static_cast<unsigned short>(0) : ah;
-                    acc = fma_f16(ah, yh, acc);
-                }
-            }
+        const int at{l * kCoefBlock + (raw & 63)};
+        const bool llf{(raw / N) < kSide && (raw % N) < kSide};
+        const auto yh{__half_as_ushort(coef[kCoefStride + at])};
+        if (kWhich == 2) {
+            const float yr{__half2float(__ushort_as_half(yh))};
+            float a{add_f16(__half_as_ushort(coef[2 * kCoefStride + at]), -yr)};
+            a = llf ? 0.0f : a;
+            acc = jx_fma(a, yr, acc);
+        } else {
+            auto ah{kWhich == 0 ? __half_as_ushort(coef[at]) : yh};
+            ah = llf ? static_cast<unsigned short>(0) : ah;
+            acc = fma_f16(ah, yh, acc);
         }
     }
+#pragma unroll
+    for (int off{16}; off > 0; off >>= 1) acc = acc + __shfl_xor_sync(0xffffffffu, acc, off);
     return acc;
+}
+
+template <int N>
+__device__ __forceinline__ float cfl_sum_kind(const __half* coef, int lb, int which, int lane) {
+    return which == 0 ? cfl_sum_warp<N, 0>(coef, lb, lane)
+                      : (which == 1 ? cfl_sum_warp<N, 1>(coef, lb, lane) : cfl_sum_warp<N, 2>(coef, lb, lane));
 }
 
 // DC of the 8x8 position (ox, oy) of a first block f of side 8M from its
@@ -477,18 +466,6 @@ __device__ __forceinline__ void llf_to_dc(const __half* coef, int f, int ox, int
             }
         }
         dcv[c] = static_cast<float>(static_cast<double>(M) * sum);
-    }
-}
-
-// The three sums of every first block of side N, sum kind `which` per warp
-// and one first block per lane (list entries first..first+count-1).
-template <int N>
-__device__ __forceinline__ void cfl_class(const __half* coef, const unsigned char* list, int first, int count,
-                                          int which, int lane, float (*cfl)[64]) {
-    for (int i{lane}; i < count; i += 32) {
-        const int lb{list[first + i]};
-        cfl[which][lb] = which == 0 ? cfl_sum<N, 0>(coef, lb)
-                                    : (which == 1 ? cfl_sum<N, 1>(coef, lb) : cfl_sum<N, 2>(coef, lb));
     }
 }
 
@@ -1300,18 +1277,20 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
 
     // ---- 6. chroma from luma over the tile (src/frontend_quantize.cu:49-117),
     // and DC from the low-frequency corners (src/frontend_quantize.cu:180-200,
-    // src/vardct_layout.h:88-111), which needs no CfL result. Warps 0-5: one
-    // of the three per-block CfL sums per thread, each accumulated in raw
-    // order as the reference does. Warps 6-7: one 8x8 DC position per thread.
+    // src/vardct_layout.h:88-111), which needs no CfL result. Warps 0-5 take
+    // the (first block, sum kind) pairs round-robin, the largest transforms
+    // first, each sum across the warp (cfl_sum_warp). Warps 6-7: one 8x8 DC
+    // position per thread.
     if (tid < 192) {
-        // Warps 0-2 take the long DCT32 chains, one sum kind each and one
-        // first block per lane; warps 3-5 the DCT16 and then the DCT8 chains
-        // the same way. Every warp's chains have one length.
-        if (warp < 3) {
-            cfl_class<32>(coef, sm.fb_list, 0, sm.n32, warp, lane, sm.cfl);
-        } else {
-            cfl_class<16>(coef, sm.fb_list, sm.n32, sm.n16, warp - 3, lane, sm.cfl);
-            cfl_class<8>(coef, sm.fb_list, sm.n32 + sm.n16, sm.n8, warp - 3, lane, sm.cfl);
+        const int nfb{sm.n32 + sm.n16 + sm.n8};
+        for (int t{warp}; t < 3 * nfb; t += 6) {
+            const int i{t / 3};
+            const int which{t - 3 * i};
+            const int lb{sm.fb_list[i]};
+            const float v{i < sm.n32 ? cfl_sum_kind<32>(coef, lb, which, lane)
+                                     : (i < sm.n32 + sm.n16 ? cfl_sum_kind<16>(coef, lb, which, lane)
+                                                            : cfl_sum_kind<8>(coef, lb, which, lane))};
+            if (lane == 0) sm.cfl[which][lb] = v;
         }
     } else if (tid >= 192) {
         const int p{tid - 192};

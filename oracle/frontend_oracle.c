@@ -694,25 +694,43 @@ static void process_tile(const OracleFrame* in, const OracleScalars* sc, const O
                        &T->coef[c][lb * 64], 64 * sizeof(uint16_t));
             }
 
-    /* 6. chroma from luma. */
+    /* 6. chroma from luma. Per first block, the three sums of
+     * src/frontend_quantize.cu:49-74 (x*y, y*y, (b - y)*y over the non-LLF
+     * coefficients) in 32 partial FMA chains, chain l over raw positions
+     * l, l + 32, ... in order (an LLF position adds fma(0, y, acc)), then an
+     * xor-butterfly tree over the 32 partials; the per-tile tree as the
+     * reference's. */
     float part[3][64];
     for (int lb = 0; lb < 64; ++lb) {
-        float sxy = 0.0f, syy = 0.0f, sby = 0.0f;
+        float sums3[3] = {0.0f, 0.0f, 0.0f};
         if (bx0 + (lb & 7) < bw && by0 + (lb >> 3) < bh && T->acs[lb] != 0) {
             const int n = T->acs[lb], side = n >> 3;
-            for (int raw = 0; raw < n * n; ++raw) {
-                if ((raw / n) < side && (raw % n) < side) continue;
-                const int q = raw >> 6;
-                const int idx = (lb + (q / side) * 8 + q % side) * 64 + (raw & 63);
-                const float xr = oracle_h2f(T->coef[0][idx]);
-                const float yr = oracle_h2f(T->coef[1][idx]);
-                const float br = oracle_h2f(T->coef[2][idx]);
-                sxy = fmaf(xr, yr, sxy);
-                syy = fmaf(yr, yr, syy);
-                sby = fmaf(br - yr, yr, sby);
+            float p[3][32];
+            for (int l = 0; l < 32; ++l) {
+                float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+                for (int raw = l; raw < n * n; raw += 32) {
+                    const int llf = (raw / n) < side && (raw % n) < side;
+                    const int q = raw >> 6;
+                    const int idx = (lb + (q / side) * 8 + q % side) * 64 + (raw & 63);
+                    const float xr = oracle_h2f(T->coef[0][idx]);
+                    const float yr = oracle_h2f(T->coef[1][idx]);
+                    const float br = oracle_h2f(T->coef[2][idx]);
+                    a0 = fmaf(llf ? 0.0f : xr, yr, a0);
+                    a1 = fmaf(llf ? 0.0f : yr, yr, a1);
+                    a2 = fmaf(llf ? 0.0f : br - yr, yr, a2);
+                }
+                p[0][l] = a0; p[1][l] = a1; p[2][l] = a2;
+            }
+            for (int k = 0; k < 3; ++k) {
+                for (int off = 16; off > 0; off >>= 1) {
+                    float nx[32];
+                    for (int l = 0; l < 32; ++l) nx[l] = p[k][l] + p[k][l ^ off];
+                    memcpy(p[k], nx, sizeof(nx));
+                }
+                sums3[k] = p[k][0];
             }
         }
-        part[0][lb] = sxy; part[1][lb] = syy; part[2][lb] = sby;
+        part[0][lb] = sums3[0]; part[1][lb] = sums3[1]; part[2][lb] = sums3[2];
     }
     float sums[3];
     for (int k = 0; k < 3; ++k) {

@@ -13,7 +13,11 @@ restatement's code:
   on the restatement's own FP16 coefficients must give its integers exactly
   (the exact-rint check of tests/quant_selfconsistency_test.py:126-179), and
   every AC and DC value must reconstruct within half a quantisation step (the
-  bound of src/frontend_quantize_gpu_test.cc:142-246).
+  bound of src/frontend_quantize_gpu_test.cc:142-246);
+* the CfL maps: the per-block sums in the reference's single chain per block
+  (src/frontend_quantize.cu:49-74) and its 64-entry tile tree, quantised as
+  src/cfl.h:58-77, against the maps of the restatement's 32-chain warp sums;
+  equal except next to a rounding boundary.
 
 The CUDA path equals the restatement bit for bit (tests/test_gpu_parity.py),
 so these pins hold for it too.
@@ -280,3 +284,71 @@ def test_quantiser_exact_rint_and_half_step(frame):
                     assert abs(r.dc[blk] / q[0] - dcv[0, p]) <= 0.5 / q[0] + 1e-3
                     assert abs(r.dc[2 * nb + blk] / q[2] + y_dc - dcv[2, p]) <= 0.5 / q[2] + 1e-3
     assert checked > 1000
+
+
+# ---- chroma-from-luma maps --------------------------------------------------------------
+
+def _ref_order_sums(coef: np.ndarray, acs: np.ndarray, bw: int, bh: int) -> np.ndarray:
+    """The reference's per-block sums (src/frontend_quantize.cu:49-74): one
+    chain per first block over its non-LLF coefficients in raw order, FMA
+    products of the FP16 values; [3][bh][bw] (zero off first blocks)."""
+    ld = np.longdouble
+    nb = bw * bh
+    out = np.zeros((3, bh, bw), np.float32)
+    for n in (8, 16, 32):
+        ys, xs = np.nonzero(acs == n)
+        if ys.size == 0:
+            continue
+        side = n // 8
+        acc = np.zeros((3, ys.size), np.float32)
+        for raw in range(n * n):
+            if raw // n < side and raw % n < side:
+                continue
+            q = raw // 64
+            slots = ((ys + q // side) * bw + xs + q % side) * 64 + raw % 64
+            x, y, b = (coef[c * nb * 64 + slots].astype(np.float32) for c in range(3))
+            acc[0] = (x.astype(ld) * y + acc[0]).astype(np.float32)
+            acc[1] = (y.astype(ld) * y + acc[1]).astype(np.float32)
+            acc[2] = ((b - y).astype(np.float32).astype(ld) * y + acc[2]).astype(np.float32)
+        out[:, ys, xs] = acc
+    return out
+
+
+def test_cfl_maps_match_reference_order(frame):
+    """The CfL sums run as 32 interleaved partial chains and a tree across a
+    warp; the maps must equal those of the reference's single chain per block
+    (and its 64-entry tile tree) except where the quotient times 84 lies
+    within 1e-4 (relative) of a rounding boundary."""
+    w, h, d, r = frame
+    bw, bh = w // 8, h // 8
+    cmw = (bw + 7) // 8
+    coef = r.coeff.view(np.float16)
+    part = _ref_order_sums(coef, r.acs.reshape(bh, bw), bw, bh)
+    near = checked = 0
+    for ty in range((bh + 7) // 8):
+        for tx in range(cmw):
+            p = np.zeros((3, 64), np.float32)
+            sub = part[:, ty * 8:ty * 8 + 8, tx * 8:tx * 8 + 8]
+            for c in range(3):
+                blk = np.zeros((8, 8), np.float32)
+                blk[:sub.shape[1], :sub.shape[2]] = sub[c]
+                v = blk.ravel()
+                s = 32
+                while s > 0:
+                    v = v.copy()
+                    v[:s] = v[:s] + v[s:2 * s]
+                    s //= 2
+                p[c, 0] = v[0]
+            sxy, syy, sby = (float(p[c, 0]) for c in range(3))
+            want = []
+            for num in (sxy, sby):
+                f = np.float32(num / syy) if syy > 0 else np.float32(0.0)
+                v84 = float(np.float32(f * np.float32(84.0)))
+                want.append((int(np.clip(np.rint(v84), -128, 127)), v84))
+            got = (int(r.ytox[ty * cmw + tx]), int(r.ytob[ty * cmw + tx]))
+            for (m, v84), g in zip(want, got):
+                checked += 1
+                if m != g:
+                    assert abs(abs(v84 - np.floor(v84)) - 0.5) <= 1e-4 * max(1.0, abs(v84)), (tx, ty, m, g, v84)
+                    near += 1
+    assert checked > 20 and near <= max(1, checked // 100)
