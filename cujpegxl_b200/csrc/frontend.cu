@@ -103,7 +103,6 @@ struct Small {
     unsigned char owner[64];
     signed char acs[64];
     int n32, n16, n8;
-    int mx, mb;
     signed char net[4];   // learned split class of each 32x32 region, -1 = RD heuristic
     float2 pow_lut[6];    // factor table of jx_pow24_2, for the packed sRGB transfer
 };
@@ -1322,36 +1321,39 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
         }
     }
     __syncthreads();
-    if (warp == 0) {
+    // The tile's maps: every warp reduces the 64 partials itself (the same
+    // tree, so the same maps on every warp) instead of waiting at one more
+    // barrier for warp 0 to do it. The trees leave the sums in lane 0, which
+    // hands its maps to the other lanes.
+    int cfl_mx;
+    int cfl_mb;
+    {
         const float2 sxy_yy{warp_tree2(__fadd2_rn(make_float2(sm.cfl[0][lane], sm.cfl[1][lane]),
                                                   make_float2(sm.cfl[0][lane + 32], sm.cfl[1][lane + 32])))};
         const float sxy{sxy_yy.x};
         const float syy{sxy_yy.y};
         const float sby{warp_tree(sm.cfl[2][lane] + sm.cfl[2][lane + 32])};
-        if (lane == 0) {
-            // The reference divides the float sums in double and rounds the
-            // quotient to float; with 53 >= 2 * 24 + 2 significand bits that
-            // double rounding equals float division's single rounding
-            // (Figueroa, "When is double rounding innocuous?", SIGNUM 1995),
-            // so the float quotient is the same value.
-            const float fx{syy > 0.0f ? sxy / syy : 0.0f};
-            const float fb{syy > 0.0f ? sby / syy : 0.0f};
-            int mx{static_cast<int>(lrintf(fx * static_cast<float>(kCflColorFactor)))};
-            int mb{static_cast<int>(lrintf(fb * static_cast<float>(kCflColorFactor)))};
-            mx = mx < -128 ? -128 : (mx > 127 ? 127 : mx);
-            mb = mb < -128 ? -128 : (mb > 127 ? 127 : mb);
-            sm.mx = mx;
-            sm.mb = mb;
+        // The reference divides the float sums in double and rounds the
+        // quotient to float; with 53 >= 2 * 24 + 2 significand bits that
+        // double rounding equals float division's single rounding
+        // (Figueroa, "When is double rounding innocuous?", SIGNUM 1995),
+        // so the float quotient is the same value.
+        const float fx{syy > 0.0f ? sxy / syy : 0.0f};
+        const float fb{syy > 0.0f ? sby / syy : 0.0f};
+        int mx{static_cast<int>(lrintf(fx * static_cast<float>(kCflColorFactor)))};
+        int mb{static_cast<int>(lrintf(fb * static_cast<float>(kCflColorFactor)))};
+        cfl_mx = __shfl_sync(0xffffffffu, mx < -128 ? -128 : (mx > 127 ? 127 : mx), 0);
+        cfl_mb = __shfl_sync(0xffffffffu, mb < -128 ? -128 : (mb > 127 ? 127 : mb), 0);
+        if (tid == 0) {
             const int tile{ty * ((W + kTile - 1) / kTile) + tx};
-            out.ytox[tile] = static_cast<std::int8_t>(mx);
-            out.ytob[tile] = static_cast<std::int8_t>(mb);
+            out.ytox[tile] = static_cast<std::int8_t>(cfl_mx);
+            out.ytob[tile] = static_cast<std::int8_t>(cfl_mb);
         }
     }
-    __syncthreads();
 
     // ---- 7. quantisation (src/frontend_quantize.cu:125-201).
-    const float ytox{static_cast<float>(sm.mx) * kCflColorScale};
-    const float ytob{jx_fma(static_cast<float>(sm.mb), kCflColorScale, kCflBaseB)};
+    const float ytox{static_cast<float>(cfl_mx) * kCflColorScale};
+    const float ytob{jx_fma(static_cast<float>(cfl_mb), kCflColorScale, kCflBaseB)};
     const std::size_t cplane{static_cast<std::size_t>(nblocks) * 64};
     // Four adjacent slots (raw indices 4m .. 4m + 3, which lie in one row of
     // their block: every row is 8, 16 or 32 long) per thread: lanes 0-15 of a
