@@ -931,7 +931,7 @@ cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* 
     return CUJPEGXL_OK;
 }
 
-uint32_t cujpegxl_b200_kernels_per_encode(void) { return 11u; }
+uint32_t cujpegxl_b200_kernels_per_encode(void) { return 12u; }
 
 void cujpegxl_b200_debug_fail_allocation(uint32_t nth) { g_fail_countdown.store(nth); }
 

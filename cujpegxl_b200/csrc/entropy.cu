@@ -1755,8 +1755,14 @@ JXB_ENTROPY_KERNELS(emit, __launch_bounds__(kAcThreads), kPhaseItems, 0u)
 // a few resident CTAs that skip the stored stripes with one load each.
 constexpr unsigned kUnstoredCtas = 148;
 
+// Every stripe adds its token count to the pool fill whether or not it fits,
+// so a frame has an unstored stripe exactly when its final fill exceeds the
+// capacity; a frame without one is passed over after one load.
+__device__ __forceinline__ bool frame_all_stored(const EntropyDev& e) { return *e.tok_count <= e.tok_capacity; }
+
 #define JXB_UNSTORED_KERNELS(NAME)                                                                         \
     __global__ void __launch_bounds__(kAcThreads) NAME##_kernel(const __grid_constant__ EntropyDev e) {       \
+        if (frame_all_stored(e)) return;                                                                      \
         for (unsigned s{blockIdx.x}; s < static_cast<unsigned>(e.nstripes); s += gridDim.x) {                 \
             if (e.stripe_tok[2 * s] != kNoTokens) continue;                                                   \
             NAME##_body(e, s, 0u);                                                                            \
@@ -1767,6 +1773,11 @@ constexpr unsigned kUnstoredCtas = 148;
         const unsigned total{b.begin[kPhaseStripes][b.nframes]};                                              \
         for (unsigned i{blockIdx.x}; i < total; i += gridDim.x) {                                             \
             const int f{batch_frame(b, kPhaseStripes, i)};                                                    \
+            if (frame_all_stored(b.frames[f])) {                                                              \
+                /* on to this block's last stripe of frame f */                                               \
+                i += (b.begin[kPhaseStripes][f + 1] - 1 - i) / gridDim.x * gridDim.x;                         \
+                continue;                                                                                     \
+            }                                                                                                 \
             const unsigned s{i - b.begin[kPhaseStripes][f]};                                                  \
             if (b.frames[f].stripe_tok[2 * s] != kNoTokens) continue;                                         \
             NAME##_body(b.frames[f], s, 0u);                                                                  \
@@ -1779,6 +1790,7 @@ JXB_UNSTORED_KERNELS(emit_unstored)
 #undef JXB_UNSTORED_KERNELS
 #undef JXB_ENTROPY_KERNELS
 
+__global__ void __launch_bounds__(256) clear_kernel(const __grid_constant__ EntropyDev e) { clear_body(e); }
 __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
     clear_body(b.frames[blockIdx.x]);
 }
@@ -1802,16 +1814,10 @@ static_assert(sizeof(EntropyBatch) <= 32000, "a batched entropy launch's paramet
 bool entropy_launch(const EntropyDev& e, void* stream) {
     if (e.nsec > kMaxSections) return false;
     cudaStream_t st{static_cast<cudaStream_t>(stream)};
-    if (cudaMemsetAsync(e.ac_hist, 0, kNumClusters * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
-        cudaMemsetAsync(e.dc_hist, 0, static_cast<std::size_t>(e.ndc) * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
-        cudaMemsetAsync(e.am_hist, 0, static_cast<std::size_t>(e.ndc) * 256 * sizeof(std::uint32_t), st) != cudaSuccess ||
-        cudaMemsetAsync(e.fb_count, 0, static_cast<std::size_t>(e.ndc) * sizeof(std::uint32_t), st) != cudaSuccess ||
-        cudaMemsetAsync(e.tok_count, 0, sizeof(std::uint32_t), st) != cudaSuccess) {
-        return false;
-    }
     const unsigned misc{(e.ac_first + kMiscItemsPerBlock - 1) / kMiscItemsPerBlock};
     const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
+    clear_kernel<<<1, 256, 0, st>>>(e);  // histograms, first-block counts, pool fill
     tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
     lengths_kernel<<<stripes + misc, kAcThreads, 0, st>>>(e);

@@ -16,9 +16,10 @@
 //   5. an emit pass writes every item's bits at its final position.
 // Passes 1, 3 and 5 are one launch each: a CTA per AC stripe (one warp per
 // block-channel while tokenising, stored tokens afterwards), then a CTA per
-// 256 other items (one thread each); passes 3 and 5 take stripes whose
+// 512 other items (two per thread); passes 3 and 5 take stripes whose
 // tokens did not fit the pool in one more launch each, with their
-// coefficients staged again.
+// coefficients staged again. A clear kernel zeroes the histograms and the
+// pool fill first.
 #pragma once
 
 #include <cstddef>
@@ -167,7 +168,7 @@ bool entropy_launch(const EntropyDev& e, void* stream);
 // begin[phase][f + 1] - 1. The frames live in the launch's parameter block.
 constexpr int kEntropyBatchFrames = 64;
 enum EntropyPhase : int {
-    kPhaseItems = 0,    // item passes: one block per AC stripe, then one per 256 other items
+    kPhaseItems = 0,    // item passes: one block per AC stripe, then one per 512 other items
     kPhaseCodes = 1,    // prefix codes: one block per histogram
     kPhaseScan = 2,     // item scan tiles
     kPhaseFrame = 3,    // one block per frame

@@ -120,13 +120,29 @@ static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two frontend CTAs no longe
 constexpr int kChromaMargin = 2;
 constexpr int kChromaWin = kTile / 2 + 2 * kChromaMargin;  // 36
 
+// a / w for a weight w of the dequantisation tables, from w_inv = RN(1 / w)
+// by Markstein's method: q0 = RN(a * w_inv), the residual a - q0 * w is exact
+// in one FMA, and RN(q0 + residual * w_inv) is the IEEE quotient RN(a / w).
+// That equality is checked for every weight of the tables (all three sizes
+// and channels) and every significand of a by
+// tests/cpu_checks/quant_div_check.c; both sides scale exactly with a's
+// exponent and are odd in a, so it holds for every a whose quotient and
+// residual stay normal, which includes every |a| > w / 2 the quantiser
+// divides. (The selection's quantiser keeps the IEEE division: its quotients
+// are formed in an out-of-line function, where loading the reciprocal cost
+// more than the division.)
+__device__ __forceinline__ float div_weight(float a, float w, float w_inv) {
+    const float q0{a * w_inv};
+    return jx_fma(jx_fma(-q0, w, a), w_inv, q0);
+}
+
 // lrintf((v * qgsf) / w) for a positive weight w (src/frontend_quantize.cu:
 // 165-178). When |v * qgsf| <= w / 2 the rounded quotient is at most 1/2 in
 // magnitude and rounds to zero, so the division is skipped; 0.5f * w is exact.
-__device__ __forceinline__ int quantize(float v, float qgsf, float w) {
+__device__ __forceinline__ int quantize(float v, float qgsf, float w, float w_inv) {
     const float scaled{v * qgsf};
     if (fabsf(scaled) <= 0.5f * w) return 0;
-    return static_cast<int>(lrintf(scaled / w));
+    return static_cast<int>(lrintf(div_weight(scaled, w, w_inv)));
 }
 
 // RatioOfDerivativesOfCubicRootToSimpleGamma (src/adaptive_quant_impl.cuh:44-55).
@@ -1400,20 +1416,26 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                 const float4 wx4{*reinterpret_cast<const float4*>(wt + raw)};
                 const float4 wy4{*reinterpret_cast<const float4*>(wt + 1024 + raw)};
                 const float4 wb4{*reinterpret_cast<const float4*>(wt + 2048 + raw)};
+                const float4 ix4{*reinterpret_cast<const float4*>(wt + kDequantInv + raw)};
+                const float4 iy4{*reinterpret_cast<const float4*>(wt + kDequantInv + 1024 + raw)};
+                const float4 ib4{*reinterpret_cast<const float4*>(wt + kDequantInv + 2048 + raw)};
                 const float wx[4]{wx4.x, wx4.y, wx4.z, wx4.w};
                 const float wy[4]{wy4.x, wy4.y, wy4.z, wy4.w};
                 const float wb[4]{wb4.x, wb4.y, wb4.z, wb4.w};
+                const float ix[4]{ix4.x, ix4.y, ix4.z, ix4.w};
+                const float iy[4]{iy4.x, iy4.y, iy4.z, iy4.w};
+                const float ib[4]{ib4.x, ib4.y, ib4.z, ib4.w};
 #pragma unroll
                 for (int h{0}; h < 4; ++h) {
                     if (llf_row && col + h < side) continue;  // an LLF slot
-                    const int qy{quantize(yr[h], qgsf, wy[h])};
+                    const int qy{quantize(yr[h], qgsf, wy[h], iy[h])};
                     // A zero Y quantum reconstructs to a signed zero, and
                     // fma(-m, +-0, v) equals v up to the sign of a zero
                     // result, which quantises to 0 either way.
                     const float yq{qy == 0 ? 0.0f : (static_cast<float>(qy) * wy[h]) / qgsf};
-                    ax[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytox, yq, xr[h]), qgsf, wx[h]));
+                    ax[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytox, yq, xr[h]), qgsf, wx[h], ix[h]));
                     ay[h] = static_cast<std::int16_t>(qy);
-                    ab[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytob, yq, br[h]), qgsf, wb[h]));
+                    ab[h] = static_cast<std::int16_t>(quantize(jx_fma(-ytob, yq, br[h]), qgsf, wb[h], ib[h]));
                 }
             }
             const std::size_t g{(static_cast<std::size_t>(by0 + lby) * bw + bx0 + lbx) * 64 + slot};
@@ -1636,6 +1658,11 @@ bool frontend_tables_init(FrontendTables* tables) {
                                      static_cast<double>(k) / md);
             }
         }
+    }
+    // Reciprocals RN(1 / w) after the weights (zero where an entry is unused).
+    deq.resize(2 * deq.size());
+    for (std::size_t i{0}; i < static_cast<std::size_t>(kDequantInv); ++i) {
+        deq[kDequantInv + i] = deq[i] != 0.0f ? 1.0f / deq[i] : 0.0f;
     }
     float* d_deq{nullptr};
     float* d_sw{nullptr};

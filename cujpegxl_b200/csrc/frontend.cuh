@@ -59,8 +59,11 @@ struct FrontendInputs {
 
 // Read-only tables in device memory (built once per device by
 // frontend_tables_init).
+// Offset of the reciprocals RN(1 / w) that follow the dequantisation weights.
+constexpr int kDequantInv = 3 * 3 * 1024;
+
 struct FrontendTables {
-    const float* dequant;     // [3 sizes][3 ch][1024] stride 1024 (size 8, 16, 32)
+    const float* dequant;     // [3 sizes][3 ch][1024] stride 1024 (size 8, 16, 32), then their reciprocals
     const float* sel_weight;  // [3 sizes][1024] DCT8 Y weight sampled at round(f*8/N)
     const float* log2_1p;     // [kLog2TableSize] log2f(1 + i)
     const double* llf_basis;  // [2][4][4] orthonormal m-point basis for m = 2, 4
