@@ -116,3 +116,23 @@ def test_batch_with_learned_decisions_matches_single_encoders():
         batch.sync()
         assert [batch.read(i) for i in range(len(FRAMES))] == plain
     net.close()
+
+
+def test_batch_with_token_pool_overflow_in_some_frames():
+    """Frames at distance 0.05 need more AC tokens than their pool holds, so
+    some of their stripes are tokenised again in the passes over unstored
+    stripes, which pass over the other frames (whose pools held everything)
+    frame by frame. Every file equals its lone encode."""
+    frames = [(520, 392, 1.0), (520, 392, 0.05), (264, 264, 2.0), (512, 384, 0.05), (640, 384, 1.0)]
+    keep, inputs, expected = [], [], []
+    for i, (w, h, d) in enumerate(frames):
+        nv = make_nv12(w, h, 700 + i)
+        k, luma, chroma, lp, cp = device_nv12(nv, w, h)
+        keep.append(k)
+        inputs.append((luma, chroma, lp, cp))
+        expected.append(_single(nv, w, h, d))
+    with Batch(frames) as batch:
+        for _ in range(2):
+            batch.encode(inputs)
+            assert batch.sync() == [len(x) for x in expected]
+            assert [batch.read(i) for i in range(len(frames))] == expected
