@@ -70,9 +70,10 @@ struct TrainSmem {
 };
 
 // Inference: the four regions of a 64x64 tile side by side, one warp group
-// each. x1[r] also holds the region's later activations (x3, x4 and the FP32
+// each. x1[r] holds the region's input (four channels per pixel, the first
+// half of the buffer) and then its later activations (x3, x4 and the FP32
 // outputs) once L1 has consumed it; x2 holds the tile's NV12 window until the
-// inputs are built.
+// inputs are built, then L1's output, then the partial sums of L3 and L4.
 constexpr int kInferThreads = 512;
 constexpr int kX3Off = 0;                          // BF16 offsets inside x1[r]
 constexpr int kX4Off = kX3Off + 64 * kActS;
@@ -87,6 +88,7 @@ static_assert(sizeof(NetWeights) % 16 == 0 && sizeof(NetSmem) % 16 == 0 && sizeo
               "16-byte shared-memory layout");
 static_assert(2 * (kOutOff + 2 * 16 * kNetC) <= 2 * kNetInPix * kNetIn, "later activations exceed x1");
 static_assert(sizeof(InferSmem) + 1024 <= 228 * 1024, "inference CTA too large");
+static_assert(4 * 512 * sizeof(float) <= 256 * kActS * sizeof(bf16), "L3/L4 partial sums exceed x2");
 
 __device__ __forceinline__ unsigned saddr(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -304,6 +306,72 @@ __device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w,
     }
 }
 
+// L3/L4 of the inference with the reduction split over the four warps of
+// the region: warp kW takes reduction steps kS0 .. kS1 - 1 for all four
+// output-channel tiles, stores its partial sums to `part`, and after a
+// barrier every thread adds the four partials of its outputs in warp order.
+template <int kInW, int kStride, int kS0, int kS1>
+__device__ __forceinline__ void cols_partial(unsigned in, unsigned zero, unsigned w, float* part, int lane) {
+    float acc[4][4]{};
+    const Im2colRows<kInW, 4, kStride, 1, kNetC, kActS> rows{in, lane & 15};
+#pragma unroll
+    for (int s{kS0}; s < kS1; ++s) {
+        const int k0{16 * s};
+        unsigned a[4];
+        ldsm_x4(a, rows.at(zero, k0, lane >> 4));
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            unsigned r[4];
+            ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kWS + k0 +
+                                                      ((lane >> 3) & 1) * 8));
+            mma(acc[2 * h], a, r[0], r[1]);
+            mma(acc[2 * h + 1], a, r[2], r[3]);
+        }
+    }
+    // part[(n * 4 + j) * 32 + lane]: fragment element j of channel tile n.
+#pragma unroll
+    for (int n{0}; n < 4; ++n) {
+#pragma unroll
+        for (int j{0}; j < 4; ++j) part[(n * 4 + j) * 32 + lane] = acc[n][j];
+    }
+}
+
+template <int kInW, int kStride, bool kRelu>
+__device__ __forceinline__ void fwd_cols_split(unsigned in, unsigned zero, unsigned w, const float* bias, bf16* outb,
+                                               float* outf, float* part, int warp, int lane) {
+    constexpr int kSteps{kNetK / 16};  // 18
+    switch (warp) {
+        case 0: cols_partial<kInW, kStride, 0, 5>(in, zero, w, part, lane); break;
+        case 1: cols_partial<kInW, kStride, 5, 10>(in, zero, w, part + 512, lane); break;
+        case 2: cols_partial<kInW, kStride, 10, 14>(in, zero, w, part + 1024, lane); break;
+        default: cols_partial<kInW, kStride, 14, kSteps>(in, zero, w, part + 1536, lane); break;
+    }
+    __syncthreads();
+    // Warp w finishes channel tile w: lane's fragment elements of tile w.
+    const int n{warp};
+    float v[4];
+#pragma unroll
+    for (int j{0}; j < 4; ++j) {
+        const int at{(n * 4 + j) * 32 + lane};
+        v[j] = ((part[at] + part[512 + at]) + part[1024 + at]) + part[1536 + at];
+    }
+    const int p{lane >> 2};
+    const int c{8 * n + 2 * (lane & 3)};
+    const float v0{v[0] + bias[c]};
+    const float v1{v[1] + bias[c + 1]};
+    const float v2{v[2] + bias[c]};
+    const float v3{v[3] + bias[c + 1]};
+    if (kRelu) {
+        store_pair(outb + p * kActS + c, fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+        store_pair(outb + (p + 8) * kActS + c, fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
+    } else {
+        outf[p * kNetC + c] = v0;
+        outf[p * kNetC + c + 1] = v1;
+        outf[(p + 8) * kNetC + c] = v2;
+        outf[(p + 8) * kNetC + c + 1] = v3;
+    }
+}
+
 // Gradient into a BF16 buffer, zero where the layer input (post-ReLU) is zero.
 __device__ __forceinline__ void store_masked(bf16* g, const bf16* x, int at, float v0, float v1) {
     const __nv_bfloat162 xv{*reinterpret_cast<const __nv_bfloat162*>(x + at)};
@@ -450,23 +518,124 @@ __device__ __forceinline__ uint4 input_pixel(const NetParamsDev& p, float x, flo
     return r;
 }
 
+// L1 of the inference on inputs of four channels per pixel ([34][34][4]
+// BF16, natural column order). Reduction step ky (16 columns) covers input
+// row 2 oy + ky: its first eight columns are taps (ky, 0) and (ky, 1) (pixels
+// 2 ox and 2 ox + 1, adjacent in memory), the next four tap (ky, 2) (pixel
+// 2 ox + 2) and the last four pixel 2 ox + 3 against zero weights. Three
+// steps instead of the five of the eight-channel layout (whose upper four
+// channels and last eight columns are zeros), and an ldmatrix's eight rows
+// (consecutive ox) are 16 contiguous bytes each.
+constexpr int kL1PackedK = 48;
+__device__ __forceinline__ void pack_w1(NetWeights& s, const NetParamsDev& p, int tid, int nthreads) {
+    for (int i{tid}; i < kNetC * kL1PackedK; i += nthreads) {
+        const int co{i / kL1PackedK};
+        const int k{i - co * kL1PackedK};
+        const int ky{k >> 4};
+        const int j{k & 15};
+        std::uint16_t v{0};
+        if (j < 12) {
+            const int tap{3 * ky + (j < 8 ? j >> 2 : 2)};
+            v = p.w[kNetW1 + co * kNetK1 + tap * kNetIn + (j & 3)];
+        }
+        reinterpret_cast<std::uint16_t*>(s.w1)[co * kW1S + k] = v;
+    }
+}
+
+__device__ __forceinline__ void fwd_l1_packed(unsigned in, unsigned w, const float* bias, bf16* out, int warp,
+                                              int lane) {
+#pragma unroll 1
+    for (int i0{0}; i0 < 4; i0 += 2) {
+        unsigned base[2];
+#pragma unroll
+        for (int i{0}; i < 2; ++i) {
+            const int pos{(warp + 4 * (i0 + i)) * 16 + (lane & 15)};
+            const int oy{pos >> 4};
+            const int ox{pos & 15};
+            base[i] = in + 2u * static_cast<unsigned>((2 * oy * kNetInW + 2 * ox) * 4) + 16u * (lane >> 4);
+        }
+        float acc[2][4][4];
+#pragma unroll
+        for (int i{0}; i < 2; ++i) {
+#pragma unroll
+            for (int n{0}; n < 4; ++n) {
+#pragma unroll
+                for (int j{0}; j < 4; ++j) acc[i][n][j] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int ky{0}; ky < 3; ++ky) {
+            unsigned b[4][2];
+#pragma unroll
+            for (int h{0}; h < 2; ++h) {
+                unsigned r[4];
+                ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kW1S + 16 * ky +
+                                                          ((lane >> 3) & 1) * 8));
+                b[2 * h][0] = r[0];
+                b[2 * h][1] = r[1];
+                b[2 * h + 1][0] = r[2];
+                b[2 * h + 1][1] = r[3];
+            }
+#pragma unroll
+            for (int i{0}; i < 2; ++i) {
+                unsigned a[4];
+                ldsm_x4(a, base[i] + 2u * static_cast<unsigned>(ky * kNetInW * 4));
+#pragma unroll
+                for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
+            }
+        }
+#pragma unroll
+        for (int i{0}; i < 2; ++i) {
+            const int p{(warp + 4 * (i0 + i)) * 16 + (lane >> 2)};
+            const int s0{(p / 16) * 16 + par_col<16, true>(p % 16)};
+            const int s1{((p + 8) / 16) * 16 + par_col<16, true>((p + 8) % 16)};
+#pragma unroll
+            for (int n{0}; n < 4; ++n) {
+                const int c{n * 8 + 2 * (lane & 3)};
+                const float b0{bias[c]};
+                const float b1{bias[c + 1]};
+                store_pair(out + s0 * kActS + c, fmaxf(acc[i][n][0] + b0, 0.0f), fmaxf(acc[i][n][1] + b1, 0.0f));
+                store_pair(out + s1 * kActS + c, fmaxf(acc[i][n][2] + b0, 0.0f), fmaxf(acc[i][n][3] + b1, 0.0f));
+            }
+        }
+    }
+}
+
 // The four layers over the region in s.x1; ends with s.out filled.
 // warp: the warp's index (0..3) within the group of four warps that owns the
 // region; every thread of the CTA calls this together.
-// kPar: x1 and x2 are stored with their columns parity-split (par_col).
-template <bool kPar = false>
+// kInfer: the inference layout and schedule: x1 holds four channels per
+// pixel in natural column order (L1 by fwd_l1_packed), x2 is stored with its
+// columns parity-split (par_col), and L3 and L4 split their reduction over
+// the group's warps with x2 as the scratch of their partial sums. Otherwise
+// (training) x1 holds eight channels per pixel and nothing is parity-split.
+template <bool kInfer = false>
 __device__ __forceinline__ void net_forward(const NetWeights& wt, bf16* x1, bf16* x2, bf16* x3, bf16* x4,
                                             float* out, int warp, int lane) {
     const unsigned zero{saddr(wt.zero)};
-    fwd_rows<kNetInW, 16, 2, 0, kNetIn, kNetIn, kNetK1, kW1S, kPar, kPar>(saddr(x1), zero, saddr(wt.w1), wt.bias[0],
-                                                                        x2, warp, lane);
+    if constexpr (kInfer) {
+        fwd_l1_packed(saddr(x1), saddr(wt.w1), wt.bias[0], x2, warp, lane);
+    } else {
+        fwd_rows<kNetInW, 16, 2, 0, kNetIn, kNetIn, kNetK1, kW1S, kInfer, kInfer>(saddr(x1), zero, saddr(wt.w1),
+                                                                            wt.bias[0], x2, warp, lane);
+    }
     __syncthreads();
-    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS, kPar, false>(saddr(x2), zero, saddr(wt.w[0]), wt.bias[1], x3,
+    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS, kInfer, false>(saddr(x2), zero, saddr(wt.w[0]), wt.bias[1], x3,
                                                                  warp, lane);
     __syncthreads();
-    fwd_cols<8, 2, true>(saddr(x3), zero, saddr(wt.w[1]), wt.bias[2], x4, nullptr, warp, lane);
+    if constexpr (kInfer) {
+        fwd_cols_split<8, 2, true>(saddr(x3), zero, saddr(wt.w[1]), wt.bias[2], x4, nullptr,
+                                   reinterpret_cast<float*>(x2), warp, lane);
+    } else {
+        fwd_cols<8, 2, true>(saddr(x3), zero, saddr(wt.w[1]), wt.bias[2], x4, nullptr, warp, lane);
+    }
     __syncthreads();
-    fwd_cols<4, 1, false>(saddr(x4), zero, saddr(wt.w[2]), wt.bias[3], nullptr, out, warp, lane);
+    if constexpr (kInfer) {
+        fwd_cols_split<4, 1, false>(saddr(x4), zero, saddr(wt.w[2]), wt.bias[3], nullptr, out,
+                                    reinterpret_cast<float*>(x2), warp, lane);
+    } else {
+        fwd_cols<4, 1, false>(saddr(x4), zero, saddr(wt.w[2]), wt.bias[3], nullptr, out, warp, lane);
+    }
     __syncthreads();
 }
 
@@ -539,38 +708,62 @@ __device__ __forceinline__ float hw_log2(float x) {
     return y;
 }
 
-// The network's input pixel: xyb_pixel's NV12 -> XYB conversion, from the
-// pixel's luma byte and its four chroma taps ((cb, cr) pairs as 16-bit words:
-// top-left, top-right, bottom-left, bottom-right, weights wxa (left) and wya
-// (top) in {1, 3}), with the two transfer functions taken from the hardware
-// exp2/log2 (x^2.4 = 2^(2.4 log2 x), cbrt x = 2^(log2 x / 3)) instead of the
-// frontend's exact ones. The values differ from the frontend's by about 1e-6
-// relative, far below the BF16 rounding of the input (4e-3), at a fraction of
-// the instructions.
-__device__ __forceinline__ void net_xyb_taps(int luma, unsigned aa, unsigned ab, unsigned ba, unsigned bb, int wxa,
-                                             int wya, float& ox, float& oy, float& ob) {
-    const float yv{static_cast<float>(luma) * kInv255};
+// The network's input pixels: xyb_pixel's NV12 -> XYB conversion of two
+// pixels at once (component h of every result is pixel h), from each pixel's
+// luma byte and its four chroma taps ((cb, cr) pairs as 16-bit words:
+// top-left, top-right, bottom-left, bottom-right, weights wxa (left) and
+// wya (top) in {1, 3}), with the two transfer functions taken from the
+// hardware exp2/log2 (x^2.4 = 2^(2.4 log2 x), cbrt x = 2^(log2 x / 3))
+// instead of the frontend's exact ones. The values differ from the
+// frontend's by about 1e-6 relative, far below the BF16 rounding of the
+// input (4e-3), at a fraction of the instructions. The arithmetic runs on
+// packed f32x2 pairs (each component rounded as the scalar operation); the
+// transfer functions stay scalar.
+__device__ __forceinline__ void net_xyb_taps2(const int (&luma)[2], const unsigned (&aa)[2], const unsigned (&ab)[2],
+                                              const unsigned (&ba)[2], const unsigned (&bb)[2], int wxa,
+                                              const int (&wya)[2], float2& ox, float2& oy, float2& ob) {
+    const float2 yv{__fmul2_rn(make_float2(static_cast<float>(luma[0]), static_cast<float>(luma[1])), f2dup(kInv255))};
     const int wxb{4 - wxa};
-    const int wyb{4 - wya};
-    const int scb{wya * (wxa * static_cast<int>(aa & 0xffu) + wxb * static_cast<int>(ab & 0xffu)) +
-                  wyb * (wxa * static_cast<int>(ba & 0xffu) + wxb * static_cast<int>(bb & 0xffu))};
-    const int scr{wya * (wxa * static_cast<int>(aa >> 8) + wxb * static_cast<int>(ab >> 8)) +
-                  wyb * (wxa * static_cast<int>(ba >> 8) + wxb * static_cast<int>(bb >> 8))};
-    const float cb{static_cast<float>(scb) * (1.0f / 4080.0f) - kChromaCenter};
-    const float cr{static_cast<float>(scr) * (1.0f / 4080.0f) - kChromaCenter};
-    auto lin = [](float e) {
-        e = clamp01(e);
-        return clamp01(e <= 0.04045f ? e * (1.0f / 12.92f) : hw_exp2(2.4f * hw_log2((e + 0.055f) * (1.0f / 1.055f))));
+    int scb[2], scr[2];
+#pragma unroll
+    for (int h{0}; h < 2; ++h) {
+        const int wyb{4 - wya[h]};
+        scb[h] = wya[h] * (wxa * static_cast<int>(aa[h] & 0xffu) + wxb * static_cast<int>(ab[h] & 0xffu)) +
+                 wyb * (wxa * static_cast<int>(ba[h] & 0xffu) + wxb * static_cast<int>(bb[h] & 0xffu));
+        scr[h] = wya[h] * (wxa * static_cast<int>(aa[h] >> 8) + wxb * static_cast<int>(ab[h] >> 8)) +
+                 wyb * (wxa * static_cast<int>(ba[h] >> 8) + wxb * static_cast<int>(bb[h] >> 8));
+    }
+    const float2 cb{__fadd2_rn(__fmul2_rn(make_float2(static_cast<float>(scb[0]), static_cast<float>(scb[1])),
+                                          f2dup(1.0f / 4080.0f)),
+                               f2dup(-kChromaCenter))};
+    const float2 cr{__fadd2_rn(__fmul2_rn(make_float2(static_cast<float>(scr[0]), static_cast<float>(scr[1])),
+                                          f2dup(1.0f / 4080.0f)),
+                               f2dup(-kChromaCenter))};
+    auto lin = [](float2 e) {
+        e = clamp01_2(e);
+        const float2 lo{__fmul2_rn(e, f2dup(1.0f / 12.92f))};
+        const float2 t{__fmul2_rn(__fadd2_rn(e, f2dup(0.055f)), f2dup(1.0f / 1.055f))};
+        const float2 l{__fmul2_rn(f2dup(2.4f), make_float2(hw_log2(t.x), hw_log2(t.y)))};
+        const float2 hi{hw_exp2(l.x), hw_exp2(l.y)};
+        return clamp01_2(make_float2(e.x <= 0.04045f ? lo.x : hi.x, e.y <= 0.04045f ? lo.y : hi.y));
     };
-    const float r{lin(jx_fma(kCrToR, cr, yv))};
-    const float g{lin(jx_fma(-kCrToG, cr, jx_fma(-kCbToG, cb, yv)))};
-    const float b{lin(jx_fma(kCbToB, cb, yv))};
-    auto cbrt_pos = [](float v) { return v > 0.0f ? hw_exp2(hw_log2(v) * (1.0f / 3.0f)) : 0.0f; };
-    const float m0{cbrt_pos(jx_fma(kM02, b, jx_fma(kM01, g, jx_fma(kM00, r, kOpsinBias)))) + kNegCbrtBias};
-    const float m1{cbrt_pos(jx_fma(kM12, b, jx_fma(kM11, g, jx_fma(kM10, r, kOpsinBias)))) + kNegCbrtBias};
-    const float m2{cbrt_pos(jx_fma(kM22, b, jx_fma(kM21, g, jx_fma(kM20, r, kOpsinBias)))) + kNegCbrtBias};
-    ox = 0.5f * (m0 - m1);
-    oy = 0.5f * (m0 + m1);
+    const float2 r{lin(__ffma2_rn(f2dup(kCrToR), cr, yv))};
+    const float2 g{lin(__ffma2_rn(f2dup(-kCrToG), cr, __ffma2_rn(f2dup(-kCbToG), cb, yv)))};
+    const float2 b{lin(__ffma2_rn(f2dup(kCbToB), cb, yv))};
+    auto cbrt_pos = [](float2 v) {
+        const float2 l{__fmul2_rn(make_float2(hw_log2(v.x), hw_log2(v.y)), f2dup(1.0f / 3.0f))};
+        return make_float2(v.x > 0.0f ? hw_exp2(l.x) : 0.0f, v.y > 0.0f ? hw_exp2(l.y) : 0.0f);
+    };
+    const float2 bias{f2dup(kOpsinBias)};
+    const float2 nb{f2dup(kNegCbrtBias)};
+    const float2 m0{__fadd2_rn(
+        cbrt_pos(__ffma2_rn(f2dup(kM02), b, __ffma2_rn(f2dup(kM01), g, __ffma2_rn(f2dup(kM00), r, bias)))), nb)};
+    const float2 m1{__fadd2_rn(
+        cbrt_pos(__ffma2_rn(f2dup(kM12), b, __ffma2_rn(f2dup(kM11), g, __ffma2_rn(f2dup(kM10), r, bias)))), nb)};
+    const float2 m2{__fadd2_rn(
+        cbrt_pos(__ffma2_rn(f2dup(kM22), b, __ffma2_rn(f2dup(kM21), g, __ffma2_rn(f2dup(kM20), r, bias)))), nb)};
+    ox = __fmul2_rn(f2dup(0.5f), __fadd2_rn(m0, f2neg(m1)));
+    oy = __fmul2_rn(f2dup(0.5f), __fadd2_rn(m0, m1));
     ob = m2;
 }
 
@@ -590,6 +783,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     const int lane{tid & 31};
     const int grp{warp >> 2};
     load_net(s.wt, p, tid, kInferThreads);
+    __syncthreads();
+    pack_w1(s.wt, p, tid, kInferThreads);
     const int W{in.width};
     const int H{in.height};
     const int bw{W >> 3};
@@ -660,14 +855,13 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         if (full != 0) {   // block-uniform
             const int cx0{(px0 >> 1) - 2};
             const int cy0{(py0 >> 1) - 2};
-            // Thread t takes stored (parity-split) column t % 34 of rows
-            // t / 34, t / 34 + 15, ... of every full region: its column's
-            // chroma taps and clamps are computed once, and a warp's stores
-            // are contiguous.
+            // Thread t takes column t % 34 of rows t / 34, t / 34 + 15, ...
+            // of the regions, rows row (region rx) and 32 + row (region
+            // 2 + rx) as one pixel pair: its column's chroma taps and clamps
+            // are computed once, and a warp's stores are contiguous.
             constexpr int kRowLanes{kInferThreads / kNetInW};  // 15
             if (tid < kNetInW * kRowLanes) {
-                const int c{tid % kNetInW};
-                const int x{c < (kNetInW + 1) / 2 ? 2 * c : 2 * (c - (kNetInW + 1) / 2) + 1};
+                const int x{tid % kNetInW};
                 const auto* cw{reinterpret_cast<const std::uint16_t*>(win_chroma)};
 #pragma unroll 1
                 for (int rx{0}; rx < 2; ++rx) {
@@ -677,22 +871,46 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                     const int xa{((gx & 1) ? jx : max(jx - 1, 0)) - cx0};
                     const int xb{((gx & 1) ? min(jx + 1, (W >> 1) - 1) : jx) - cx0};
                     const int wxa{(gx & 1) ? 3 : 1};
+                    // Rows row (region rx) and 32 + row (region 2 + rx) as one pair.
+                    const bool top{((full >> rx) & 1u) != 0};
+                    const bool bot{((full >> (2 + rx)) & 1u) != 0};
+                    if (!top && !bot) continue;
 #pragma unroll
-                    for (int ry{0}; ry < 2; ++ry) {
-                        const int r{2 * ry + rx};
-                        if (((full >> r) & 1u) == 0) continue;
+                    for (int row{tid / kNetInW}; row < kNetInW; row += kRowLanes) {
+                        int luma[2], wya[2];
+                        unsigned aa[2], ab[2], ba[2], bb[2];
 #pragma unroll
-                        for (int row{tid / kNetInW}; row < kNetInW; row += kRowLanes) {
-                            const int wy{32 * ry + row};
+                        for (int h{0}; h < 2; ++h) {
+                            const int wy{32 * h + row};
                             const int gy{min(max(py0 - 1 + wy, 0), H - 1)};
                             const int jy{gy >> 1};
                             const int ya{(((gy & 1) ? jy : max(jy - 1, 0)) - cy0) * kTileChroma};
                             const int yb{(((gy & 1) ? min(jy + 1, (H >> 1) - 1) : jy) - cy0) * kTileChroma};
-                            float xv, yv, bv;
-                            net_xyb_taps(win_luma[wy * kTileWin + wx], cw[ya + xa], cw[ya + xb], cw[yb + xa],
-                                         cw[yb + xb], wxa, (gy & 1) ? 3 : 1, xv, yv, bv);
-                            *reinterpret_cast<uint4*>(&s.x1[r][(row * kNetInW + c) * kNetIn]) =
-                                input_pixel(p, xv, yv, bv, log2_distance);
+                            luma[h] = win_luma[wy * kTileWin + wx];
+                            aa[h] = cw[ya + xa];
+                            ab[h] = cw[ya + xb];
+                            ba[h] = cw[yb + xa];
+                            bb[h] = cw[yb + xb];
+                            wya[h] = (gy & 1) ? 3 : 1;
+                        }
+                        float2 xv, yv, bv;
+                        net_xyb_taps2(luma, aa, ab, ba, bb, wxa, wya, xv, yv, bv);
+                        const float2 nx{__fmul2_rn(__fadd2_rn(xv, f2dup(-p.shift[0])), f2dup(p.scale[0]))};
+                        const float2 ny{__fmul2_rn(__fadd2_rn(yv, f2dup(-p.shift[1])), f2dup(p.scale[1]))};
+                        const float2 nbv{__fmul2_rn(__fadd2_rn(bv, f2dup(-p.shift[2])), f2dup(p.scale[2]))};
+                        const float nd{(log2_distance - p.shift[3]) * p.scale[3]};
+                        const int at{(row * kNetInW + x) * 4};
+                        if (top) {
+                            const __nv_bfloat162 lo{__floats2bfloat162_rn(nx.x, ny.x)};
+                            const __nv_bfloat162 hi{__floats2bfloat162_rn(nbv.x, nd)};
+                            *reinterpret_cast<uint2*>(&s.x1[rx][at]) =
+                                make_uint2(*reinterpret_cast<const unsigned*>(&lo), *reinterpret_cast<const unsigned*>(&hi));
+                        }
+                        if (bot) {
+                            const __nv_bfloat162 lo{__floats2bfloat162_rn(nx.y, ny.y)};
+                            const __nv_bfloat162 hi{__floats2bfloat162_rn(nbv.y, nd)};
+                            *reinterpret_cast<uint2*>(&s.x1[2 + rx][at]) =
+                                make_uint2(*reinterpret_cast<const unsigned*>(&lo), *reinterpret_cast<const unsigned*>(&hi));
                         }
                     }
                 }
