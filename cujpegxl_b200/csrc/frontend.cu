@@ -671,120 +671,126 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
         }
     }
 
-    // ---- 2. adaptive quantisation (src/frontend_fused.cu:233-342).
+    // ---- 2. adaptive quantisation (src/frontend_fused.cu:233-342). A tile
+    // whose four regions all take their quant field from the network skips
+    // the phase (the branch is uniform over the CTA).
     const float* Y{xyb + kXplane};
-    {
-        // Pixels (dx, dx + 1) of each cell row in pairs on packed f32x2
-        // arithmetic (the division and square root stay scalar); the sum
-        // still accumulates in raster order.
-        const int ccx{tid & 15};
-        const int ccy{tid >> 4};
-        const int ix0{ccx * 4 + kHalo};  // even: the float2 loads below are aligned
-        float sum{0.0f};
-#pragma unroll
-        for (int dy{0}; dy < 4; ++dy) {
-            const int iy{ccy * 4 + dy + kHalo};
-            const float* C{Y + iy * kXs + ix0};
-            const float* U{C - kXs};
-            const float* D{C + kXs};
-            const float2 c0{*reinterpret_cast<const float2*>(C - 2)};  // ix0-2, ix0-1
-            const float2 c1{*reinterpret_cast<const float2*>(C)};      // ix0, ix0+1
-            const float2 c2{*reinterpret_cast<const float2*>(C + 2)};  // ix0+2, ix0+3
-            const float2 c3{*reinterpret_cast<const float2*>(C + 4)};  // ix0+4, ix0+5
-            const float2 up[2]{*reinterpret_cast<const float2*>(U), *reinterpret_cast<const float2*>(U + 2)};
-            const float2 dn[2]{*reinterpret_cast<const float2*>(D), *reinterpret_cast<const float2*>(D + 2)};
-            const float2 ctr[2]{c1, c2};
-            const float2 lft[2]{make_float2(c0.y, c1.x), make_float2(c1.y, c2.x)};
-            const float2 rgt[2]{make_float2(c1.y, c2.x), make_float2(c2.y, c3.x)};
-#pragma unroll
-            for (int h{0}; h < 2; ++h) {
-                const float2 yv{ctr[h]};
-                const float2 base{__fmul2_rn(
-                    f2dup(0.25f), __fadd2_rn(__fadd2_rn(__fadd2_rn(dn[h], up[h]), lft[h]), rgt[h]))};
-                // ratio_gamma<false>(yv + kMatchGammaOffset)
-                float2 v{__fadd2_rn(yv, f2dup(kMatchGammaOffset))};
-                v = make_float2(v.x < 0.0f ? 0.0f : v.x, v.y < 0.0f ? 0.0f : v.y);
-                const float2 v2{__fmul2_rn(v, v)};
-                const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
-                const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
-                const float2 ratio{div2_ratio(den, num)};
-                float2 d{__fmul2_rn(ratio, __fadd2_rn(yv, f2neg(base)))};
-                d = __fmul2_rn(d, d);
-                d = make_float2(fminf(d.x, kDiffLimit), fminf(d.y, kDiffLimit));
-                // Masking square root 0.25 * sqrt(d * mul + offset) (src/adaptive_quant_impl.cuh:57-61).
-                const float2 t{__ffma2_rn(d, f2dup(sc.mask_sqrt_mul), f2dup(kMaskLogOffset))};
-                const float2 m{__fmul2_rn(f2dup(0.25f), make_float2(sqrtf(t.x), sqrtf(t.y)))};
-                sum = sum + m.x;
-                sum = sum + m.y;
-            }
-        }
-        sm.pre[tid] = 0.25f * sum;
-    }
-    __syncthreads();
-    // The four eroded cells of each of this warp's 8 blocks (block warp + 8j),
-    // one per lane: lane 4j + k holds cell k = (k & 1, k >> 1) of block j's
-    // 2x2 cells. Their sum (e0 + e2) + (e1 + e3) is the order in which a
-    // 32-lane tree with the cells in lanes 0-3 and zeros elsewhere adds them.
-    float ero_sum;
-    {
-        const int lb{warp + 8 * (lane >> 2)};
-        const int k{lane & 3};
-        const int lbx{lb & 7};
-        const int lby{lb >> 3};
-        const float e{erosion_cell(sm.pre, (lbx >> 2) * 8, (lby >> 2) * 8, 2 * (lbx & 3) + (k & 1),
-                                   2 * (lby & 3) + (k >> 1), sc.km0, sc.km1, sc.km2, sc.km3)};
-        const float s{e + __shfl_down_sync(0xffffffffu, e, 2)};
-        ero_sum = s + __shfl_down_sync(0xffffffffu, s, 1);
-    }
-    for (int lb{warp}; lb < 64; lb += kThreads / 32) {
-        const int lbx{lb & 7};
-        const int lby{lb >> 3};
-        const int gbx{bx0 + lbx};
-        const int gby{by0 + lby};
-        const float eroded{__shfl_sync(0xffffffffu, ero_sum, 4 * (lb >> 3))};
-        if (gbx >= bw || gby >= bh || ((qmask >> region_of_block(lb)) & 1u) != 0) {
-            continue;  // warp-uniform
-        }
-        const int fx{lane & 7};
-        // Rows fy and fy + 4 of the block as the two components of packed
-        // pairs; each half's tree is the reference's, run on both at once.
-        const int fy{lane >> 3};
-        const int ix{lbx * 8 + fx + kHalo};
-        const int iy{lby * 8 + fy + kHalo};
-        const int i0{iy * kXs + ix};
-        const int i1{i0 + 4 * kXs};
-        const float2 yv{Y[i0], Y[i1]};
-        const float2 xv{xyb[i0], xyb[i1]};
-        const float2 bv{xyb[2 * kXplane + i0], xyb[2 * kXplane + i1]};
-        float2 hf{0.0f, 0.0f};
-        if (fx < 7) {
-            const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + 1], Y[i1 + 1])))};
-            hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)), fminf(kHfValMin, fabsf(d.y))));
-        }
+    if (qmask != 0xFu) {
         {
-            // Row fy + 4 has no lower neighbour in the block when it is 7; its
-            // term is then +0, which leaves the non-negative sum unchanged.
-            const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + kXs], Y[i1 + kXs])))};
-            hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)),
-                                            fy + 4 < 7 ? fminf(kHfValMin, fabsf(d.y)) : 0.0f));
+            // Pixels (dx, dx + 1) of each cell row in pairs on packed f32x2
+            // arithmetic (the division and square root stay scalar); the sum
+            // still accumulates in raster order.
+            const int ccx{tid & 15};
+            const int ccy{tid >> 4};
+            const int ix0{ccx * 4 + kHalo};  // even: the float2 loads below are aligned
+            float sum{0.0f};
+    #pragma unroll
+            for (int dy{0}; dy < 4; ++dy) {
+                const int iy{ccy * 4 + dy + kHalo};
+                const float* C{Y + iy * kXs + ix0};
+                const float* U{C - kXs};
+                const float* D{C + kXs};
+                const float2 c0{*reinterpret_cast<const float2*>(C - 2)};  // ix0-2, ix0-1
+                const float2 c1{*reinterpret_cast<const float2*>(C)};      // ix0, ix0+1
+                const float2 c2{*reinterpret_cast<const float2*>(C + 2)};  // ix0+2, ix0+3
+                const float2 c3{*reinterpret_cast<const float2*>(C + 4)};  // ix0+4, ix0+5
+                const float2 up[2]{*reinterpret_cast<const float2*>(U), *reinterpret_cast<const float2*>(U + 2)};
+                const float2 dn[2]{*reinterpret_cast<const float2*>(D), *reinterpret_cast<const float2*>(D + 2)};
+                const float2 ctr[2]{c1, c2};
+                const float2 lft[2]{make_float2(c0.y, c1.x), make_float2(c1.y, c2.x)};
+                const float2 rgt[2]{make_float2(c1.y, c2.x), make_float2(c2.y, c3.x)};
+    #pragma unroll
+                for (int h{0}; h < 2; ++h) {
+                    const float2 yv{ctr[h]};
+                    const float2 base{__fmul2_rn(
+                        f2dup(0.25f), __fadd2_rn(__fadd2_rn(__fadd2_rn(dn[h], up[h]), lft[h]), rgt[h]))};
+                    // ratio_gamma<false>(yv + kMatchGammaOffset)
+                    float2 v{__fadd2_rn(yv, f2dup(kMatchGammaOffset))};
+                    v = make_float2(v.x < 0.0f ? 0.0f : v.x, v.y < 0.0f ? 0.0f : v.y);
+                    const float2 v2{__fmul2_rn(v, v)};
+                    const float2 num{__ffma2_rn(f2dup(kRatioNumMul), v2, f2dup(kRatioEps))};
+                    const float2 den{__ffma2_rn(__fmul2_rn(f2dup(kRatioDenMul), v), v2, f2dup(kRatioVOffset))};
+                    const float2 ratio{div2_ratio(den, num)};
+                    float2 d{__fmul2_rn(ratio, __fadd2_rn(yv, f2neg(base)))};
+                    d = __fmul2_rn(d, d);
+                    d = make_float2(fminf(d.x, kDiffLimit), fminf(d.y, kDiffLimit));
+                    // Masking square root 0.25 * sqrt(d * mul + offset) (src/adaptive_quant_impl.cuh:57-61).
+                    const float2 t{__ffma2_rn(d, f2dup(sc.mask_sqrt_mul), f2dup(kMaskLogOffset))};
+                    const float2 m{__fmul2_rn(f2dup(0.25f), make_float2(sqrtf(t.x), sqrtf(t.y)))};
+                    sum = sum + m.x;
+                    sum = sum + m.y;
+                }
+            }
+            sm.pre[tid] = 0.25f * sum;
         }
-        const float2 iny{__fadd2_rn(yv, f2dup(kGammaBias))};
-        const float2 gp{__fadd2_rn(ratio_gamma_inv2(__fadd2_rn(iny, f2neg(xv))), ratio_gamma_inv2(__fadd2_rn(iny, xv)))};
-        const float2 pye{__fadd2_rn(__fadd2_rn(yv, f2dup(kBlueOffset)), make_float2(fabsf(xv.x), fabsf(xv.y)))};
-        const float2 bd{__fadd2_rn(bv, f2neg(pye))};
-        const float2 bp{bv.x > pye.x ? fminf(bd.x, kBlueLimit) : 0.0f, bv.y > pye.y ? fminf(bd.y, kBlueLimit) : 0.0f};
-        const float2 red0{warp_tree2(hf)};
-        const float2 red1{warp_tree2(gp)};
-        const float2 red2{warp_tree2(bp)};
-        if (lane == 0) {
-            // The block's quant field is finished from these sums by its own
-            // thread in step 4e, where most warps are otherwise idle. The
-            // eroded sum gets the second half's tree of zeros added, as the
-            // per-half reduction did.
-            sm.aq_sums[0][lb] = red0.x + red0.y;
-            sm.aq_sums[1][lb] = red1.x + red1.y;
-            sm.aq_sums[2][lb] = red2.x + red2.y;
-            sm.aq_sums[3][lb] = eroded + 0.0f;
+        __syncthreads();
+        // The four eroded cells of each of this warp's 8 blocks (block warp + 8j),
+        // one per lane: lane 4j + k holds cell k = (k & 1, k >> 1) of block j's
+        // 2x2 cells. Their sum (e0 + e2) + (e1 + e3) is the order in which a
+        // 32-lane tree with the cells in lanes 0-3 and zeros elsewhere adds them.
+        float ero_sum;
+        {
+            const int lb{warp + 8 * (lane >> 2)};
+            const int k{lane & 3};
+            const int lbx{lb & 7};
+            const int lby{lb >> 3};
+            const float e{erosion_cell(sm.pre, (lbx >> 2) * 8, (lby >> 2) * 8, 2 * (lbx & 3) + (k & 1),
+                                       2 * (lby & 3) + (k >> 1), sc.km0, sc.km1, sc.km2, sc.km3)};
+            const float s{e + __shfl_down_sync(0xffffffffu, e, 2)};
+            ero_sum = s + __shfl_down_sync(0xffffffffu, s, 1);
+        }
+        for (int lb{warp}; lb < 64; lb += kThreads / 32) {
+            const int lbx{lb & 7};
+            const int lby{lb >> 3};
+            const int gbx{bx0 + lbx};
+            const int gby{by0 + lby};
+            const float eroded{__shfl_sync(0xffffffffu, ero_sum, 4 * (lb >> 3))};
+            if (gbx >= bw || gby >= bh || ((qmask >> region_of_block(lb)) & 1u) != 0) {
+                continue;  // warp-uniform
+            }
+            const int fx{lane & 7};
+            // Rows fy and fy + 4 of the block as the two components of packed
+            // pairs; each half's tree is the reference's, run on both at once.
+            const int fy{lane >> 3};
+            const int ix{lbx * 8 + fx + kHalo};
+            const int iy{lby * 8 + fy + kHalo};
+            const int i0{iy * kXs + ix};
+            const int i1{i0 + 4 * kXs};
+            const float2 yv{Y[i0], Y[i1]};
+            const float2 xv{xyb[i0], xyb[i1]};
+            const float2 bv{xyb[2 * kXplane + i0], xyb[2 * kXplane + i1]};
+            float2 hf{0.0f, 0.0f};
+            if (fx < 7) {
+                const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + 1], Y[i1 + 1])))};
+                hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)), fminf(kHfValMin, fabsf(d.y))));
+            }
+            {
+                // Row fy + 4 has no lower neighbour in the block when it is 7; its
+                // term is then +0, which leaves the non-negative sum unchanged.
+                const float2 d{__fadd2_rn(yv, f2neg(make_float2(Y[i0 + kXs], Y[i1 + kXs])))};
+                hf = __fadd2_rn(hf, make_float2(fminf(kHfValMin, fabsf(d.x)),
+                                                fy + 4 < 7 ? fminf(kHfValMin, fabsf(d.y)) : 0.0f));
+            }
+            const float2 iny{__fadd2_rn(yv, f2dup(kGammaBias))};
+            const float2 gp{__fadd2_rn(ratio_gamma_inv2(__fadd2_rn(iny, f2neg(xv))),
+                                       ratio_gamma_inv2(__fadd2_rn(iny, xv)))};
+            const float2 pye{__fadd2_rn(__fadd2_rn(yv, f2dup(kBlueOffset)), make_float2(fabsf(xv.x), fabsf(xv.y)))};
+            const float2 bd{__fadd2_rn(bv, f2neg(pye))};
+            const float2 bp{bv.x > pye.x ? fminf(bd.x, kBlueLimit) : 0.0f,
+                            bv.y > pye.y ? fminf(bd.y, kBlueLimit) : 0.0f};
+            const float2 red0{warp_tree2(hf)};
+            const float2 red1{warp_tree2(gp)};
+            const float2 red2{warp_tree2(bp)};
+            if (lane == 0) {
+                // The block's quant field is finished from these sums by its own
+                // thread in step 4e, where most warps are otherwise idle. The
+                // eroded sum gets the second half's tree of zeros added, as the
+                // per-half reduction did.
+                sm.aq_sums[0][lb] = red0.x + red0.y;
+                sm.aq_sums[1][lb] = red1.x + red1.y;
+                sm.aq_sums[2][lb] = red2.x + red2.y;
+                sm.aq_sums[3][lb] = eroded + 0.0f;
+            }
         }
     }
 
