@@ -3,7 +3,7 @@
 the benchmark set measured in the same run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--streams S]
-                    [--no-extras] [--workload 4k|mixed64]
+                    [--no-extras | --extras NAME,...] [--workload 4k|mixed64]
 
 Headline (`value`): the seeded synthetic 3840x2160 NV12 frame (seed 0),
 distance 1.0, the plain path (XYB, AQ, gaborish, transform selection, DCT,
@@ -26,7 +26,8 @@ pinned host memory.
 roofline: the fused frontend kernel, its algorithmic bytes per 4K frame over
 its event-timed duration, against the measured HBM copy bandwidth.
 
-Extras (N = 1, rank 0; --no-extras skips them), each timed in this run:
+Extras (N = 1, rank 0; --no-extras skips them, --extras a,b runs a subset),
+each timed in this run:
   distances: the 4K frame at d = 0.5, 2 and 4 (frames/s over the same step,
     bpp, PSNR-Y through the in-repo decoder);
   learned: the 4K step with the shipped transform-decision network (split
@@ -65,6 +66,7 @@ sys.path.insert(0, str(REPO))
 W_4K, H_4K = 3840, 2160
 BATCH = 16
 LATENCY_FRAMES = 128
+EXTRAS = ("reference_device", "distances", "learned", "mixed64", "serving")
 PUBLISHED_FPS = 15.0  # reference README.md:17, GTX 1080 Ti, 4K sustained
 HELD_OUT = [(3840, 2160, 0), (1920, 1080, 424242)]  # frames outside the network's training and validation seeds
 P99_TARGET_MS = 8.0  # serving-loop latency target per 4K frame
@@ -456,9 +458,12 @@ def run_ours(args) -> None:
             line["cpu_baseline"] = cpu
 
     extras = rank == 0 and world == 1 and not args.no_extras
-    if extras:
+    want = set(args.extras.split(",")) if extras else set()
+    if "reference_device" in want:
         line["reference_device"] = bench_reference_device(step, args)
+    if "distances" in want:
         line["distances"] = bench_distances(step, nv12, args)
+    if "learned" in want:
         line["learned"] = bench_learned(step, nv12, data, quality, args, local)
     # Torch's allocators record events on the streams their blocks were used
     # on when they are freed, so release every torch object that touched the
@@ -471,8 +476,9 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     for e in encs:
         e.close()
-    if extras:
+    if "mixed64" in want:
         line["mixed64"] = bench_mixed64(args, local, value)
+    if "serving" in want:
         line["serving"] = bench_serving(args, local)
     if line is not None:
         print(json.dumps(line), flush=True)
@@ -782,10 +788,15 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the headline line: skip the distance, learned, batch and serving workloads")
+    ap.add_argument("--extras", default=",".join(EXTRAS),
+                    help="comma-separated subset of the extra workloads to run (default: all of them)")
     ap.add_argument("--streams", type=int, default=8, help="encoders (CUDA streams) per GPU")
     ap.add_argument("--workload", default="4k", choices=["4k", "mixed64"],
                     help="mixed64: the 64-frame uneven-resolution batch as the headline")
     args = ap.parse_args()
+    unknown = set(args.extras.split(",")) - set(EXTRAS)
+    if unknown:
+        ap.error(f"unknown extras {sorted(unknown)}; choose from {list(EXTRAS)}")
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mixed64":
