@@ -9,7 +9,7 @@ Headline (`value`): the seeded synthetic 3840x2160 NV12 frame (seed 0),
 distance 1.0, the plain path (XYB, AQ, gaborish, transform selection, DCT,
 CfL, quantise, histograms, prefix codes, packing, headers). One step encodes
 a batch of 16 device-resident copies of that frame, frame i on encoder i % S
-(S encoders, each with its own CUDA stream and device arena, default 8); the
+(S encoders, each with its own CUDA stream and device arena, default 12); the
 16 distinct input buffers (199 MB) exceed the 126 MB L2, so no step reads its
 input from L2. frames/s over exactly K steps, CUDA events (start on the first
 encoder's stream, the others wait on it and are joined back before the stop
@@ -790,7 +790,7 @@ def main() -> None:
                     help="only the headline line: skip the distance, learned, batch and serving workloads")
     ap.add_argument("--extras", default=",".join(EXTRAS),
                     help="comma-separated subset of the extra workloads to run (default: all of them)")
-    ap.add_argument("--streams", type=int, default=8, help="encoders (CUDA streams) per GPU")
+    ap.add_argument("--streams", type=int, default=12, help="encoders (CUDA streams) per GPU")
     ap.add_argument("--workload", default="4k", choices=["4k", "mixed64"],
                     help="mixed64: the 64-frame uneven-resolution batch as the headline")
     args = ap.parse_args()
