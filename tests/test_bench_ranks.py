@@ -59,3 +59,18 @@ def test_single_rank_needs_no_process_group():
 
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
     assert bench.whole_job_rate(16, 1, 20.0) == 800.0
+
+
+def test_extras_option_rejects_unknown_names():
+    """`--extras` takes a comma-separated subset of the extra workloads and
+    refuses a name outside them before any device work."""
+    import subprocess
+
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--extras", "learned,nosuch"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "unknown extras ['nosuch']" in r.stderr
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    assert set(bench.EXTRAS) == {"reference_device", "distances", "learned", "mixed64", "serving"}
