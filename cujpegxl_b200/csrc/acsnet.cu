@@ -78,10 +78,12 @@ constexpr int kInferThreads = 512;
 constexpr int kX3Off = 0;                          // BF16 offsets inside x1[r]
 constexpr int kX4Off = kX3Off + 64 * kActS;
 constexpr int kOutOff = kX4Off + 16 * kActS;       // FP32 [16][32] from here
+constexpr int kInferX1 = kNetInPix * kNetIn;   // elements per region of x1
+constexpr int kInferX2 = 256 * kActS;          // elements per region of x2
 struct InferSmem {
     NetWeights wt;
-    bf16 x1[4][kNetInPix * kNetIn];
-    bf16 x2[4][256 * kActS];
+    bf16 x1[4][kInferX1];
+    bf16 x2[4][kInferX2];
 };
 
 static_assert(sizeof(NetWeights) % 16 == 0 && sizeof(NetSmem) % 16 == 0 && sizeof(TrainSmem) % 16 == 0,
@@ -303,6 +305,61 @@ __device__ __forceinline__ void fwd_cols(unsigned in, unsigned zero, unsigned w,
         outf[p * kNetC + c + 1] = v1;
         outf[(p + 8) * kNetC + c] = v2;
         outf[(p + 8) * kNetC + c + 1] = v3;
+    }
+}
+
+// L2 of the inference for one position tile `mt` of two regions at once (the
+// regions' L1 outputs in0 and in1, their L2 outputs out0 and out1): each
+// weight fragment loaded serves both regions, which cuts the layer's
+// shared-memory traffic by a third (its ldmatrix traffic bounds it); eight
+// warps cover the tile's four regions.
+__device__ __forceinline__ void fwd_l2_pair(unsigned in0, unsigned in1, unsigned zero, unsigned w, const float* bias,
+                                            bf16* out0, bf16* out1, int mt, int lane) {
+    using Rows = Im2colRows<16, 8, 2, 1, kNetC, kActS, true>;
+    const Rows rows0{in0, mt * 16 + (lane & 15)};
+    const Rows rows1{in1, mt * 16 + (lane & 15)};
+    float acc[2][4][4];
+#pragma unroll
+    for (int i{0}; i < 2; ++i) {
+#pragma unroll
+        for (int n{0}; n < 4; ++n) {
+#pragma unroll
+            for (int j{0}; j < 4; ++j) acc[i][n][j] = 0.0f;
+        }
+    }
+#pragma unroll
+    for (int k0{0}; k0 < kNetK; k0 += 16) {
+        unsigned b[4][2];
+#pragma unroll
+        for (int h{0}; h < 2; ++h) {
+            unsigned r[4];
+            ldsm_x4(r, w + 2u * static_cast<unsigned>((h * 16 + (lane & 7) + ((lane >> 4) << 3)) * kWS + k0 +
+                                                      ((lane >> 3) & 1) * 8));
+            b[2 * h][0] = r[0];
+            b[2 * h][1] = r[1];
+            b[2 * h + 1][0] = r[2];
+            b[2 * h + 1][1] = r[3];
+        }
+#pragma unroll
+        for (int i{0}; i < 2; ++i) {
+            unsigned a[4];
+            ldsm_x4(a, (i == 0 ? rows0 : rows1).at(zero, k0, lane >> 4));
+#pragma unroll
+            for (int n{0}; n < 4; ++n) mma(acc[i][n], a, b[n][0], b[n][1]);
+        }
+    }
+    const int p{mt * 16 + (lane >> 2)};
+#pragma unroll
+    for (int i{0}; i < 2; ++i) {
+        bf16* out{i == 0 ? out0 : out1};
+#pragma unroll
+        for (int n{0}; n < 4; ++n) {
+            const int c{n * 8 + 2 * (lane & 3)};
+            const float b0{bias[c]};
+            const float b1{bias[c + 1]};
+            store_pair(out + p * kActS + c, fmaxf(acc[i][n][0] + b0, 0.0f), fmaxf(acc[i][n][1] + b1, 0.0f));
+            store_pair(out + (p + 8) * kActS + c, fmaxf(acc[i][n][2] + b0, 0.0f), fmaxf(acc[i][n][3] + b1, 0.0f));
+        }
     }
 }
 
@@ -611,7 +668,7 @@ __device__ __forceinline__ void fwd_l1_packed(unsigned in, unsigned w, const flo
 // (training) x1 holds eight channels per pixel and nothing is parity-split.
 template <bool kInfer = false>
 __device__ __forceinline__ void net_forward(const NetWeights& wt, bf16* x1, bf16* x2, bf16* x3, bf16* x4,
-                                            float* out, int warp, int lane) {
+                                            float* out, int warp, int lane, int grp = 0) {
     const unsigned zero{saddr(wt.zero)};
     if constexpr (kInfer) {
         fwd_l1_packed(saddr(x1), saddr(wt.w1), wt.bias[0], x2, warp, lane);
@@ -620,8 +677,20 @@ __device__ __forceinline__ void net_forward(const NetWeights& wt, bf16* x1, bf16
                                                                             wt.bias[0], x2, warp, lane);
     }
     __syncthreads();
-    fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS, kInfer, false>(saddr(x2), zero, saddr(wt.w[0]), wt.bias[1], x3,
-                                                                 warp, lane);
+    if constexpr (kInfer) {
+        // Groups 0 and 1 take regions (0, 1) and (2, 3); the four regions'
+        // buffers lie kInferX1 / kInferX2 elements apart.
+        if (grp < 2) {
+            const int r0{2 * grp};
+            bf16* x2r0{x2 + (r0 - grp) * kInferX2};
+            bf16* x1r0{x1 + (r0 - grp) * kInferX1};
+            fwd_l2_pair(saddr(x2r0), saddr(x2r0 + kInferX2), zero, saddr(wt.w[0]), wt.bias[1], x1r0 + kX3Off,
+                        x1r0 + kInferX1 + kX3Off, warp, lane);
+        }
+    } else {
+        fwd_rows<16, 8, 2, 1, kNetC, kActS, kNetK, kWS, kInfer, false>(saddr(x2), zero, saddr(wt.w[0]), wt.bias[1],
+                                                                     x3, warp, lane);
+    }
     __syncthreads();
     if constexpr (kInfer) {
         fwd_cols_split<8, 2, true>(saddr(x3), zero, saddr(wt.w[1]), wt.bias[2], x4, nullptr,
@@ -863,7 +932,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             if (tid < kNetInW * kRowLanes) {
                 const int x{tid % kNetInW};
                 const auto* cw{reinterpret_cast<const std::uint16_t*>(win_chroma)};
-#pragma unroll 1
+#pragma unroll
                 for (int rx{0}; rx < 2; ++rx) {
                     const int wx{32 * rx + x};
                     const int gx{min(max(px0 - 1 + wx, 0), W - 1)};
@@ -918,7 +987,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             __syncthreads();
             // Groups of regions outside the image run on stale data and
             // their results are dropped.
-            net_forward<true>(s.wt, x1, s.x2[grp], x1 + kX3Off, x1 + kX4Off, o, warp & 3, lane);
+            net_forward<true>(s.wt, x1, s.x2[grp], x1 + kX3Off, x1 + kX4Off, o, warp & 3, lane, grp);
         }
         if ((warp & 3) == 0) {
             const int rx{2 * (t % tw) + (grp & 1)};
