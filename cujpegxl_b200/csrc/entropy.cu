@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 
 #include "entropy.cuh"
@@ -205,6 +206,13 @@ __device__ __forceinline__ void put_bits_at(unsigned int* words, unsigned long l
 // A stripe's inputs in shared memory: the three coefficient planes of its
 // block rows (row stride kRowSlots), the natural orders, strategies and
 // non-zero counts (nzn row 0 is the block row above the stripe).
+// Rows of the zero-density cluster table, padded to 16 bytes.
+constexpr int kZdRow = (kZeroDensityCount + 15) & ~15;
+constexpr int kCoeffCtxBytes = 64 + 64 + 2 * kZdRow;
+// The context tables every stripe CTA stages (layout of StripeStage's
+// nz_ctx .. zd_cluster), filled on each device by entropy_kernels_init.
+__device__ __align__(16) std::uint8_t g_coeff_ctx[kCoeffCtxBytes];
+
 struct StripeStage {
     std::int16_t coef[3][kStripeRows][kRowSlots];
     std::uint16_t order[64 + 256 + 1024];
@@ -213,6 +221,13 @@ struct StripeStage {
     std::int8_t acs[kStripeRows][kAcGroupBlocks];
     std::uint16_t active[kStripeItems];  // items with coefficient tokens
     std::uint32_t aux[kStripeItems];     // per-item bits (bits pass) or bit offset (emit pass)
+    // The coefficient-token context as table lookups (a copy of
+    // g_coeff_ctx): coeff_nz_ctx and coeff_freq_ctx of 1..63, and the
+    // cluster of zero-density context z for luma (row 0) and chroma (row 1)
+    // block contexts.
+    alignas(16) std::uint8_t nz_ctx[64];
+    std::uint8_t freq_ctx[64];
+    std::uint8_t zd_cluster[2][kZdRow];
     int nactive;
 };
 
@@ -256,6 +271,12 @@ __device__ void stage_stripe(const EntropyDev& e, const Stripe& st, const GroupG
             s.nzn[c][r + 1][x] = e.nzn[cb];
             if (r == 0) s.nzn[c][0][x] = st.r0 > 0 ? e.nzn[cb - e.bw] : 0;
         }
+    }
+    static_assert(kCoeffCtxBytes % 16 == 0 && offsetof(StripeStage, zd_cluster) + 2 * kZdRow ==
+                                                   offsetof(StripeStage, nz_ctx) + kCoeffCtxBytes,
+                  "context tables: one contiguous 16-byte-aligned copy");
+    for (int i{tid}; i < kCoeffCtxBytes / 16; i += kAcThreads) {
+        cp_async16(reinterpret_cast<uint4*>(s.nz_ctx) + i, reinterpret_cast<const uint4*>(g_coeff_ctx) + i);
     }
     if (tid == 0) s.nactive = 0;
     cp_async_wait_all();
@@ -332,7 +353,16 @@ __device__ void coeff_tokens(const StripeStage& s, const StripeItem& it, int lan
         std::uint32_t tok{0}, nb{0}, bits{0};
         int cl{0};
         if (has) {
-            cl = context_cluster(coeff_context(bctx, left, k, covered, l2, p));
+            // context_cluster(coeff_context(bctx, left, k, covered, l2, p)):
+            // the context is the block context's zero-density base plus z,
+            // and its cluster depends only on z and luma/chroma. coeff_nz_ctx
+            // is constant from 33 on, so the clamp to 63 changes nothing; z
+            // stays below kZeroDensityCount whenever the item's count is its
+            // non-zeros, and the clamp keeps the lookup in the table otherwise.
+            const std::uint32_t nzi{min((left + covered - 1) >> l2, 63u)};
+            const std::uint32_t z{min((static_cast<std::uint32_t>(s.nz_ctx[nzi]) + s.freq_ctx[k >> l2]) * 2 + p,
+                                      static_cast<std::uint32_t>(kZeroDensityCount - 1))};
+            cl = s.zd_cluster[bctx < 7 ? 0 : 1][z];
             hybrid_uint(pack_signed(val), tok, nb, bits);
         }
         f(has, cl, tok, nb, bits);
@@ -1895,6 +1925,19 @@ bool prefix_code_test(const std::uint32_t* hist, int length, std::uint8_t* depth
 }
 
 bool entropy_kernels_init() {
+    std::uint8_t ctx[kCoeffCtxBytes]{};
+    for (int i{1}; i < 64; ++i) {
+        ctx[i] = static_cast<std::uint8_t>(coeff_nz_ctx(static_cast<std::uint32_t>(i)));
+        ctx[64 + i] = static_cast<std::uint8_t>(coeff_freq_ctx(static_cast<std::uint32_t>(i)));
+    }
+    for (int g{0}; g < 2; ++g) {
+        for (int z{0}; z < kZeroDensityCount; ++z) {
+            // Block context 0 stands for every luma context, 7 for every chroma one.
+            ctx[128 + g * kZdRow + z] = static_cast<std::uint8_t>(context_cluster(
+                static_cast<std::uint32_t>(kNumBlockCtx * kNonZeroBuckets + kZeroDensityCount * (7 * g) + z)));
+        }
+    }
+    if (cudaMemcpyToSymbol(g_coeff_ctx, ctx, sizeof(ctx)) != cudaSuccess) return false;
     return cudaFuncSetAttribute(codes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(sizeof(WarpCodeSmem))) == cudaSuccess &&
            cudaFuncSetAttribute(layout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
