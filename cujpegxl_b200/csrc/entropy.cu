@@ -1698,15 +1698,22 @@ __device__ __forceinline__ void misc_emit_body(const EntropyDev& e, const unsign
 }
 
 // Clears a frame's histograms and counters (the first step of every encode).
-__device__ __forceinline__ void clear_body(const EntropyDev& e) {
-    for (int i{static_cast<int>(threadIdx.x)}; i < kNumClusters * 256; i += blockDim.x) e.ac_hist[i] = 0;
-    for (int i{static_cast<int>(threadIdx.x)}; i < e.ndc * 256; i += blockDim.x) {
+// Zeroes a frame's histograms, first-block counts and token-pool fill; block
+// blk of nblk takes every nblk-th 256-word stretch.
+__device__ __forceinline__ void clear_body(const EntropyDev& e, unsigned blk, unsigned nblk) {
+    const unsigned stride{nblk * blockDim.x};
+    const unsigned t0{blk * blockDim.x + threadIdx.x};
+    for (unsigned i{t0}; i < static_cast<unsigned>(kNumClusters * 256); i += stride) e.ac_hist[i] = 0;
+    for (unsigned i{t0}; i < static_cast<unsigned>(e.ndc) * 256u; i += stride) {
         e.dc_hist[i] = 0;
         e.am_hist[i] = 0;
     }
-    for (int i{static_cast<int>(threadIdx.x)}; i < e.ndc; i += blockDim.x) e.fb_count[i] = 0;
-    if (threadIdx.x == 0) *e.tok_count = 0;
+    for (unsigned i{t0}; i < static_cast<unsigned>(e.ndc); i += stride) e.fb_count[i] = 0;
+    if (t0 == 0) *e.tok_count = 0;
 }
+
+// Blocks of a frame's clear: one per 32 DC groups (8192 histogram words each).
+__host__ __device__ constexpr unsigned clear_blocks(int ndc) { return 1u + static_cast<unsigned>(ndc) / 32u; }
 
 // ---- kernels: one frame per launch, and every frame of a batch per launch -----------
 
@@ -1820,9 +1827,11 @@ JXB_UNSTORED_KERNELS(emit_unstored)
 #undef JXB_UNSTORED_KERNELS
 #undef JXB_ENTROPY_KERNELS
 
-__global__ void __launch_bounds__(256) clear_kernel(const __grid_constant__ EntropyDev e) { clear_body(e); }
+__global__ void __launch_bounds__(256) clear_kernel(const __grid_constant__ EntropyDev e) {
+    clear_body(e, blockIdx.x, gridDim.x);
+}
 __global__ void __launch_bounds__(256) clear_batch_kernel(const __grid_constant__ EntropyBatch b) {
-    clear_body(b.frames[blockIdx.x]);
+    clear_body(b.frames[blockIdx.x], 0u, 1u);
 }
 
 constexpr std::size_t kHistSmem{sizeof(StripeStage) + kNumClusters * kAcSymbols * sizeof(std::uint32_t)};
@@ -1847,7 +1856,7 @@ bool entropy_launch(const EntropyDev& e, void* stream) {
     const unsigned misc{(e.ac_first + kMiscItemsPerBlock - 1) / kMiscItemsPerBlock};
     const unsigned stripes{static_cast<unsigned>(e.nstripes)};
     const std::uint32_t layout_smem{layout_sizes_bytes(e.nsec) + layout_head_bytes(e.nsec)};
-    clear_kernel<<<1, 256, 0, st>>>(e);  // histograms, first-block counts, pool fill
+    clear_kernel<<<clear_blocks(e.ndc), 256, 0, st>>>(e);  // histograms, first-block counts, pool fill
     tokens_kernel<<<stripes + misc, kAcThreads, kHistSmem, st>>>(e);
     codes_kernel<<<kNumClusters + 2 * e.ndc, 32, sizeof(WarpCodeSmem), st>>>(e);
     lengths_kernel<<<stripes + misc, kAcThreads, 0, st>>>(e);
