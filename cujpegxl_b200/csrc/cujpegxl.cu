@@ -420,25 +420,6 @@ bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp
 cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output);
 
 // Waits for the encode and copies the file into `output`.
-cujpegxl_status finish_pageable(cujpegxl_encoder* e, cujpegxl_output* output) {
-    if (cudaMemcpyAsync(e->result_pinned, e->ed.result, 4 * 8, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
-        cudaStreamSynchronize(e->stream) != cudaSuccess) {
-        return CUJPEGXL_INTERNAL_ERROR;
-    }
-    if (e->result_pinned[2] != 0) return CUJPEGXL_INTERNAL_ERROR;
-    const std::size_t total{static_cast<std::size_t>(e->result_pinned[0])};
-    if (total > output->capacity) {
-        output->size = total;
-        return CUJPEGXL_BUFFER_TOO_SMALL;
-    }
-    if (cudaMemcpyAsync(output->data, e->ed.out, total, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
-        cudaStreamSynchronize(e->stream) != cudaSuccess) {
-        return CUJPEGXL_INTERNAL_ERROR;
-    }
-    output->size = total;
-    return CUJPEGXL_OK;
-}
-
 // Non-zero counts of uploaded planes (the frontend computes these itself):
 // per first-block and channel the count over its non-LLF coefficients, and
 // its normalised value at every covered position (src/entropy.cu:686-721).
@@ -526,9 +507,38 @@ bool enqueue_readback(cujpegxl_encoder* e, std::uint8_t* dst, std::size_t capaci
     return cudaGetLastError() == cudaSuccess;
 }
 
+// A pageable output buffer: the file is copied on the device side into the
+// encoder's page-locked NV12 staging buffer (free again once the encode has
+// read its input) behind the encode, so the call waits once, and then to the
+// caller's memory by a host copy; a pageable device-to-host copy would go
+// through the driver's own staging after a second wait. A file larger than
+// the staging buffer is copied from device memory instead.
+cujpegxl_status finish_pageable(cujpegxl_encoder* e, cujpegxl_output* output) {
+    const std::size_t staging{static_cast<std::size_t>(e->config.width) * e->config.height * 3 / 2};
+    if (!enqueue_readback(e, e->nv12_pinned, staging, e->result_pinned, e->stream) ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    if (e->result_pinned[1] == 2) return CUJPEGXL_INTERNAL_ERROR;
+    const std::size_t total{static_cast<std::size_t>(e->result_pinned[0])};
+    if (total > output->capacity) {
+        output->size = total;
+        return CUJPEGXL_BUFFER_TOO_SMALL;
+    }
+    if (e->result_pinned[1] == 0) {
+        std::memcpy(output->data, e->nv12_pinned, total);
+    } else if (cudaMemcpyAsync(output->data, e->ed.out, total, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+               cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        return CUJPEGXL_INTERNAL_ERROR;
+    }
+    output->size = total;
+    return CUJPEGXL_OK;
+}
+
 // Waits for the encode and copies the file into `output`. A page-locked
 // output buffer is written by readback_kernel right behind the encode, so the
-// call waits once; other buffers take the result words first, then the copy.
+// call waits once; other buffers are reached through the encoder's
+// page-locked staging buffer (finish_pageable), also after one wait.
 cujpegxl_status finish(cujpegxl_encoder* e, cujpegxl_output* output) {
     if (!device_reachable_host(output->data)) return finish_pageable(e, output);
     if (!enqueue_readback(e, output->data, output->capacity, e->result_pinned, e->stream) ||
