@@ -266,13 +266,14 @@ class Batch:
         """The frontend schedule the batch's autotuner chose (after the first
         encode): resident CTAs, tiles per claim, dynamic or round-robin
         claims, frame order, whether it came from an earlier batch of the same
-        geometry mix, and its measured batch time."""
+        geometry mix, its measured batch time and the tiles each CTA runs at
+        a time."""
         s = _capi.BatchSchedule()
         check("batch_schedule", self._L.cujpegxl_b200_batch_schedule(self._h, ctypes.byref(s)))
         return {"frontend_ctas": s.frontend_ctas, "tiles_per_claim": s.tiles_per_claim,
                 "claims": "dynamic" if s.dynamic_claims else "round-robin",
                 "order": "largest first" if s.largest_first else "given", "from_cache": bool(s.from_cache),
-                "candidates": s.candidates, "tuned_ms": s.tuned_ms}
+                "candidates": s.candidates, "tuned_ms": s.tuned_ms, "tiles_per_cta": s.tiles_per_cta}
 
     def stream(self) -> int:
         s = ctypes.c_size_t(0)

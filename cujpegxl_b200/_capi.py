@@ -76,7 +76,8 @@ class NetBatch(ctypes.Structure):
 class BatchSchedule(ctypes.Structure):
     _fields_ = [("frontend_ctas", ctypes.c_uint32), ("tiles_per_claim", ctypes.c_uint32),
                 ("dynamic_claims", ctypes.c_uint32), ("largest_first", ctypes.c_uint32),
-                ("from_cache", ctypes.c_uint32), ("candidates", ctypes.c_uint32), ("tuned_ms", ctypes.c_float)]
+                ("from_cache", ctypes.c_uint32), ("candidates", ctypes.c_uint32), ("tuned_ms", ctypes.c_float),
+                ("tiles_per_cta", ctypes.c_uint32)]
 
 
 class DevicePlanes(ctypes.Structure):

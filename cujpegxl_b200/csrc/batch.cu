@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -64,9 +65,11 @@ bool same_inputs(const std::vector<cujpegxl_nv12_input>& a, const cujpegxl_nv12_
     return true;
 }
 
-// The frontend launch schedule the autotuner chooses among.
+// The frontend launch schedule the autotuner chooses among: CTAs of two
+// tiles at a time (paired, one per SM) or of one tile (ctas_per_sm per SM).
 struct Schedule {
-    int ctas_per_sm{2};
+    bool paired{true};
+    int ctas_per_sm{1};
     int chunk{1};
     bool dynamic{true};
     bool largest_first{true};
@@ -153,7 +156,7 @@ bool capture(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, const Sc
         eb->nframes = static_cast<int>(n);
         jxb::entropy_batch_plan(*eb);
         ok = (!sc.dynamic || cudaMemsetAsync(fb->counter, 0, sizeof(std::uint32_t), b->root) == cudaSuccess) &&
-             jxb::frontend_batch_launch(*fb, sc.ctas_per_sm * b->sms, b->root) &&
+             jxb::frontend_batch_launch(*fb, sc.ctas_per_sm * b->sms, sc.paired, b->root) &&
              jxb::entropy_batch_launch(*eb, b->root);
     }
     delete fb;
@@ -185,6 +188,15 @@ bool instantiate(cujpegxl_b200_batch* b, const cujpegxl_nv12_input* inputs, cons
     return ok;
 }
 
+// The CTA shape the environment restricts the candidates to, if any
+// (CUJPEGXL_B200_BATCH_TILES_PER_CTA = 1 or 2), so that tests can check both
+// shapes' output; 0 otherwise.
+int forced_tiles_per_cta() {
+    const char* v{std::getenv("CUJPEGXL_B200_BATCH_TILES_PER_CTA")};
+    if (v == nullptr) return 0;
+    return std::strcmp(v, "1") == 0 ? 1 : (std::strcmp(v, "2") == 0 ? 2 : 0);
+}
+
 std::vector<std::uint64_t> cache_key(const cujpegxl_b200_batch* b) {
     std::vector<std::uint64_t> key{static_cast<std::uint64_t>(b->device)};
     for (cujpegxl_encoder* e : b->encs) {
@@ -192,19 +204,24 @@ std::vector<std::uint64_t> cache_key(const cujpegxl_b200_batch* b) {
         key.push_back((static_cast<std::uint64_t>(ed.width) << 32) | static_cast<std::uint64_t>(ed.height));
     }
     key.push_back(jxb::encoder_has_network(b->encs.front()) ? 1u : 0u);
+    key.push_back(static_cast<std::uint64_t>(forced_tiles_per_cta()));
     return key;
 }
 
-// The candidates: dynamic claims of 1, 2 or 4 tiles with one or two CTAs per
-// SM, and round-robin claims of single tiles with two, each with the frames
-// largest-first and in the given order.
+// The candidates: paired CTAs (one per SM, two tiles at a time) and
+// single-tile CTAs (two per SM), each with dynamic claims of 1, 2 or 4 tiles
+// (per half, when paired) or round-robin claims of single tiles, and the
+// frames largest-first or in the given order.
 std::vector<Schedule> candidates() {
+    const int forced{forced_tiles_per_cta()};
     std::vector<Schedule> out;
     for (const bool largest : {true, false}) {
-        for (const int per_sm : {2, 1}) {
-            for (const int chunk : {1, 2, 4}) out.push_back(Schedule{per_sm, chunk, true, largest, 0.0f});
+        for (const bool paired : {true, false}) {
+            if (forced != 0 && forced != (paired ? 2 : 1)) continue;
+            const int per_sm{paired ? 1 : 2};
+            for (const int chunk : {1, 2, 4}) out.push_back(Schedule{paired, per_sm, chunk, true, largest, 0.0f});
+            out.push_back(Schedule{paired, per_sm, 1, false, largest, 0.0f});
         }
-        out.push_back(Schedule{2, 1, false, largest, 0.0f});
     }
     return out;
 }
@@ -439,6 +456,7 @@ cujpegxl_status cujpegxl_b200_batch_schedule(const cujpegxl_b200_batch* batch,
                                              cujpegxl_b200_batch_schedule_info* out) {
     if (batch == nullptr || out == nullptr || !batch->tuned) return CUJPEGXL_INVALID_ARGUMENT;
     out->frontend_ctas = static_cast<uint32_t>(batch->schedule.ctas_per_sm * batch->sms);
+    out->tiles_per_cta = batch->schedule.paired ? 2u : 1u;
     out->tiles_per_claim = static_cast<uint32_t>(batch->schedule.chunk);
     out->dynamic_claims = batch->schedule.dynamic ? 1u : 0u;
     out->largest_first = batch->schedule.largest_first ? 1u : 0u;

@@ -114,6 +114,20 @@ constexpr std::size_t kSmemBytes =
     sizeof(float) * (kRegionAFloats + 3 * kSplane) + sizeof(Small);
 // Two CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA.
 static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two frontend CTAs no longer fit on one SM");
+// One tile's shared memory, rounded to 16 bytes: the single-frame kernel runs
+// two tiles per CTA, one per half of its threads, at this stride.
+constexpr std::size_t kTileSmemStride = (kSmemBytes + 15) / 16 * 16;
+// The single-frame kernel's CTA: two tiles of kThreads threads each, all of
+// an SM's shared memory (227 KB per CTA at most).
+constexpr int kPairThreads = 2 * kThreads;
+static_assert(2 * kTileSmemStride <= 227 * 1024, "two tiles no longer fit in one CTA");
+
+// Synchronises the kThreads threads of one tile on named barrier `bar` (1 or
+// 2; barrier 0 is __syncthreads), with the ordering of shared memory that
+// __syncthreads gives.
+__device__ __forceinline__ void tile_sync(int bar) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(kThreads) : "memory");
+}
 
 // Chroma window of a tile in shared memory: kChromaWin x kChromaWin (cb, cr)
 // pairs starting kChromaMargin chroma samples before the tile's first.
@@ -490,7 +504,7 @@ __device__ __forceinline__ void llf_to_dc(const __half* coef, int f, int ox, int
 // the CTA starts another tile.
 __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const FrontendScalars& sc,
                                               const FrontendTables& tb, const FrontendOutputs& out, int tx,
-                                              int ty, float* smem) {
+                                              int ty, float* smem, int bar) {
     // Region A: the XYB planes, later the selection and final-DCT row
     // scratch. Region B: the sharpened planes, later the FP16 coefficients
     // and the NV12 window before both.
@@ -498,7 +512,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
     float* shp{smem + kRegionAFloats};               // [3][64*kSs]
     Small& sm{*reinterpret_cast<Small*>(smem + kRegionAFloats + 3 * kSplane)};
 
-    const int tid{static_cast<int>(threadIdx.x)};
+    const int tid{static_cast<int>(threadIdx.x) & (kThreads - 1)};
     const int lane{tid & 31};
     const int warp{tid >> 5};
     const int W{in.width};
@@ -632,7 +646,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             if (tid == k) sm.pow_lut[k] = make_float2(pow24_factor_c(k), pow24_factor_scale(k));
         }
     }
-    __syncthreads();
+    tile_sync(bar);
     // Regions whose transform split (and, with net_qf, quant field) the
     // network decided; zero without a network.
     unsigned dmask{0};
@@ -657,7 +671,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
         *reinterpret_cast<float2*>(xyb + kXplane + i) = y;
         *reinterpret_cast<float2*>(xyb + 2 * kXplane + i) = b;
     }
-    __syncthreads();
+    tile_sync(bar);
 
     if (out.dbg_xyb != nullptr) {
         for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
@@ -724,7 +738,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             }
             sm.pre[tid] = 0.25f * sum;
         }
-        __syncthreads();
+        tile_sync(bar);
         // The four eroded cells of each of this warp's 8 blocks (block warp + 8j),
         // one per lane: lane 4j + k holds cell k = (k & 1, k >> 1) of block j's
         // 2x2 cells. Their sum (e0 + e2) + (e1 + e3) is the order in which a
@@ -840,7 +854,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             *reinterpret_cast<float2*>(shp + c * kSplane + (y0 + h) * kSs + x) = sv;
         }
     }
-    __syncthreads();
+    tile_sync(bar);
 
     if (out.dbg_sharp != nullptr) {
         for (int i{tid}; i < 3 * kTile * kTile; i += kThreads) {
@@ -879,7 +893,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                 row_pass<8, 0, 8, true>(SY + (lby * 8 + r) * kSs + lbx * 8, rows + lb * 72 + r);
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         for (int k{tid}; k < 512; k += kThreads) {
             const int lb{k >> 3};
             const int fx{k & 7};
@@ -889,7 +903,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                                  crate + lb * 72 + fx * 9, fx, qg, tb.sel_weight, tb.log2_1p, sm.log2_small);
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         // Distortion and rate ride one packed pair through each step.
 #pragma unroll 2
         for (int lb{warp}; lb < 64; lb += kThreads / 32) {
@@ -917,7 +931,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                 row_pass<16, 0, 16, true>(SY + (qy * 16 + r) * kSs + qx * 16, rows + qd * 272 + r);
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         for (int k{tid}; k < 256; k += kThreads) {
             const int qd{k >> 4};
             const int fx{k & 15};
@@ -928,7 +942,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                                    tb.log2_1p, sm.log2_small);
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         for (int qd{warp}; qd < 16; qd += kThreads / 32) {
             if (bx0 + 2 * (qd & 3) + 2 <= bw && by0 + 2 * (qd >> 2) + 2 <= bh &&
                 ((dmask >> (((qd >> 3) << 1) | ((qd & 3) >> 1))) & 1u) == 0) {
@@ -970,7 +984,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                 }
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         for (int k{tid}; k < 256; k += kThreads) {
             const int ri{k >> 6};
             const int fx{k & 31};
@@ -987,7 +1001,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
                 }
             }
         }
-        __syncthreads();
+        tile_sync(bar);
         if (warp < 4) {
             const int ri{warp};
             if (bx0 + 4 * (ri & 1) + 4 <= bw && by0 + 4 * (ri >> 1) + 4 <= bh &&
@@ -1142,7 +1156,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             sm.qf[lb] = qi;
         }
     }
-    __syncthreads();
+    tile_sync(bar);
     if (out.dbg_cost != nullptr) {
         for (int lb{tid}; lb < 64; lb += kThreads) {
             const int lbx{lb & 7};
@@ -1212,7 +1226,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             off += cnt * step;
         }
     }
-    __syncthreads();
+    tile_sync(bar);
 
     // ---- 5. variable DCT of X, Y, B -> FP16 coefficients (src/frontend_transform.cu:190-266).
     // The three channels' row passes run in one phase (each channel has its
@@ -1254,7 +1268,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             row_pass<8, 0, 8, false>(P + ((lb >> 3) * 8 + r) * kSs + (lb & 7) * 8, drows + sm.fb_off[f] + r);
         }
     }
-    __syncthreads();
+    tile_sync(bar);
     for (int k3{tid}; k3 < 3 * tall; k3 += kThreads) {
         const int c{k3 >= 2 * tall ? 2 : (k3 >= tall ? 1 : 0)};
         const int k{k3 - c * tall};
@@ -1282,7 +1296,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             dct_col<8, 0, 8>(drows + sm.fb_off[f] + fx * 9, cc, fx, lb & 7, lb >> 3);
         }
     }
-    __syncthreads();
+    tile_sync(bar);
 
     if (out.dbg_coeff != nullptr) {
         for (int i{tid}; i < 3 * 4096; i += kThreads) {
@@ -1344,7 +1358,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             out.dc[2 * static_cast<std::size_t>(nblocks) + blk] = static_cast<int>(lrintf((dcv[2] - ydr) * dcq_b));
         }
     }
-    __syncthreads();
+    tile_sync(bar);
     // The tile's maps: every warp reduces the 64 partials itself (the same
     // tree, so the same maps on every warp) instead of waiting at one more
     // barrier for warp 0 to do it. The trees leave the sums in lane 0, which
@@ -1475,7 +1489,7 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
             if (cb) atomicAdd(&sm.nz[2][f], static_cast<int>(cb));
         }
     }
-    __syncthreads();
+    tile_sync(bar);
 
     // ---- 8. side information.
     for (int k{tid}; k < 64; k += kThreads) {
@@ -1502,10 +1516,21 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+// Tiles (2 blockIdx.x, blockIdx.y) and (2 blockIdx.x + 1, blockIdx.y), one per
+// half of the CTA, each half on its own named barrier. The two tiles start
+// together and run the same code at about the same time, so each instruction
+// fetch serves the warps of both; as two CTAs per SM (each one tile at its
+// own point of the long unrolled code) the tiles' instruction fetches
+// competed, and a DCT32 selection row pass took about 7K cycles against
+// 2.9K when its code was still cached.
+__global__ void __launch_bounds__(kPairThreads, 1)
     frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
     extern __shared__ __align__(16) float smem[];
-    frontend_tile(in, sc, tb, out, static_cast<int>(blockIdx.x), static_cast<int>(blockIdx.y), smem);
+    const int half{static_cast<int>(threadIdx.x) / kThreads};
+    const int tx{2 * static_cast<int>(blockIdx.x) + half};
+    if (tx * kTile >= in.width) return;  // the right half of an odd tile row: no barrier waits on it
+    frontend_tile(in, sc, tb, out, tx, static_cast<int>(blockIdx.y), smem + half * (kTileSmemStride / sizeof(float)),
+                  1 + half);
 }
 
 // One tile of a batched launch, kept out of line: inlined into the work loop,
@@ -1516,8 +1541,17 @@ __global__ void __launch_bounds__(kThreads, 2)
 // batch: 1653 -> 1732 frames/s). The frame and tables are passed by value
 // (read from the call's copy, not through a pointer into the parameter
 // block): 1.8% fewer cycles per tile.
-__device__ __noinline__ void batch_tile(const FrontendJob j, const FrontendTables tb, int local, float* smem) {
-    frontend_tile(j.in, j.sc, tb, j.out, local % j.tiles_x, local / j.tiles_x, smem);
+__device__ __noinline__ void batch_tile(const FrontendJob j, const FrontendTables tb, int local, float* smem,
+                                       int bar) {
+    frontend_tile(j.in, j.sc, tb, j.out, local % j.tiles_x, local / j.tiles_x, smem, bar);
+}
+
+// The frame of work-list item `item` and the item's tile within it.
+__device__ __forceinline__ void batch_item(const FrontendBatch& b, std::uint32_t item, float* smem, int bar) {
+    int f{0};
+    while (f + 1 < b.nframes && b.jobs[f + 1].tile_begin <= item) ++f;
+    const FrontendJob& j{b.jobs[f]};
+    batch_tile(j, b.tb, static_cast<int>(item - j.tile_begin), smem, bar);
 }
 
 // Frames of a batch as one work list of tiles (frame j's tiles are items
@@ -1542,12 +1576,43 @@ __global__ void __launch_bounds__(kThreads, 2) frontend_batch_kernel(const __gri
         if (first >= b.total_tiles) break;
         const std::uint32_t last{min(first + chunk, b.total_tiles)};
         for (std::uint32_t item{first}; item < last; ++item) {
-            int f{0};
-            while (f + 1 < b.nframes && b.jobs[f + 1].tile_begin <= item) ++f;
-            const FrontendJob& j{b.jobs[f]};
-            batch_tile(j, b.tb, static_cast<int>(item - j.tile_begin), smem);
+            batch_item(b, item, smem, 1);
             __syncthreads();
         }
+    }
+}
+
+// The same work list taken two chunks at a time: half h of the CTA runs
+// chunk h of each claim on its own tile memory and named barrier, so that,
+// as in the single-frame kernel, two tiles run the same code together; both
+// halves finish a claim before the next.
+__global__ void __launch_bounds__(kPairThreads, 1)
+    frontend_batch_pair_kernel(const __grid_constant__ FrontendBatch b) {
+    extern __shared__ __align__(16) float smem[];
+    const int half{static_cast<int>(threadIdx.x) / kThreads};
+    float* tile_smem{smem + half * (kTileSmemStride / sizeof(float))};
+    // The claim word is half 0's Small::n32; it is read before either tile
+    // starts and written again only after both have finished.
+    Small& sm{*reinterpret_cast<Small*>(smem + kRegionAFloats + 3 * kSplane)};
+    const std::uint32_t chunk{static_cast<std::uint32_t>(b.chunk)};
+    for (std::uint32_t round{0};; ++round) {
+        std::uint32_t first;
+        if (b.counter != nullptr) {
+            if (threadIdx.x == 0) sm.n32 = static_cast<int>(atomicAdd(b.counter, 2 * chunk));
+            __syncthreads();
+            first = static_cast<std::uint32_t>(sm.n32);
+            __syncthreads();
+        } else {
+            first = (round * gridDim.x + blockIdx.x) * 2 * chunk;
+        }
+        if (first >= b.total_tiles) break;
+        const std::uint32_t mine{first + static_cast<std::uint32_t>(half) * chunk};
+        const std::uint32_t last{min(mine + chunk, b.total_tiles)};
+        for (std::uint32_t item{mine}; item < last; ++item) {
+            batch_item(b, item, tile_smem, 1 + half);
+            tile_sync(1 + half);
+        }
+        __syncthreads();
     }
 }
 
@@ -1704,22 +1769,29 @@ bool frontend_tables_init(FrontendTables* tables) {
     tables->log2_1p = d_l2;
     tables->llf_basis = d_ob;
     return cudaFuncSetAttribute(frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kSmemBytes)) == cudaSuccess &&
+                                static_cast<int>(2 * kTileSmemStride)) == cudaSuccess &&
            cudaFuncSetAttribute(frontend_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(kSmemBytes)) == cudaSuccess;
+                                static_cast<int>(kSmemBytes)) == cudaSuccess &&
+           cudaFuncSetAttribute(frontend_batch_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(2 * kTileSmemStride)) == cudaSuccess;
 }
 
 bool frontend_launch(const FrontendInputs& in, const FrontendScalars& s, const FrontendTables& t,
                      const FrontendOutputs& out, void* stream) {
-    const dim3 grid{static_cast<unsigned>((in.width + kTile - 1) / kTile),
-                    static_cast<unsigned>((in.height + kTile - 1) / kTile)};
-    frontend_kernel<<<grid, kThreads, kSmemBytes, static_cast<cudaStream_t>(stream)>>>(in, s, t, out);
+    const int tiles_x{(in.width + kTile - 1) / kTile};
+    const dim3 grid{static_cast<unsigned>((tiles_x + 1) / 2), static_cast<unsigned>((in.height + kTile - 1) / kTile)};
+    frontend_kernel<<<grid, kPairThreads, 2 * kTileSmemStride, static_cast<cudaStream_t>(stream)>>>(in, s, t, out);
     return cudaGetLastError() == cudaSuccess;
 }
 
-bool frontend_batch_launch(const FrontendBatch& b, int ctas, void* stream) {
+bool frontend_batch_launch(const FrontendBatch& b, int ctas, bool paired, void* stream) {
     if (b.nframes <= 0 || b.nframes > kBatchFrames || ctas <= 0 || b.chunk <= 0) return false;
-    frontend_batch_kernel<<<static_cast<unsigned>(ctas), kThreads, kSmemBytes, static_cast<cudaStream_t>(stream)>>>(b);
+    cudaStream_t st{static_cast<cudaStream_t>(stream)};
+    if (paired) {
+        frontend_batch_pair_kernel<<<static_cast<unsigned>(ctas), kPairThreads, 2 * kTileSmemStride, st>>>(b);
+    } else {
+        frontend_batch_kernel<<<static_cast<unsigned>(ctas), kThreads, kSmemBytes, st>>>(b);
+    }
     return cudaGetLastError() == cudaSuccess;
 }
 

@@ -103,10 +103,9 @@ struct FrontendBatch {
     FrontendJob jobs[kBatchFrames];
 };
 
-// Launches `ctas` resident CTAs that run every tile of every frame in `b`.
-bool frontend_batch_launch(const FrontendBatch& b, int ctas, void* stream);
-
-// Frontend CTAs resident per SM (its launch bounds and shared memory).
-constexpr int kFrontendCtasPerSm = 2;
+// Launches `ctas` resident CTAs that run every tile of every frame in `b`:
+// paired, CTAs of two tiles at a time (one per half, claimed together; one
+// CTA per SM), else CTAs of one tile at a time (two per SM).
+bool frontend_batch_launch(const FrontendBatch& b, int ctas, bool paired, void* stream);
 
 }  // namespace jxb

@@ -227,9 +227,11 @@ uint32_t cujpegxl_b200_batch_lanes(const cujpegxl_b200_batch* batch);
 
 /* The frontend schedule the batch's autotuner chose on its first encode (or
  * took from an earlier batch of the same geometry mix): resident CTAs of the
- * persistent frontend launch, tiles per claim, claims from a counter (1) or
- * round-robin (0), frames largest-first (1) or in the given order (0), and
- * the measured time of one batch with it. */
+ * persistent frontend launch, tiles per claim (per tile slot of a CTA), claims
+ * from a counter (1) or round-robin (0), frames largest-first (1) or in the
+ * given order (0), the measured time of one batch with it, and the tiles
+ * each CTA runs at a time (2: one per half of a 512-thread CTA, claimed
+ * together; 1: 256-thread CTAs). */
 typedef struct cujpegxl_b200_batch_schedule_info {
     uint32_t frontend_ctas;
     uint32_t tiles_per_claim;
@@ -238,6 +240,7 @@ typedef struct cujpegxl_b200_batch_schedule_info {
     uint32_t from_cache;
     uint32_t candidates;
     float tuned_ms;
+    uint32_t tiles_per_cta;
 } cujpegxl_b200_batch_schedule_info;
 cujpegxl_status cujpegxl_b200_batch_schedule(const cujpegxl_b200_batch* batch,
                                              cujpegxl_b200_batch_schedule_info* out);

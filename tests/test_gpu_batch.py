@@ -55,7 +55,7 @@ def test_batch_matches_single_encoders_across_relaunch_and_rebinding():
         sched = batch.schedule()
         assert batch.lanes == 1
         assert sched["frontend_ctas"] > 0 and sched["tiles_per_claim"] in (1, 2, 4)
-        assert sched["candidates"] >= 8 and sched["tuned_ms"] > 0
+        assert sched["candidates"] >= 8 and sched["tuned_ms"] > 0 and sched["tiles_per_cta"] in (1, 2)
     w, h, d = FRAMES[2]
     assert expected_a[2] == api.encode(nvs_a[2], w, h, d)
     # A second batch of the same geometry mix takes the tuned schedule from
@@ -65,6 +65,26 @@ def test_batch_matches_single_encoders_across_relaunch_and_rebinding():
         assert again.sync() == [len(x) for x in expected_a]
         assert [again.read(i) for i in range(len(FRAMES))] == expected_a
         assert again.schedule()["from_cache"]
+
+
+@pytest.mark.parametrize("tiles_per_cta", [1, 2])
+def test_batch_matches_single_encoders_with_each_cta_shape(monkeypatch, tiles_per_cta):
+    # Every candidate the autotuner may choose among runs one of the two
+    # persistent frontend kernels (two tiles per 512-thread CTA, or one per
+    # 256-thread CTA); restricting the candidates to one shape checks that
+    # kernel's files byte for byte.
+    monkeypatch.setenv("CUJPEGXL_B200_BATCH_TILES_PER_CTA", str(tiles_per_cta))
+    keep, inputs, nvs = _inputs(300)
+    expected = [_single(nv, w, h, d) for nv, (w, h, d) in zip(nvs, FRAMES)]
+    with Batch(FRAMES) as batch:
+        for _ in range(2):
+            batch.encode(inputs)
+            assert batch.sync() == [len(x) for x in expected]
+            for i, x in enumerate(expected):
+                assert batch.read(i) == x
+        sched = batch.schedule()
+        assert sched["tiles_per_cta"] == tiles_per_cta
+        assert sched["candidates"] == 8
 
 
 def test_batch_of_more_frames_than_one_launch_takes():
