@@ -139,8 +139,8 @@ typedef struct cujpegxl_b200_device_planes {
  *  - Frames above 4,194,304 pixels (width*height) are rejected with
  *    CUJPEGXL_UNSUPPORTED_RESOLUTION; other geometry rules are those of
  *    cujpegxl_encoder_create.
- *  - The first call on a device looks up the array's device address and sets
- *    kernel attributes; make that first call before any stream capture.
+ *  - The first call on a device also looks up the array's device address and
+ *    sets kernel attributes (host runtime calls that later calls skip).
  *  - Calls share the array: calls that overlap on the GPU (different streams
  *    or threads without ordering) race and corrupt each other's output.
  *  - Work is enqueued on `stream` (a cudaStream_t as an integer, 0 for the
