@@ -112,7 +112,8 @@ __device__ __forceinline__ int region_of_block(int lb) { return ((lb >> 5) << 1)
 
 constexpr std::size_t kSmemBytes =
     sizeof(float) * (kRegionAFloats + 3 * kSplane) + sizeof(Small);
-// Two CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA.
+// The batch kernel's single-tile CTAs run two per SM: 228 KB of shared
+// memory, 1 KB of it reserved per CTA.
 static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two frontend CTAs no longer fit on one SM");
 // One tile's shared memory, rounded to 16 bytes: the single-frame kernel runs
 // two tiles per CTA, one per half of its threads, at this stride.
