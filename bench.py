@@ -790,13 +790,16 @@ def main() -> None:
                     help="only the headline line: skip the distance, learned, batch and serving workloads")
     ap.add_argument("--extras", default=",".join(EXTRAS),
                     help="comma-separated subset of the extra workloads to run (default: all of them)")
-    ap.add_argument("--streams", type=int, default=12, help="encoders (CUDA streams) per GPU")
+    ap.add_argument("--streams", type=int, default=12,
+                    help=f"encoders (CUDA streams) per GPU, 1..{BATCH} (each takes frames of the {BATCH}-frame step)")
     ap.add_argument("--workload", default="4k", choices=["4k", "mixed64"],
                     help="mixed64: the 64-frame uneven-resolution batch as the headline")
     args = ap.parse_args()
     unknown = set(args.extras.split(",")) - set(EXTRAS)
     if unknown:
         ap.error(f"unknown extras {sorted(unknown)}; choose from {list(EXTRAS)}")
+    if not 1 <= args.streams <= BATCH:
+        ap.error(f"--streams must be 1..{BATCH}, got {args.streams}")
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mixed64":

@@ -74,3 +74,14 @@ def test_extras_option_rejects_unknown_names():
     import bench
 
     assert set(bench.EXTRAS) == {"reference_device", "distances", "learned", "mixed64", "serving"}
+
+
+def test_streams_option_is_bounded_by_the_step():
+    """Every encoder stream takes its own frames of the step, so `--streams`
+    above the step's frame count is refused before any device work."""
+    import subprocess
+
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--streams", "24"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "--streams must be 1..16, got 24" in r.stderr
