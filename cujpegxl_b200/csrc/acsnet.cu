@@ -851,6 +851,10 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     const int warp{tid >> 5};
     const int lane{tid & 31};
     const int grp{warp >> 2};
+    // Set when a region of the current tile inside the image is left to the
+    // heuristic (its tile goes to the back of out.tile_order).
+    __shared__ unsigned sh_heuristic;
+    if (tid == 0) sh_heuristic = 0;
     load_net(s.wt, p, tid, kInferThreads);
     __syncthreads();
     pack_w1(s.wt, p, tid, kInferThreads);
@@ -998,13 +1002,26 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                     const SplitHead h{split_head(split_logit(o, lane))};
                     cls = h.margin >= margin ? h.top : -1;
                 }
-                if (lane == 0) out.cls[ry * rw + rx] = static_cast<std::int8_t>(cls);
+                if (lane == 0) {
+                    out.cls[ry * rw + rx] = static_cast<std::int8_t>(cls);
+                    if (cls < 0) atomicOr(&sh_heuristic, 1u);
+                }
                 if (cls >= 0 && out.qf != nullptr && lane < 16) {
                     // fmaxf maps a NaN to 1.
                     const float q{fminf(fmaxf(rintf(exp2f(o[lane * kNetC])), 1.0f), static_cast<float>(kQuantMax))};
                     out.qf[static_cast<std::size_t>(ry * 4 + (lane >> 2)) * bw + rx * 4 + (lane & 3)] =
                         static_cast<std::int16_t>(static_cast<int>(q));
                 }
+            }
+        }
+        if (out.tile_order != nullptr) {  // the same for every thread
+            __syncthreads();  // every region's flag is in
+            if (tid == 0) {
+                const unsigned n{static_cast<unsigned>(ntiles)};
+                const unsigned at{sh_heuristic == 0 ? atomicAdd(&out.tile_order[n], 1u)
+                                                    : n - 1u - atomicAdd(&out.tile_order[n + 1], 1u)};
+                out.tile_order[at] = static_cast<std::uint32_t>(t);
+                sh_heuristic = 0;
             }
         }
     }
@@ -1265,6 +1282,11 @@ bool acsnet_infer_launch(const FrontendInputs& in, const NetParamsDev& p, float 
                          const NetDecisionsDev& out, void* stream) {
     const int ntiles{((in.width + 63) >> 6) * ((in.height + 63) >> 6)};
     const int grid{ntiles < sm_count() ? ntiles : sm_count()};
+    if (out.tile_order != nullptr &&
+        cudaMemsetAsync(out.tile_order + ntiles, 0, 2 * sizeof(std::uint32_t), static_cast<cudaStream_t>(stream)) !=
+            cudaSuccess) {
+        return false;
+    }
     acsnet_infer_kernel<<<grid, kInferThreads, sizeof(InferSmem), static_cast<cudaStream_t>(stream)>>>(
         in, p, log2_distance, margin, out);
     return cudaGetLastError() == cudaSuccess;

@@ -79,6 +79,10 @@ struct NetBatchDev {
 struct NetDecisionsDev {
     std::int8_t* cls;    // [rh][rw] split class, -1 where the heuristic decides
     std::int16_t* qf;    // [bh][bw] quant field of blocks in decided regions
+    // Null, or [ntiles + 2]: the raster indices of the 64x64 tiles, those
+    // whose regions inside the image are all decided from the front, the
+    // others from the back (the last two words count them).
+    std::uint32_t* tile_order;
 };
 
 struct FrontendInputs;

@@ -56,6 +56,7 @@ struct cujpegxl_encoder {
     float net_margin{0.2f};
     std::uint32_t net_flags{0};
     std::int8_t* net_class{nullptr};
+    std::uint32_t* tile_order{nullptr};  // [64x64 tiles + 2], written by the inference kernel
     std::int16_t* net_qf{nullptr};
     bool allow_single{false};  // created with CUJPEGXL_B200_ENCODER_SINGLE_GROUP
 };
@@ -258,6 +259,7 @@ bool allocate(cujpegxl_encoder* e) {
     const std::size_t o_nv12{a.take(static_cast<std::size_t>(W) * H * 3 / 2)};
     const std::size_t o_ncls{a.take(((bw + 3) / 4) * ((bh + 3) / 4))};
     const std::size_t o_nqf{a.take(nb * 2)};
+    const std::size_t o_tord{a.take((nt + 2) * 4)};
     std::size_t o_dbg{0};
     if (e->debug) {
         o_dbg = a.take(2 * 3 * static_cast<std::size_t>(W) * H * 4 + 3 * nb * 64 * 2 + 3 * nb * 4);
@@ -351,6 +353,7 @@ bool allocate(cujpegxl_encoder* e) {
     e->nv12_dev = b + o_nv12;
     e->net_class = reinterpret_cast<std::int8_t*>(b + o_ncls);
     e->net_qf = reinterpret_cast<std::int16_t*>(b + o_nqf);
+    e->tile_order = reinterpret_cast<std::uint32_t*>(b + o_tord);
 
     bool ok{cudaMemcpy(b + o_sec, plan.sections.data(), plan.sections.size() * sizeof(jxb::Section),
                        cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -402,16 +405,18 @@ bool enqueue_frame(cujpegxl_encoder* e, const std::uint8_t* luma, std::size_t lp
     jxb::FrontendTables ft{};
     if (!device_tables(e->device, &ft)) return false;
     jxb::FrontendInputs in{luma, chroma, lp, cp, static_cast<int>(e->config.width),
-                           static_cast<int>(e->config.height), nullptr, nullptr};
+                           static_cast<int>(e->config.height), nullptr, nullptr, nullptr};
     cudaStream_t st{stream != nullptr ? stream : e->stream};
     if ((stages & 1u) && e->net != nullptr) {
-        const jxb::NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr};
+        const jxb::NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr,
+                                       e->tile_order};
         if (!jxb::acsnet_infer_launch(in, *jxb::acsnet_params(e->net), std::log2(e->config.distance),
                                       e->net_margin, dec, st)) {
             return false;
         }
         in.net_class = dec.cls;
         in.net_qf = dec.qf;
+        in.tile_order = dec.tile_order;
     }
     if ((stages & 1u) && !jxb::frontend_launch(in, e->fs, ft, e->fo, st)) return false;
     return (stages & 2u) == 0 || jxb::entropy_launch(e->ed, st);
@@ -573,9 +578,11 @@ bool encoder_frontend_job(cujpegxl_encoder* e, const cujpegxl_nv12_input& input,
     if (!device_tables(e->device, tables)) return false;
     FrontendInputs in{reinterpret_cast<const std::uint8_t*>(input.luma), reinterpret_cast<const std::uint8_t*>(input.chroma),
                       input.luma_pitch, input.chroma_pitch, static_cast<int>(e->config.width),
-                      static_cast<int>(e->config.height), nullptr, nullptr};
+                      static_cast<int>(e->config.height), nullptr, nullptr, nullptr};
     if (e->net != nullptr) {
-        const NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr};
+        // The batched frontend takes tiles from its own work list.
+        const NetDecisionsDev dec{e->net_class, (e->net_flags & CUJPEGXL_B200_ACSNET_QF) ? e->net_qf : nullptr,
+                                  nullptr};
         if (!acsnet_infer_launch(in, *acsnet_params(e->net), std::log2(e->config.distance), e->net_margin, dec,
                                  stream)) {
             return false;

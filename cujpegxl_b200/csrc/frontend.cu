@@ -1524,14 +1524,29 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
 // own point of the long unrolled code) the tiles' instruction fetches
 // competed, and a DCT32 selection row pass took about 7K cycles against
 // 2.9K when its code was still cached.
+// kOrdered: the tiles come from in.tile_order (a separate instantiation, so
+// that the kernel without the order compiles as it did before it existed).
+template <bool kOrdered>
 __global__ void __launch_bounds__(kPairThreads, 1)
     frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
     extern __shared__ __align__(16) float smem[];
     const int half{static_cast<int>(threadIdx.x) / kThreads};
-    const int tx{2 * static_cast<int>(blockIdx.x) + half};
-    if (tx * kTile >= in.width) return;  // the right half of an odd tile row: no barrier waits on it
-    frontend_tile(in, sc, tb, out, tx, static_cast<int>(blockIdx.y), smem + half * (kTileSmemStride / sizeof(float)),
-                  1 + half);
+    int tx{2 * static_cast<int>(blockIdx.x) + half};
+    int ty{static_cast<int>(blockIdx.y)};
+    if constexpr (kOrdered) {
+        // Entries 2b, 2b + 1 of the order for CTA b (raster over the grid,
+        // which has at least ntiles / 2 CTAs).
+        const int tiles_x{(in.width + kTile - 1) / kTile};
+        const int ntiles{tiles_x * ((in.height + kTile - 1) / kTile)};
+        const int slot{2 * (static_cast<int>(blockIdx.y * gridDim.x + blockIdx.x)) + half};
+        if (slot >= ntiles) return;  // no barrier waits on it
+        const int tile{static_cast<int>(in.tile_order[slot])};
+        tx = tile % tiles_x;
+        ty = tile / tiles_x;
+    } else {
+        if (tx * kTile >= in.width) return;  // the right half of an odd tile row: no barrier waits on it
+    }
+    frontend_tile(in, sc, tb, out, tx, ty, smem + half * (kTileSmemStride / sizeof(float)), 1 + half);
 }
 
 // One tile of a batched launch, kept out of line: inlined into the work loop,
@@ -1769,7 +1784,9 @@ bool frontend_tables_init(FrontendTables* tables) {
     tables->sel_weight = d_sw;
     tables->log2_1p = d_l2;
     tables->llf_basis = d_ob;
-    return cudaFuncSetAttribute(frontend_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(frontend_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(2 * kTileSmemStride)) == cudaSuccess &&
+           cudaFuncSetAttribute(frontend_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(2 * kTileSmemStride)) == cudaSuccess &&
            cudaFuncSetAttribute(frontend_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(kSmemBytes)) == cudaSuccess &&
@@ -1781,7 +1798,13 @@ bool frontend_launch(const FrontendInputs& in, const FrontendScalars& s, const F
                      const FrontendOutputs& out, void* stream) {
     const int tiles_x{(in.width + kTile - 1) / kTile};
     const dim3 grid{static_cast<unsigned>((tiles_x + 1) / 2), static_cast<unsigned>((in.height + kTile - 1) / kTile)};
-    frontend_kernel<<<grid, kPairThreads, 2 * kTileSmemStride, static_cast<cudaStream_t>(stream)>>>(in, s, t, out);
+    if (in.tile_order != nullptr) {
+        frontend_kernel<true><<<grid, kPairThreads, 2 * kTileSmemStride, static_cast<cudaStream_t>(stream)>>>(in, s, t,
+                                                                                                           out);
+    } else {
+        frontend_kernel<false><<<grid, kPairThreads, 2 * kTileSmemStride, static_cast<cudaStream_t>(stream)>>>(in, s, t,
+                                                                                                            out);
+    }
     return cudaGetLastError() == cudaSuccess;
 }
 

@@ -55,6 +55,11 @@ struct FrontendInputs {
     // decided regions ([bh][bw]).
     const std::int8_t* net_class;
     const std::int16_t* net_qf;
+    // Null, or the order in which the single-frame kernel takes the 64x64
+    // tiles (raster indices; its CTA b runs entries 2b and 2b + 1): with
+    // learned decisions, the tiles whose regions are all decided come first,
+    // so that a CTA's two tiles, which it waits for together, cost alike.
+    const std::uint32_t* tile_order;
 };
 
 // Read-only tables in device memory (built once per device by
