@@ -193,7 +193,9 @@ cujpegxl_status cujpegxl_b200_encoder_memory(cujpegxl_encoder* encoder, size_t* 
  * work list, then each entropy pass runs once for all frames (frames in
  * groups of 64 per launch). The first encode times the candidate frontend
  * schedules (cujpegxl_b200_batch_schedule) and keeps the fastest, and later
- * batches of the same geometry mix reuse it; later encodes with the same
+ * batches of the same geometry mix reuse it (the environment variable
+ * CUJPEGXL_B200_BATCH_TILES_PER_CTA, 1 or 2, restricts the candidates to
+ * one CTA shape, read when a batch tunes); later encodes with the same
  * input addresses relaunch that graph, new addresses are recaptured and the
  * graph updated in place. The call is asynchronous:
  * cujpegxl_b200_batch_sync waits and reports every frame's size, after which
