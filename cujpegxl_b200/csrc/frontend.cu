@@ -1517,15 +1517,16 @@ __device__ __forceinline__ void frontend_tile(const FrontendInputs& in, const Fr
     }
 }
 
-// Tiles (2 blockIdx.x, blockIdx.y) and (2 blockIdx.x + 1, blockIdx.y), one per
-// half of the CTA, each half on its own named barrier. The two tiles start
-// together and run the same code at about the same time, so each instruction
-// fetch serves the warps of both; as two CTAs per SM (each one tile at its
-// own point of the long unrolled code) the tiles' instruction fetches
-// competed, and a DCT32 selection row pass took about 7K cycles against
-// 2.9K when its code was still cached.
-// kOrdered: the tiles come from in.tile_order (a separate instantiation, so
-// that the kernel without the order compiles as it did before it existed).
+// Two tiles per CTA, one per half, each half on its own named barrier:
+// tiles (2 blockIdx.x, blockIdx.y) and (2 blockIdx.x + 1, blockIdx.y), or with
+// kOrdered entries 2b and 2b + 1 of in.tile_order for CTA b. The two tiles
+// start together and run the same code at about the same time, so each
+// instruction fetch serves the warps of both; as two CTAs per SM (each one
+// tile at its own point of the long unrolled code) the tiles' instruction
+// fetches competed, and a DCT32 selection row pass took about 7K cycles
+// against 2.9K when its code was still cached. kOrdered is a separate
+// instantiation so that the kernel without an order carries none of its
+// index arithmetic (which slowed it by 0.6%).
 template <bool kOrdered>
 __global__ void __launch_bounds__(kPairThreads, 1)
     frontend_kernel(FrontendInputs in, FrontendScalars sc, FrontendTables tb, FrontendOutputs out) {
