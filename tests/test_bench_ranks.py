@@ -85,3 +85,23 @@ def test_streams_option_is_bounded_by_the_step():
                        capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
     assert "--streams must be 1..16, got 24" in r.stderr
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`--impl reference` times the CPU restatement on the host cores and
+    prints one JSON line with the same metric as the GPU arm, a
+    cpu_baseline describing the run and an e2e block without copies."""
+    import json
+    import subprocess
+
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"] == "4K frames/s" and line["unit"] == "frames/s" and line["higher_is_better"] is True
+    assert line["value"] > 0 and line["steps"] == 1 and line["n_gpus"] == 1
+    assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": "frames/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
