@@ -41,4 +41,6 @@ def test_half_conversion_exact():
     vals = np.concatenate([rng.normal(0, 1e-4, 20000), rng.normal(0, 2.0, 20000), rng.uniform(-7e4, 7e4, 2000),
                            (np.arange(-3000, 3000) * 2.0 ** -25)]).astype(np.float32)
     got = np.array([o.oracle_f2h(float(v)) for v in vals], np.uint16)
-    np.testing.assert_array_equal(got, vals.astype(np.float16).view(np.uint16))
+    with np.errstate(over="ignore"):  # values past 65504 round to infinity, as they should
+        want = vals.astype(np.float16).view(np.uint16)
+    np.testing.assert_array_equal(got, want)
